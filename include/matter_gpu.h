@@ -1,0 +1,206 @@
+/*
+ * matter_gpu.h — C ABI of the B200 MPM time step (libmatter_gpu.so).
+ *
+ * The reference (Matter, C++17/OpenMP) has no FFI: its setup code calls the
+ * member functions of class Simulation directly.  Each entry point below
+ * replaces one such call (or the part of it that moves data), and the host
+ * drop-in (matter_tests_b200/host/) binds them behind the unchanged
+ * Simulation surface.  All functions return MTR_OK (0) or a negative
+ * MTR_ERR_* code; no C++ exception crosses this boundary.  Pointers are plain
+ * host pointers; sizes are element counts.  A context is not thread-safe.
+ *
+ * Layout conventions shared by every entry point:
+ *   - vectors are AoS doubles, `dim` per particle (x[p*dim + d]);
+ *   - matrices are per particle, column-major, dim*dim doubles
+ *     (F[p*dim*dim + c*dim + r]) — the storage order of the reference's
+ *     Eigen TM in std::vector<TM> (data_structures.hpp:29-45);
+ *   - particle scalars are six doubles per particle in the order
+ *     MTR_SCALAR_* below.
+ */
+#ifndef MATTER_GPU_H
+#define MATTER_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes ------------------------------------------------------- */
+#define MTR_OK                    0
+#define MTR_ERR_INVALID          -1  /* bad argument or unsupported option   */
+#define MTR_ERR_CUDA             -2  /* a CUDA runtime call failed           */
+#define MTR_ERR_OOM              -3  /* device allocation failed             */
+#define MTR_ERR_DEVICE_STATUS    -4  /* the step raised a status flag; see mtr_status */
+#define MTR_ERR_TIMEOUT          -5  /* bounded wait for the device expired  */
+#define MTR_ERR_NO_DEVICE        -6  /* no CUDA device is visible            */
+#define MTR_ERR_STATE            -7  /* call out of order (e.g. step before upload) */
+
+/* ---- device status flags (mtr_status) ----------------------------------- */
+#define MTR_STATUS_GRID_OVERFLOW   0x0001u /* grid outgrew capacity; host regrows and retries */
+#define MTR_STATUS_STENCIL_OOB     0x0002u /* a particle stencil left the grid (skipped)     */
+#define MTR_STATUS_BAD_BC          0x0004u /* invalid BC enum (boundary_collision.cpp:66-70) */
+#define MTR_STATUS_RMA_NOCONV      0x0008u /* Newton loop hit its cap where the reference sets exit=1 */
+#define MTR_STATUS_RMA_NOSTEP      0x0010u /* limited search found no admissible step        */
+#define MTR_STATUS_NEG_DGAMMA      0x0020u /* Perzyna delta_gamma < 0 (plasticity.cpp:286-289) */
+#define MTR_STATUS_NONFINITE       0x0040u /* NaN/Inf in particle state                       */
+#define MTR_STATUS_BAD_MODEL       0x0080u /* invalid plastic/hardening model                 */
+#define MTR_STATUS_RESID_DIFF      0x0100u /* Perzyna Newton derivative ~ 0                   */
+
+/* ---- enums: numbering identical to tools.hpp:53-57 ---------------------- */
+enum mtr_plate_type { MTR_PLATE_TOP = 0, MTR_PLATE_BOTTOM, MTR_PLATE_LEFT, MTR_PLATE_RIGHT,
+                      MTR_PLATE_FRONT, MTR_PLATE_BACK };
+enum mtr_elastic_model { MTR_EL_HENCKY = 0, MTR_EL_NEOHOOKEAN };
+enum mtr_plastic_model { MTR_PM_NOPLASTICITY = 0, MTR_PM_VM, MTR_PM_DP, MTR_PM_DPSOFT, MTR_PM_MCC,
+                         MTR_PM_VMVISC, MTR_PM_DPVISC, MTR_PM_MCCVISC, MTR_PM_DPMUI, MTR_PM_MCCMUI,
+                         MTR_PM_SNOW };
+enum mtr_hardening_law { MTR_HL_NOHARD = 0, MTR_HL_EXPOEXPL, MTR_HL_EXPOIMPL, MTR_HL_SINHEXPL,
+                         MTR_HL_SINHIMPL };
+enum mtr_bc { MTR_BC_NOSLIP = 0, MTR_BC_SLIPSTICK, MTR_BC_SLIPFREE };
+
+/* analytic level-set objects (objects/object_*.hpp); prm[] meaning per kind */
+enum mtr_object_kind {
+  MTR_OBJ_BUMP = 0,        /* object_bump.hpp:15-41     no parameters                         */
+  MTR_OBJ_GROUND = 1,      /* object_ground.hpp:16-36   prm[0] = y_ground                     */
+  MTR_OBJ_RAMP = 2,        /* object_ramp.hpp:15-40     no parameters                         */
+  MTR_OBJ_CURVE = 3,       /* object_curve.hpp:15-37    no parameters                         */
+  MTR_OBJ_GATE = 4,        /* object_gate.hpp:16-41     prm[0] = height                       */
+  MTR_OBJ_SILO = 5,        /* object_silo.hpp:16-54     prm[0] = cut (3D only)                */
+  MTR_OBJ_BOX_ROTATED = 6, /* object_box.hpp:18-43       prm[0..2] center, prm[3..5] half
+                              extents, prm[6..14] rotation, column-major (dim-sized in 2D)    */
+  MTR_OBJ_TERRAIN_GAUSS = 7 /* no reference counterpart: surface y = prm[0] + sum_k h_k *
+                              exp(-r_k^2 / (2 sigma_k^2)), prm[1] = nbumps (<= 4), bump k at
+                              prm[2+4k..5+4k] = (x_k, z_k, h_k, sigma_k); 2D ignores z_k      */
+};
+
+/* scalar slots per particle (data_structures.hpp:16-21) */
+enum { MTR_SCALAR_EPS_PL_DEV = 0, MTR_SCALAR_EPS_PL_VOL, MTR_SCALAR_EPS_PL_VOL_PRADHANA,
+       MTR_SCALAR_DELTA_GAMMA, MTR_SCALAR_VISCOSITY, MTR_SCALAR_MUI, MTR_NUM_SCALARS };
+
+enum mtr_precision { MTR_PREC_FP64 = 0, MTR_PREC_MIXED = 1 };
+
+/* Public fields of Simulation (simulation.hpp:28-106) that the step reads,
+ * plus the compile-time choices of tools.hpp:19-21 (dim, spline degree) that
+ * become run-time fields here. */
+typedef struct mtr_params {
+  int32_t dim;              /* 2 or 3 (tools.hpp:20 THREEDIM)                    */
+  int32_t spline_deg;       /* 2 or 3 (tools.hpp:21 SPLINEDEG)                   */
+  int32_t precision;        /* enum mtr_precision                                */
+  int32_t elastic_model;    /* enum mtr_elastic_model                            */
+  int32_t plastic_model;    /* enum mtr_plastic_model                            */
+  int32_t hardening_law;    /* enum mtr_hardening_law                            */
+  int32_t use_pradhana, use_mises_q, use_mibf, use_musl;
+  int32_t gravity_special;
+  int32_t pbc;              /* must be 0 (periodic BCs are not part of this path) */
+  uint32_t end_frame;
+  int32_t change_particle_positions; /* hard-coded teleport hook, position_update.cpp:35-41 */
+  double fps, cfl, cfl_elastic, flip_ratio, rho, gravity_time;
+  double gravity[3];
+  double grid_reference_point[3];
+  double dx, particle_mass, particle_volume;
+  double E, nu, stress_tolerance, xi;
+  double q_max, q_min, p_min;
+  double M, q_cohesion;
+  double perzyna_exp, perzyna_visc;
+  double beta, p0;
+  double rho_s, grain_diameter, I_ref, mu_1, mu_2;
+} mtr_params;
+
+/* ObjectPlate state (object_plate.hpp:13-24, 136-190). v_object[2] unused in 2D. */
+typedef struct mtr_plate {
+  int32_t plate_type;       /* enum mtr_plate_type */
+  int32_t bc;               /* enum mtr_bc         */
+  double friction;
+  double pos_object, pos_lower, pos_upper;
+  double v_object[3];
+  double v_object_original[3];
+  double vmin_factor, load_factor;
+} mtr_plate;
+
+typedef struct mtr_object {
+  int32_t kind;             /* enum mtr_object_kind */
+  int32_t bc;               /* enum mtr_bc          */
+  double friction;
+  double prm[24];
+} mtr_object;
+
+typedef struct mtr_clock {
+  double time;              /* simulated time after the last completed step      */
+  double dt;                /* dt of the last completed step                      */
+  uint32_t step;            /* current_time_step                                  */
+  uint32_t frame;
+  int32_t done;             /* 1 once final_time is reached (simulation.cpp:191)  */
+  int32_t reserved;
+} mtr_clock;
+
+typedef struct mtr_ctx mtr_ctx;
+
+/* Validates the parameters and derives the constants of Simulation::simulate
+ * (simulation.cpp:94-136: Lame constants, dt_max, prefactors, apicDinverse,
+ * fac_Q).  Replaces the constant block at the top of simulate(). */
+int mtr_ctx_create(const mtr_params* params, int device, mtr_ctx** out);
+
+/* Copies the particle state in (replaces the host-side Particles arrays the
+ * reference mutates in place, data_structures.hpp:8-47).  Any of v, F, B,
+ * scalars may be NULL (zero velocity, identity F, zero B, zero scalars).  With
+ * use_mibf the muI slot is initialised as simulate() does (simulation.cpp:138-145). */
+int mtr_upload(mtr_ctx* ctx, const double* x, const double* v, const double* F, const double* B,
+               const double* scalars, uint32_t Np);
+
+/* Replaces the plate and object lists (simulation.hpp:109-110). */
+int mtr_set_objects(mtr_ctx* ctx, const mtr_plate* plates, int n_plates,
+                    const mtr_object* objects, int n_objects);
+
+/* Advances up to nsteps calls of Simulation::advanceStep (simulation.cpp:219-273)
+ * including the time/frame bookkeeping of simulate() (simulation.cpp:176-200);
+ * stops early once the final time is reached.  Asynchronous on the context's
+ * stream except for a status read every `nsteps` steps. */
+int mtr_step(mtr_ctx* ctx, int nsteps);
+
+/* Runs Simulation::simulate's loop (simulation.cpp:168-201) to the end. */
+int mtr_run(mtr_ctx* ctx);
+
+/* Copies the particle state back in the original particle order (any pointer
+ * may be NULL).  Also returns pic and flip of the last step if requested. */
+int mtr_download(mtr_ctx* ctx, double* x, double* v, double* F, double* B, double* scalars);
+int mtr_download_pic_flip(mtr_ctx* ctx, double* pic, double* flip);
+
+/* Grid of the last completed step (Simulation::grid, data_structures.hpp:49-66):
+ * dims[0..2] = Nx, Ny, Nz (Nz = 1 in 2D); axis coordinates; mass, v, flip in
+ * the reference's node order ind = (i*Ny + j)*Nz + k (simulation.hpp:196-204).
+ * Pass NULL for arrays to query dims only. */
+int mtr_get_grid(mtr_ctx* ctx, uint32_t dims[3], double* gx, double* gy, double* gz,
+                 double* mass, double* v, double* flip);
+
+/* Cell keys and stable sort order of the last step's particle sort, both in
+ * the particle order of the sort's input, for bit-exact checks. */
+int mtr_get_sort(mtr_ctx* ctx, uint32_t* keys_in_input_order, uint32_t* sorted_input_index,
+                 uint32_t* input_particle_id);
+
+int mtr_get_plates(mtr_ctx* ctx, mtr_plate* plates, int n_plates);
+int mtr_get_clock(mtr_ctx* ctx, mtr_clock* clock);
+
+/* Device status word (bit flags MTR_STATUS_*) and the first particle (original
+ * id) that raised one.  The reference's analogue is the int exit flag
+ * (simulation.hpp:28) polled once per step (simulation.cpp:176-177). */
+int mtr_status(mtr_ctx* ctx, uint32_t* flags, uint32_t* first_bad);
+int mtr_clear_status(mtr_ctx* ctx);
+
+/* Bounded wait for the context's stream (polls cudaEventQuery). */
+int mtr_sync(mtr_ctx* ctx, double timeout_seconds);
+
+/* The context's CUDA stream (cudaStream_t as an opaque pointer) for timing. */
+void* mtr_stream(mtr_ctx* ctx);
+
+/* Number of kernel launches issued by the last mtr_step call. */
+int64_t mtr_launch_count(mtr_ctx* ctx);
+
+void mtr_ctx_destroy(mtr_ctx* ctx);
+
+/* Last error message of this thread (static storage). */
+const char* mtr_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MATTER_GPU_H */
