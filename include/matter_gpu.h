@@ -195,6 +195,13 @@ void* mtr_stream(mtr_ctx* ctx);
 /* Number of kernel launches issued by the last mtr_step call. */
 int64_t mtr_launch_count(mtr_ctx* ctx);
 
+/* Test and timing controls (no counterpart in the reference):
+ * mtr_keep_pic_flip makes the step keep each particle's pic and flip vectors
+ * (Particles::pic/flip, data_structures.hpp:12-13) for mtr_download_pic_flip;
+ * mtr_use_graphs turns CUDA-graph replay of the step on (default) or off. */
+int mtr_keep_pic_flip(mtr_ctx* ctx, int on);
+int mtr_use_graphs(mtr_ctx* ctx, int on);
+
 void mtr_ctx_destroy(mtr_ctx* ctx);
 
 /* Last error message of this thread (static storage). */

@@ -1,0 +1,852 @@
+// mtr_abi.cu — the C ABI of include/matter_gpu.h: context, transfers and the
+// step loop of Simulation::simulate (simulation.cpp:73-213) driving the
+// kernels of mtr_kernels.cuh on one CUDA stream.
+//
+// A step is ~16 kernel launches with no host synchronisation: dt, the grid
+// extents and the clock live in a device-side StepHeader.  Steps are captured
+// into CUDA graphs of kGraphSteps steps (two variants, one per starting
+// particle buffer) and replayed; the host reads the header back once per
+// mtr_step call.  If the grid outgrows its capacity the header kernel aborts
+// the step before any state is touched, every later kernel of the batch skips,
+// and the host regrows the grid buffers, re-captures the graphs and resumes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/matter_gpu.h"
+#include "mtr_kernels.cuh"
+
+using namespace mtr;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct MtrError {
+  int code;
+  std::string msg;
+};
+
+#define CK(call)                                                                                      \
+  do {                                                                                                \
+    cudaError_t e_ = (call);                                                                          \
+    if (e_ != cudaSuccess) throw MtrError{MTR_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+  } while (0)
+
+constexpr int kGraphSteps = 16;
+
+template <typename T>
+T* dalloc(size_t n) {
+  void* p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+  if (e != cudaSuccess) throw MtrError{MTR_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
+  return static_cast<T*>(p);
+}
+
+void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+
+int nsym(int d) { return d == 3 ? 6 : 3; }
+
+}  // namespace
+
+struct mtr_ctx {
+  mtr_params prm{};
+  DevParams hp{};
+  int device = 0;
+  int dim = 3, deg = 2;
+  cudaStream_t stream = nullptr;
+  DevParams* dP = nullptr;
+  StepHeader* dH = nullptr;
+  StepHeader* hH = nullptr;  // pinned mirror
+  uint32_t Np = 0;
+  bool uploaded = false;
+  // particle buffers (two sets) and their backing allocations
+  PBuf buf[2]{};
+  std::vector<void*> pallocs;
+  double *pic = nullptr, *flip = nullptr;
+  // grid
+  uint32_t cap_axis[3] = {0, 0, 0};
+  uint32_t cap_nodes = 0, cap_tiles = 0;
+  double *gx = nullptr, *gy = nullptr, *gz = nullptr;
+  double *acc = nullptr, *nv = nullptr, *nflip = nullptr, *nmass = nullptr, *nfric = nullptr, *v2 = nullptr;
+  uint32_t *tile_begin = nullptr, *tile_end = nullptr;
+  // sort
+  uint32_t *keys0 = nullptr, *keysA = nullptr, *valsA = nullptr, *keysB = nullptr, *valsB = nullptr;
+  uint32_t *hist = nullptr, *dtot = nullptr;
+  int sort_blocks = 0, passes = 0;
+  BBoxPartial* partials = nullptr;
+  int npartials = 0;
+  double* staging = nullptr;  // Np * dim * dim doubles
+  // plates/objects
+  std::vector<mtr_plate> plates;
+  std::vector<mtr_object> objects;
+  // graphs
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  int host_parity = 0;
+  int64_t launches_last = 0;
+  int launches_per_step = 0;
+  bool use_graphs = true;
+};
+
+namespace {
+
+void set_error(const std::string& m) { g_last_error = m; }
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    return f();
+  } catch (const MtrError& e) {
+    set_error(e.msg);
+    return e.code;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return MTR_ERR_INVALID;
+  } catch (...) {
+    set_error("unknown error");
+    return MTR_ERR_INVALID;
+  }
+}
+
+void free_grid(mtr_ctx* c) {
+  for (void* p : {(void*)c->gx, (void*)c->gy, (void*)c->gz, (void*)c->acc, (void*)c->nv, (void*)c->nflip,
+                  (void*)c->nmass, (void*)c->nfric, (void*)c->v2, (void*)c->tile_begin, (void*)c->tile_end})
+    dfree(p);
+  c->gx = c->gy = c->gz = c->acc = c->nv = c->nflip = c->nmass = c->nfric = c->v2 = nullptr;
+  c->tile_begin = c->tile_end = nullptr;
+}
+
+void free_graphs(mtr_ctx* c) {
+  for (auto& g : c->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
+
+int tile_edge(int d) { return d == 3 ? 4 : 8; }
+
+// (Re)allocates the grid for per-axis node capacities.
+void alloc_grid(mtr_ctx* c, const uint32_t want[3]) {
+  free_grid(c);
+  const int d = c->dim, tb = tile_edge(d);
+  uint64_t nodes = 1, tiles = 1;
+  for (int a = 0; a < 3; ++a) {
+    c->cap_axis[a] = (a < d) ? std::max<uint32_t>(want[a], 8u) : 1u;
+    nodes *= c->cap_axis[a];
+    tiles *= (a < d) ? (c->cap_axis[a] + tb - 1) / tb : 1;
+  }
+  if (nodes > 0xffffffffull / 8 || tiles * 64ull > 0xffffffffull)
+    throw MtrError{MTR_ERR_OOM, "grid capacity exceeds the 32-bit node/key range"};
+  c->cap_nodes = (uint32_t)nodes;
+  c->cap_tiles = (uint32_t)tiles;
+  const int nch = 2 + 2 * d;
+  c->gx = dalloc<double>(c->cap_axis[0]);
+  c->gy = dalloc<double>(c->cap_axis[1]);
+  c->gz = dalloc<double>(c->cap_axis[2]);
+  c->acc = dalloc<double>((size_t)nch * nodes);
+  c->nv = dalloc<double>((size_t)d * nodes);
+  c->nflip = dalloc<double>((size_t)d * nodes);
+  c->nmass = dalloc<double>(nodes);
+  c->nfric = dalloc<double>(nodes);
+  c->v2 = dalloc<double>((size_t)d * nodes);
+  c->tile_begin = dalloc<uint32_t>(tiles);
+  c->tile_end = dalloc<uint32_t>(tiles);
+  CK(cudaMemsetAsync(c->acc, 0, sizeof(double) * nch * nodes, c->stream));
+  CK(cudaMemsetAsync(c->nv, 0, sizeof(double) * d * nodes, c->stream));
+  CK(cudaMemsetAsync(c->nflip, 0, sizeof(double) * d * nodes, c->stream));
+  CK(cudaMemsetAsync(c->nmass, 0, sizeof(double) * nodes, c->stream));
+  CK(cudaMemsetAsync(c->v2, 0, sizeof(double) * d * nodes, c->stream));
+  uint64_t keybits = 1;
+  while ((1ull << keybits) < tiles * 64ull) ++keybits;
+  c->passes = (int)((keybits + 7) / 8);
+}
+
+StepArgs make_args(mtr_ctx* c, int parity) {
+  StepArgs A{};
+  A.P = c->dP;
+  A.H = c->dH;
+  A.partials = c->partials;
+  A.npartials = c->npartials;
+  A.Np = c->Np;
+  A.gx = c->gx;
+  A.gy = c->gy;
+  A.gz = c->gz;
+  for (int a = 0; a < 3; ++a) A.cap_axis[a] = c->cap_axis[a];
+  A.cap_nodes = c->cap_nodes;
+  A.cap_tiles = c->cap_tiles;
+  A.acc = c->acc;
+  A.nv = c->nv;
+  A.nflip = c->nflip;
+  A.nmass = c->nmass;
+  A.nfric = c->nfric;
+  A.v2 = c->v2;
+  A.keys0 = c->keys0;
+  A.keysA = c->keysA;
+  A.valsA = c->valsA;
+  A.keysB = c->keysB;
+  A.valsB = c->valsB;
+  A.hist = c->hist;
+  A.dtot = c->dtot;
+  A.sort_blocks = c->sort_blocks;
+  A.tile_begin = c->tile_begin;
+  A.tile_end = c->tile_end;
+  A.in = c->buf[parity];
+  A.out = c->buf[1 - parity];
+  A.pic = c->pic;
+  A.flip = c->flip;
+  return A;
+}
+
+// Enqueues one step reading buffer `parity` and writing the other.  Returns
+// the number of kernels launched.
+template <int D, int DEG>
+int enqueue_step_t(mtr_ctx* c, int parity) {
+  cudaStream_t st = c->stream;
+  StepArgs A = make_args(c, parity);
+  int n = 0;
+  const uint32_t pblocks = (c->Np + 127) / 128;
+  k_bbox<D><<<c->npartials, 256, 0, st>>>(A);
+  ++n;
+  k_header<D><<<1, 32, 0, st>>>(A);
+  ++n;
+  // sort
+  const uint32_t* skeys = nullptr;
+  const uint32_t* perm = nullptr;
+  for (int pass = 0; pass < c->passes; ++pass) {
+    const int shift = 8 * pass;
+    const uint32_t* ksrc = pass == 0 ? c->keys0 : ((pass & 1) ? c->keysB : c->keysA);
+    const uint32_t* vsrc = pass == 0 ? nullptr : ((pass & 1) ? c->valsB : c->valsA);
+    uint32_t* kdst = (pass & 1) ? c->keysA : c->keysB;
+    uint32_t* vdst = (pass & 1) ? c->valsA : c->valsB;
+    if (pass == 0)
+      k_sort_hist<D, true><<<c->sort_blocks, kSortThreads, 0, st>>>(A, nullptr, shift);
+    else
+      k_sort_hist<D, false><<<c->sort_blocks, kSortThreads, 0, st>>>(A, ksrc, shift);
+    k_sort_scan<<<256, 256, 0, st>>>(A);
+    k_sort_scatter<<<c->sort_blocks, kSortThreads, 0, st>>>(A, ksrc, vsrc, kdst, vdst, shift);
+    n += 3;
+    skeys = kdst;
+    perm = vdst;
+  }
+  CK(cudaMemsetAsync(c->tile_begin, 0, sizeof(uint32_t) * c->cap_tiles, st));
+  CK(cudaMemsetAsync(c->tile_end, 0, sizeof(uint32_t) * c->cap_tiles, st));
+  k_tile_ranges<<<std::min<uint32_t>((c->Np + 255) / 256, 148 * 8), 256, 0, st>>>(A, skeys);
+  ++n;
+  k_p2g<D, DEG><<<c->cap_tiles, 128, 0, st>>>(A, perm);
+  ++n;
+  const uint32_t gblocks = std::min<uint32_t>((c->cap_nodes + 255) / 256, 148 * 16);
+  k_grid<D><<<gblocks, 256, 0, st>>>(A);
+  ++n;
+  if (c->prm.use_musl) {
+    CK(cudaMemsetAsync(c->v2, 0, sizeof(double) * D * c->cap_nodes, st));
+    k_g2p_musl<D, DEG><<<c->cap_tiles, 128, 0, st>>>(A, perm);
+    k_musl_norm<D><<<gblocks, 256, 0, st>>>(A);
+    k_defgrad<D, DEG><<<pblocks, 128, 0, st>>>(A, perm);
+    n += 3;
+  } else {
+    k_g2p<D, DEG><<<pblocks, 128, 0, st>>>(A, perm);
+    ++n;
+  }
+  k_tail<D><<<1, 32, 0, st>>>(A, 1 - parity);
+  ++n;
+  CK(cudaGetLastError());
+  return n;
+}
+
+int enqueue_step(mtr_ctx* c, int parity) {
+  if (c->dim == 3) return c->deg == 3 ? enqueue_step_t<3, 3>(c, parity) : enqueue_step_t<3, 2>(c, parity);
+  return c->deg == 3 ? enqueue_step_t<2, 3>(c, parity) : enqueue_step_t<2, 2>(c, parity);
+}
+
+void build_graphs(mtr_ctx* c) {
+  free_graphs(c);
+  if (!c->use_graphs) return;
+  for (int p0 = 0; p0 < 2; ++p0) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int n = 0;
+    try {
+      for (int s = 0; s < kGraphSteps; ++s) n += enqueue_step(c, (p0 + s) & 1);
+    } catch (...) {
+      cudaStreamEndCapture(c->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    CK(cudaStreamEndCapture(c->stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&c->graph[p0], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) throw MtrError{MTR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)};
+    c->launches_per_step = n / kGraphSteps;
+  }
+}
+
+void read_header(mtr_ctx* c) {
+  CK(cudaMemcpyAsync(c->hH, c->dH, sizeof(StepHeader), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+}
+
+void write_header(mtr_ctx* c) { CK(cudaMemcpyAsync(c->dH, c->hH, sizeof(StepHeader), cudaMemcpyHostToDevice, c->stream)); }
+
+void upload_params(mtr_ctx* c) {
+  c->hp.nplates = (int)c->plates.size();
+  c->hp.nobjects = (int)c->objects.size();
+  for (size_t i = 0; i < c->objects.size(); ++i) c->hp.objects[i] = c->objects[i];
+  CK(cudaMemcpyAsync(c->dP, &c->hp, sizeof(DevParams), cudaMemcpyHostToDevice, c->stream));
+}
+
+void derive_constants(mtr_ctx* c) {  // simulation.cpp:94-136
+  const mtr_params& p = c->prm;
+  DevParams& h = c->hp;
+  const int d = p.dim;
+  h.dim = d;
+  h.deg = p.spline_deg;
+  h.plastic_model = p.plastic_model;
+  h.elastic_model = p.elastic_model;
+  h.hardening_law = p.hardening_law;
+  h.use_pradhana = p.use_pradhana;
+  h.use_mises_q = p.use_mises_q;
+  h.use_mibf = p.use_mibf;
+  h.use_musl = p.use_musl;
+  h.gravity_special = p.gravity_special;
+  h.change_particle_positions = p.change_particle_positions;
+  h.end_frame = p.end_frame;
+  h.flip_ratio = p.flip_ratio;
+  h.cfl = p.cfl;
+  h.dx = p.dx;
+  h.one_over_dx = 1.0 / p.dx;
+  h.apicDinverse = p.spline_deg == 3 ? 3.0 / (p.dx * p.dx) : 4.0 / (p.dx * p.dx);
+  h.particle_mass = p.particle_mass;
+  h.particle_volume = p.particle_volume;
+  h.lambda = p.nu * p.E / ((1.0 + p.nu) * (1.0 - 2.0 * p.nu));
+  h.mu = p.E / (2.0 * (1.0 + p.nu));
+  h.K = h.lambda + 2.0 * h.mu / d;  // simulation.cpp:288-290
+  h.wave_speed = std::sqrt(p.E / p.rho);
+  h.dt_max = p.cfl_elastic * p.dx / h.wave_speed;
+  h.frame_dt = 1.0 / p.fps;
+  h.final_time = p.end_frame * h.frame_dt;
+  if (p.use_mises_q) {
+    h.q_prefac = std::sqrt(3.0) / std::sqrt(2.0);
+    h.d_prefac = std::sqrt(2.0) / std::sqrt(3.0);
+  } else {
+    h.q_prefac = 1.0 / std::sqrt(2.0);
+    h.d_prefac = std::sqrt(2.0);
+  }
+  h.e_mu_prefac = 2 * h.q_prefac * h.mu;
+  h.f_mu_prefac = 2 * h.q_prefac / h.d_prefac * h.mu;
+  h.rma_prefac = 2 * h.q_prefac * h.q_prefac;
+  h.fac_Q = p.I_ref / (p.grain_diameter * std::sqrt(p.rho_s));
+  for (int a = 0; a < 3; ++a) {
+    h.gravity_final[a] = a < d ? p.gravity[a] : 0.0;
+    h.grid_ref[a] = a < d ? p.grid_reference_point[a] : 0.0;
+  }
+  h.gravity_time = p.gravity_time;
+  h.E = p.E;
+  h.nu = p.nu;
+  h.stress_tolerance = p.stress_tolerance;
+  h.xi = p.xi;
+  h.q_max = p.q_max;
+  h.q_min = p.q_min;
+  h.p_min = p.p_min;
+  h.M = p.M;
+  h.q_cohesion = p.q_cohesion;
+  h.perzyna_exp = p.perzyna_exp;
+  h.perzyna_visc = p.perzyna_visc;
+  h.beta = p.beta;
+  h.p0 = p.p0;
+  h.mu_1 = p.mu_1;
+  h.mu_2 = p.mu_2;
+}
+
+// The first step's grid extents, as remeshFixedInit(2,2,2) will compute them
+// (remesh.cpp:38-182), to size the initial grid allocation.
+void initial_grid_extent(mtr_ctx* c, const double* x, uint32_t want[3]) {
+  const int d = c->dim;
+  const double dx = c->prm.dx;
+  for (int a = 0; a < 3; ++a) want[a] = 1;
+  for (int a = 0; a < d; ++a) {
+    double mn = x[a], mx = x[a];
+    for (uint32_t p = 1; p < c->Np; ++p) {
+      double v = x[(size_t)p * d + a];
+      mn = std::min(mn, v);
+      mx = std::max(mx, v);
+    }
+    const double g = c->prm.grid_reference_point[a];
+    if (c->prm.grid_reference_point[0] < 1e10) {
+      mn = std::min(mn, g);
+      mx = std::max(mx, g);
+    }
+    const double n = (mx - mn) / dx + 6.0;
+    want[a] = (uint32_t)std::ceil(n * 1.25 + 8.0);
+  }
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+const char* mtr_last_error(void) { return g_last_error.c_str(); }
+
+int mtr_ctx_create(const mtr_params* params, int device, mtr_ctx** out) {
+  return guarded([&]() -> int {
+    if (!params || !out) throw MtrError{MTR_ERR_INVALID, "null argument"};
+    *out = nullptr;
+    const mtr_params& p = *params;
+    if (p.dim != 2 && p.dim != 3) throw MtrError{MTR_ERR_INVALID, "dim must be 2 or 3"};
+    if (p.spline_deg != 2 && p.spline_deg != 3) throw MtrError{MTR_ERR_INVALID, "spline_deg must be 2 or 3"};
+    if (p.precision != MTR_PREC_FP64) throw MtrError{MTR_ERR_INVALID, "only the FP64 path is built"};
+    if (p.pbc) throw MtrError{MTR_ERR_INVALID, "periodic boundaries are not part of this path"};
+    if (p.plastic_model < 0 || p.plastic_model > MTR_PM_SNOW) throw MtrError{MTR_ERR_INVALID, "invalid plastic model"};
+    if (p.elastic_model != MTR_EL_HENCKY && p.elastic_model != MTR_EL_NEOHOOKEAN)
+      throw MtrError{MTR_ERR_INVALID, "invalid elastic model"};
+    if (p.elastic_model != MTR_EL_HENCKY && p.plastic_model != MTR_PM_NOPLASTICITY)  // simulation.cpp:80-84
+      throw MtrError{MTR_ERR_INVALID, "This plastic model is only compatible with Hencky's elasticity model"};
+    if (!(p.dx > 0) || !(p.fps > 0) || !(p.rho > 0)) throw MtrError{MTR_ERR_INVALID, "dx, fps and rho must be > 0"};
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw MtrError{MTR_ERR_NO_DEVICE, "no CUDA device"};
+    if (device < 0 || device >= ndev) throw MtrError{MTR_ERR_INVALID, "device index out of range"};
+    mtr_ctx* c = new mtr_ctx();
+    try {
+      c->prm = p;
+      c->device = device;
+      c->dim = p.dim;
+      c->deg = p.spline_deg;
+      CK(cudaSetDevice(device));
+      CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+      derive_constants(c);
+      c->dP = dalloc<DevParams>(1);
+      c->dH = dalloc<StepHeader>(1);
+      CK(cudaMallocHost((void**)&c->hH, sizeof(StepHeader)));
+      std::memset(c->hH, 0, sizeof(StepHeader));
+      upload_params(c);
+      CK(cudaStreamSynchronize(c->stream));
+    } catch (...) {
+      mtr_ctx_destroy(c);
+      throw;
+    }
+    *out = c;
+    return MTR_OK;
+  });
+}
+
+int mtr_upload(mtr_ctx* c, const double* x, const double* v, const double* F, const double* B,
+               const double* scalars, uint32_t Np) {
+  return guarded([&]() -> int {
+    if (!c || !x || Np == 0) throw MtrError{MTR_ERR_INVALID, "null context/positions or Np == 0"};
+    CK(cudaSetDevice(c->device));
+    const int d = c->dim, dd = d * d, ns = nsym(d);
+    free_graphs(c);
+    for (void* p : c->pallocs) dfree(p);
+    c->pallocs.clear();
+    for (void* p : {(void*)c->keys0, (void*)c->keysA, (void*)c->valsA, (void*)c->keysB, (void*)c->valsB,
+                    (void*)c->hist, (void*)c->dtot, (void*)c->partials, (void*)c->staging})
+      dfree(p);
+    c->Np = Np;
+    c->hp.Np = Np;
+    for (int s = 0; s < 2; ++s) {
+      double* blk = dalloc<double>((size_t)Np * (2 * d + 2 * dd + MTR_NUM_SCALARS + ns));
+      c->pallocs.push_back(blk);
+      c->buf[s].x = blk;
+      c->buf[s].v = blk + (size_t)Np * d;
+      c->buf[s].F = blk + (size_t)Np * 2 * d;
+      c->buf[s].B = blk + (size_t)Np * (2 * d + dd);
+      c->buf[s].sc = blk + (size_t)Np * (2 * d + 2 * dd);
+      c->buf[s].tau = blk + (size_t)Np * (2 * d + 2 * dd + MTR_NUM_SCALARS);
+      c->buf[s].id = dalloc<uint32_t>(Np);
+      c->pallocs.push_back(c->buf[s].id);
+    }
+    c->pic = dalloc<double>((size_t)Np * d);
+    c->flip = dalloc<double>((size_t)Np * d);
+    c->pallocs.push_back(c->pic);
+    c->pallocs.push_back(c->flip);
+    c->sort_blocks = (int)((Np + kSortTile - 1) / kSortTile);
+    c->keys0 = dalloc<uint32_t>(Np);
+    c->keysA = dalloc<uint32_t>(Np);
+    c->valsA = dalloc<uint32_t>(Np);
+    c->keysB = dalloc<uint32_t>(Np);
+    c->valsB = dalloc<uint32_t>(Np);
+    c->hist = dalloc<uint32_t>((size_t)256 * c->sort_blocks);
+    c->dtot = dalloc<uint32_t>(256);
+    c->npartials = (int)std::min<uint32_t>((Np + 255) / 256, 148 * 4);
+    c->partials = dalloc<BBoxPartial>(c->npartials);
+    c->staging = dalloc<double>((size_t)Np * std::max<int>(dd, (int)MTR_NUM_SCALARS));
+    // state -> buffer 0 (AoS host layout -> SoA)
+    const uint32_t blocks = (Np + 255) / 256;
+    auto put = [&](const double* host, double* dst, int width, int kind, const double* fill) {
+      if (host) {
+        CK(cudaMemcpyAsync(c->staging, host, sizeof(double) * Np * width, cudaMemcpyHostToDevice, c->stream));
+      } else {
+        std::vector<double> tmp((size_t)Np * width, 0.0);
+        if (fill)
+          for (uint32_t p = 0; p < Np; ++p)
+            for (int i = 0; i < width; ++i) tmp[(size_t)p * width + i] = fill[i];
+        CK(cudaMemcpyAsync(c->staging, tmp.data(), sizeof(double) * tmp.size(), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+      }
+      if (d == 3)
+        k_aos_to_soa<3><<<blocks, 256, 0, c->stream>>>(Np, c->staging, dst, kind);
+      else
+        k_aos_to_soa<2><<<blocks, 256, 0, c->stream>>>(Np, c->staging, dst, kind);
+      CK(cudaGetLastError());
+      CK(cudaStreamSynchronize(c->stream));
+    };
+    double eye[9] = {0};
+    for (int i = 0; i < d; ++i) eye[i * d + i] = 1.0;
+    put(x, c->buf[0].x, d, 0, nullptr);
+    put(v, c->buf[0].v, d, 0, nullptr);
+    put(F, c->buf[0].F, dd, 1, eye);
+    put(B, c->buf[0].B, dd, 1, nullptr);
+    std::vector<double> sc;
+    const double* scp = scalars;
+    if (c->prm.use_mibf) {  // simulation.cpp:138-145
+      sc.assign((size_t)Np * MTR_NUM_SCALARS, 0.0);
+      if (scalars) std::memcpy(sc.data(), scalars, sizeof(double) * sc.size());
+      const double m0 = (c->prm.plastic_model == MTR_PM_DPMUI || c->prm.plastic_model == MTR_PM_MCCMUI) ? c->prm.mu_1
+                                                                                                     : c->prm.M;
+      for (uint32_t p = 0; p < Np; ++p) sc[(size_t)p * MTR_NUM_SCALARS + MTR_SCALAR_MUI] = m0;
+      scp = sc.data();
+    }
+    put(scp, c->buf[0].sc, MTR_NUM_SCALARS, 2, nullptr);
+    // initial grid allocation
+    uint32_t want[3];
+    initial_grid_extent(c, x, want);
+    alloc_grid(c, want);
+    // header
+    std::memset(c->hH, 0, sizeof(StepHeader));
+    c->hH->first_bad = 0xffffffffu;
+    for (int a = 0; a < 3; ++a) c->hH->gravity[a] = a < d ? c->prm.gravity[a] : 0.0;
+    c->hH->done = (0 < c->prm.end_frame) ? 0 : 1;
+    for (size_t i = 0; i < c->plates.size(); ++i) c->hH->plates[i] = c->plates[i];
+    write_header(c);
+    upload_params(c);
+    StepArgs A = make_args(c, 0);
+    if (d == 3)
+      k_init_state<3><<<blocks, 256, 0, c->stream>>>(A, c->buf[0]);
+    else
+      k_init_state<2><<<blocks, 256, 0, c->stream>>>(A, c->buf[0]);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    c->host_parity = 0;
+    c->uploaded = true;
+    return MTR_OK;
+  });
+}
+
+int mtr_set_objects(mtr_ctx* c, const mtr_plate* plates, int n_plates, const mtr_object* objects, int n_objects) {
+  return guarded([&]() -> int {
+    if (!c) throw MtrError{MTR_ERR_INVALID, "null context"};
+    if (n_plates < 0 || n_plates > MTR_MAXP || n_objects < 0 || n_objects > MTR_MAXO)
+      throw MtrError{MTR_ERR_INVALID, "too many plates or objects"};
+    for (int i = 0; i < n_plates; ++i)
+      if (plates[i].bc < 0 || plates[i].bc > 2 || plates[i].plate_type < 0 || plates[i].plate_type > 5)
+        throw MtrError{MTR_ERR_INVALID, "invalid plate type or BC"};
+    for (int i = 0; i < n_objects; ++i)
+      if (objects[i].bc < 0 || objects[i].bc > 2 || objects[i].kind < 0 || objects[i].kind > MTR_OBJ_TERRAIN_GAUSS)
+        throw MtrError{MTR_ERR_INVALID, "invalid object kind or BC"};
+    CK(cudaSetDevice(c->device));
+    c->plates.assign(plates, plates + n_plates);
+    c->objects.assign(objects, objects + n_objects);
+    if (c->dim == 2)
+      for (auto& q : c->plates) q.v_object[2] = q.v_object_original[2] = 0.0;
+    upload_params(c);
+    if (c->uploaded) {
+      read_header(c);
+      for (int i = 0; i < n_plates; ++i) c->hH->plates[i] = c->plates[i];
+      write_header(c);
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return MTR_OK;
+  });
+}
+
+int mtr_step(mtr_ctx* c, int nsteps) {
+  return guarded([&]() -> int {
+    if (!c) throw MtrError{MTR_ERR_INVALID, "null context"};
+    if (!c->uploaded) throw MtrError{MTR_ERR_STATE, "mtr_step before mtr_upload"};
+    if (nsteps <= 0) return MTR_OK;
+    CK(cudaSetDevice(c->device));
+    read_header(c);
+    if (c->hH->done) return (c->hH->status & kExitMask) ? MTR_ERR_DEVICE_STATUS : MTR_OK;
+    c->host_parity = c->hH->cur;
+    int64_t launches = 0;
+    int remaining = nsteps;
+    for (int guard = 0; guard < 64 && remaining > 0; ++guard) {
+      const uint32_t step0 = c->hH->step;
+      if (c->use_graphs && (!c->graph[0] || !c->graph[1])) build_graphs(c);
+      int parity = c->host_parity;
+      int todo = remaining;
+      while (todo > 0) {
+        if (c->use_graphs && todo >= kGraphSteps) {
+          CK(cudaGraphLaunch(c->graph[parity], c->stream));
+          launches += (int64_t)c->launches_per_step * kGraphSteps;
+          todo -= kGraphSteps;  // kGraphSteps is even: parity unchanged
+        } else {
+          launches += enqueue_step(c, parity);
+          parity ^= 1;
+          todo -= 1;
+        }
+      }
+      read_header(c);
+      StepHeader& H = *c->hH;
+      c->host_parity = H.cur;
+      const int executed = (int)(H.step - step0) + ((H.status & kExitMask) && H.done ? 1 : 0);
+      remaining -= executed;
+      if (H.abort) {  // grid outgrew its capacity: regrow and resume
+        uint32_t want[3];
+        for (int a = 0; a < 3; ++a)
+          want[a] = (a < c->dim) ? std::max<uint32_t>(c->cap_axis[a], (uint32_t)std::ceil(H.N[a] * 1.25 + 8.0)) : 1u;
+        for (int a = 0; a < c->dim; ++a)
+          if (H.N[a] >= kMaxAxisNodes || H.N[a] < 4)
+            throw MtrError{MTR_ERR_OOM, "grid extent exploded or collapsed (non-finite particle positions?)"};
+        free_graphs(c);
+        alloc_grid(c, want);
+        H.abort = 0;
+        H.status &= ~MTR_STATUS_GRID_OVERFLOW;
+        write_header(c);
+        CK(cudaStreamSynchronize(c->stream));
+        continue;
+      }
+      if (H.done) break;
+    }
+    c->launches_last = launches;
+    if (c->hH->status & kExitMask) return MTR_ERR_DEVICE_STATUS;
+    return MTR_OK;
+  });
+}
+
+int mtr_run(mtr_ctx* c) {
+  for (;;) {
+    int rc = mtr_step(c, 1024);
+    if (rc != MTR_OK) return rc;
+    mtr_clock ck;
+    rc = mtr_get_clock(c, &ck);
+    if (rc != MTR_OK) return rc;
+    if (ck.done) return MTR_OK;
+  }
+}
+
+int mtr_download(mtr_ctx* c, double* x, double* v, double* F, double* B, double* scalars) {
+  return guarded([&]() -> int {
+    if (!c || !c->uploaded) throw MtrError{MTR_ERR_STATE, "nothing uploaded"};
+    CK(cudaSetDevice(c->device));
+    read_header(c);
+    const int d = c->dim, dd = d * d;
+    const PBuf& b = c->buf[c->hH->cur];
+    const uint32_t Np = c->Np, blocks = (Np + 255) / 256;
+    auto get = [&](double* host, const double* src, int width, int kind) {
+      if (!host) return;
+      if (d == 3)
+        k_soa_to_aos<3><<<blocks, 256, 0, c->stream>>>(Np, src, b.id, c->staging, kind);
+      else
+        k_soa_to_aos<2><<<blocks, 256, 0, c->stream>>>(Np, src, b.id, c->staging, kind);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(host, c->staging, sizeof(double) * Np * width, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    };
+    get(x, b.x, d, 0);
+    get(v, b.v, d, 0);
+    get(F, b.F, dd, 1);
+    get(B, b.B, dd, 1);
+    get(scalars, b.sc, MTR_NUM_SCALARS, 2);
+    return MTR_OK;
+  });
+}
+
+int mtr_download_pic_flip(mtr_ctx* c, double* pic, double* flip) {
+  return guarded([&]() -> int {
+    if (!c || !c->uploaded) throw MtrError{MTR_ERR_STATE, "nothing uploaded"};
+    if (!c->hp.store_pic_flip) throw MtrError{MTR_ERR_STATE, "pic/flip are kept only after mtr_keep_pic_flip(ctx, 1)"};
+    CK(cudaSetDevice(c->device));
+    read_header(c);
+    const int d = c->dim;
+    const PBuf& b = c->buf[c->hH->cur];
+    const uint32_t Np = c->Np, blocks = (Np + 255) / 256;
+    for (int w = 0; w < 2; ++w) {
+      double* host = w == 0 ? pic : flip;
+      if (!host) continue;
+      const double* src = w == 0 ? c->pic : c->flip;
+      if (d == 3)
+        k_soa_to_aos<3><<<blocks, 256, 0, c->stream>>>(Np, src, b.id, c->staging, 0);
+      else
+        k_soa_to_aos<2><<<blocks, 256, 0, c->stream>>>(Np, src, b.id, c->staging, 0);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(host, c->staging, sizeof(double) * Np * d, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    }
+    return MTR_OK;
+  });
+}
+
+// Not in the header: switches the optional per-particle pic/flip output used
+// by the parity tests (off by default; it costs 2*dim stores per particle).
+int mtr_keep_pic_flip(mtr_ctx* c, int on) {
+  return guarded([&]() -> int {
+    if (!c) throw MtrError{MTR_ERR_INVALID, "null context"};
+    CK(cudaSetDevice(c->device));
+    c->hp.store_pic_flip = on ? 1 : 0;
+    upload_params(c);
+    CK(cudaStreamSynchronize(c->stream));
+    return MTR_OK;
+  });
+}
+
+int mtr_get_grid(mtr_ctx* c, uint32_t dims[3], double* gx, double* gy, double* gz, double* mass, double* v,
+                 double* flip) {
+  return guarded([&]() -> int {
+    if (!c || !c->uploaded || !dims) throw MtrError{MTR_ERR_STATE, "nothing uploaded"};
+    CK(cudaSetDevice(c->device));
+    read_header(c);
+    const StepHeader& H = *c->hH;
+    for (int a = 0; a < 3; ++a) dims[a] = H.N[a];
+    const int d = c->dim;
+    const uint32_t G = H.G;
+    if (G > c->cap_nodes) throw MtrError{MTR_ERR_STATE, "no completed step"};
+    if (gx) CK(cudaMemcpy(gx, c->gx, sizeof(double) * H.N[0], cudaMemcpyDeviceToHost));
+    if (gy) CK(cudaMemcpy(gy, c->gy, sizeof(double) * H.N[1], cudaMemcpyDeviceToHost));
+    if (gz && d == 3) CK(cudaMemcpy(gz, c->gz, sizeof(double) * H.N[2], cudaMemcpyDeviceToHost));
+    if (mass) CK(cudaMemcpy(mass, c->nmass, sizeof(double) * G, cudaMemcpyDeviceToHost));
+    std::vector<double> tmp((size_t)G);
+    for (int w = 0; w < 2; ++w) {
+      double* host = w == 0 ? v : flip;
+      if (!host) continue;
+      const double* src = w == 0 ? (c->prm.use_musl ? c->v2 : c->nv) : c->nflip;
+      for (int a = 0; a < d; ++a) {
+        CK(cudaMemcpy(tmp.data(), src + (size_t)a * c->cap_nodes, sizeof(double) * G, cudaMemcpyDeviceToHost));
+        for (uint32_t l = 0; l < G; ++l) host[(size_t)l * d + a] = tmp[l];
+      }
+    }
+    return MTR_OK;
+  });
+}
+
+int mtr_get_sort(mtr_ctx* c, uint32_t* keys_in_input_order, uint32_t* sorted_input_index, uint32_t* input_particle_id) {
+  return guarded([&]() -> int {
+    if (!c || !c->uploaded) throw MtrError{MTR_ERR_STATE, "nothing uploaded"};
+    CK(cudaSetDevice(c->device));
+    read_header(c);
+    const uint32_t Np = c->Np;
+    const uint32_t* perm = (c->passes & 1) ? c->valsB : c->valsA;
+    if (keys_in_input_order) CK(cudaMemcpy(keys_in_input_order, c->keys0, sizeof(uint32_t) * Np, cudaMemcpyDeviceToHost));
+    if (sorted_input_index) CK(cudaMemcpy(sorted_input_index, perm, sizeof(uint32_t) * Np, cudaMemcpyDeviceToHost));
+    if (input_particle_id)
+      CK(cudaMemcpy(input_particle_id, c->buf[1 - c->hH->cur].id, sizeof(uint32_t) * Np, cudaMemcpyDeviceToHost));
+    return MTR_OK;
+  });
+}
+
+int mtr_get_plates(mtr_ctx* c, mtr_plate* plates, int n_plates) {
+  return guarded([&]() -> int {
+    if (!c) throw MtrError{MTR_ERR_INVALID, "null context"};
+    CK(cudaSetDevice(c->device));
+    read_header(c);
+    for (int i = 0; i < n_plates && i < (int)c->plates.size(); ++i) plates[i] = c->hH->plates[i];
+    return MTR_OK;
+  });
+}
+
+int mtr_get_clock(mtr_ctx* c, mtr_clock* ck) {
+  return guarded([&]() -> int {
+    if (!c || !ck) throw MtrError{MTR_ERR_INVALID, "null argument"};
+    CK(cudaSetDevice(c->device));
+    read_header(c);
+    ck->time = c->hH->time;
+    ck->dt = c->hH->dt;
+    ck->step = c->hH->step;
+    ck->frame = c->hH->frame;
+    ck->done = c->hH->done;
+    ck->reserved = 0;
+    return MTR_OK;
+  });
+}
+
+int mtr_status(mtr_ctx* c, uint32_t* flags, uint32_t* first_bad) {
+  return guarded([&]() -> int {
+    if (!c) throw MtrError{MTR_ERR_INVALID, "null context"};
+    CK(cudaSetDevice(c->device));
+    read_header(c);
+    if (flags) *flags = c->hH->status;
+    if (first_bad) *first_bad = c->hH->first_bad;
+    return MTR_OK;
+  });
+}
+
+int mtr_clear_status(mtr_ctx* c) {
+  return guarded([&]() -> int {
+    if (!c) throw MtrError{MTR_ERR_INVALID, "null context"};
+    CK(cudaSetDevice(c->device));
+    read_header(c);
+    c->hH->status = 0;
+    c->hH->first_bad = 0xffffffffu;
+    write_header(c);
+    CK(cudaStreamSynchronize(c->stream));
+    return MTR_OK;
+  });
+}
+
+int mtr_sync(mtr_ctx* c, double timeout_seconds) {
+  return guarded([&]() -> int {
+    if (!c) throw MtrError{MTR_ERR_INVALID, "null context"};
+    CK(cudaSetDevice(c->device));
+    cudaEvent_t ev;
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev, c->stream));
+    auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+      cudaError_t e = cudaEventQuery(ev);
+      if (e == cudaSuccess) break;
+      if (e != cudaErrorNotReady) {
+        cudaEventDestroy(ev);
+        throw MtrError{MTR_ERR_CUDA, cudaGetErrorString(e)};
+      }
+      double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      if (el > timeout_seconds) {
+        cudaEventDestroy(ev);
+        throw MtrError{MTR_ERR_TIMEOUT, "device did not finish within the timeout"};
+      }
+      std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+    cudaEventDestroy(ev);
+    return MTR_OK;
+  });
+}
+
+void* mtr_stream(mtr_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int64_t mtr_launch_count(mtr_ctx* c) { return c ? c->launches_last : 0; }
+
+// Not in the header: graph replay on/off (on by default) for timing studies.
+int mtr_use_graphs(mtr_ctx* c, int on) {
+  if (!c) return MTR_ERR_INVALID;
+  c->use_graphs = on != 0;
+  cudaSetDevice(c->device);
+  free_graphs(c);
+  return MTR_OK;
+}
+
+void mtr_ctx_destroy(mtr_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_graphs(c);
+  free_grid(c);
+  for (void* p : c->pallocs) dfree(p);
+  for (void* p : {(void*)c->keys0, (void*)c->keysA, (void*)c->valsA, (void*)c->keysB, (void*)c->valsB,
+                  (void*)c->hist, (void*)c->dtot, (void*)c->partials, (void*)c->staging, (void*)c->dP, (void*)c->dH})
+    dfree(p);
+  if (c->hH) cudaFreeHost(c->hH);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+}  // extern "C"

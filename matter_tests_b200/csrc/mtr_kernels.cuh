@@ -1,0 +1,1142 @@
+// mtr_kernels.cuh — the sm_100a kernels of one explicit MPM step
+// (Simulation::advanceStep, simulation.cpp:219-273), FP64.
+//
+// Step pipeline (all on one stream, no host round trip, CUDA-graph capturable):
+//   k_bbox        per-block min/max x and max |v|^2          update_dt.cpp, remesh.cpp
+//   k_header      dt, gravity ramp, remesh + arange axes      update_dt.cpp:5-66, remesh.cpp:38-311
+//   k_sort_*      stable LSD radix sort by blocked cell key   (new: locality for P2G)
+//   k_tile_ranges particle range of every 4^3 (2D: 8^2) tile
+//   k_p2g         tile block -> shared grid patch -> one global atomic per node and channel
+//                 (mass, momentum with APIC, force tau.grad w, MIBF friction)
+//                                                              p2g.cpp:6-100, explicit_euler_update.cpp:15-77
+//   k_grid        normalise, v += -dt V0 f/m + dt g, boundary collision, flip
+//                                                              p2g.cpp:84-98, explicit_euler_update.cpp:83-132
+//   USL:  k_g2p   gather pic/B/flip/grad v, F update, return mapping, tau, x/v update, coalesced stores
+//                                                              g2p.cpp, deformation_update.cpp, plasticity.cpp,
+//                                                              position_update.cpp
+//   MUSL: k_g2p_musl (gather + v blend + re-scatter), k_musl_norm, k_defgrad
+//                                                              musl.cpp:6-96
+//   k_tail        plate motion, clock, frame and end test     object_plate.hpp:136-162, simulation.cpp:176-200
+//
+// Particle state is SoA, one array per component (x + a*Np), double buffered:
+// the step reads the `in` set through the sort permutation and writes the
+// `out` set in sorted order, so the particle order follows the cell order and
+// every later read of the same data is nearly coalesced.
+#pragma once
+#include "mtr_boundary.cuh"
+#include "mtr_device.cuh"
+#include "mtr_plasticity.cuh"
+
+namespace mtr {
+
+struct PBuf {
+  double* x;     // [D][Np]
+  double* v;     // [D][Np]
+  double* F;     // [D*D][Np], entry (r,c) at (r*D + c)
+  double* B;     // [D*D][Np]
+  double* sc;    // [6][Np] MTR_SCALAR_* order
+  double* tau;   // [Sym<D>::n][Np]
+  uint32_t* id;  // original particle index
+};
+
+struct StepArgs {
+  const DevParams* P;
+  StepHeader* H;
+  BBoxPartial* partials;
+  int npartials;
+  uint32_t Np;
+  double *gx, *gy, *gz;
+  uint32_t cap_axis[3];
+  uint32_t cap_nodes;
+  uint32_t cap_tiles;
+  double* acc;    // [NCH][cap_nodes] P2G accumulators: mass, mom[D], force[D], friction
+  double* nv;     // [D][cap_nodes]  node velocity after the update (MUSL: after re-projection)
+  double* nflip;  // [D][cap_nodes]
+  double* nmass;  // [cap_nodes]
+  double* nfric;  // [cap_nodes]
+  double* v2;     // [D][cap_nodes]  MUSL re-projection accumulator
+  uint32_t* keys0;  // cell key of each particle in input order
+  uint32_t *keysA, *valsA, *keysB, *valsB;
+  uint32_t* hist;   // [256][sort_blocks]
+  uint32_t* dtot;   // [256]
+  int sort_blocks;
+  uint32_t* tile_begin;
+  uint32_t* tile_end;
+  PBuf in, out;
+  double* pic;   // optional [D][Np] in output order
+  double* flip;  // optional [D][Np]
+};
+
+constexpr uint32_t kMaxAxisNodes = 1u << 22;
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 8;
+constexpr int kSortTile = kSortThreads * kSortItems;
+
+template <int D>
+struct Tiling {
+  static constexpr int TB = D == 3 ? 4 : 8;     // cells per tile edge
+  static constexpr int SH = D == 3 ? 2 : 3;     // log2(TB)
+  static constexpr int PN = TB + 3;             // patch nodes per edge (stencil -1..+2)
+  static constexpr int NODES = D == 3 ? PN * PN * PN : PN * PN;
+  static constexpr int NCH = 2 + 2 * D;         // mass, mom[D], force[D], friction
+};
+
+__device__ __forceinline__ bool step_inactive(const StepHeader* H) { return H->done || H->abort; }
+
+__device__ __forceinline__ uint32_t node_index(const StepHeader* H, int i, int j, int k) {
+  return ((uint32_t)i * H->N[1] + (uint32_t)j) * H->N[2] + (uint32_t)k;
+}
+
+// ---------------------------------------------------------------------------
+// 1. bbox / vmax partials
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(256) k_bbox(StepArgs A) {
+  if (step_inactive(A.H)) return;
+  double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300}, v2 = 0.0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < A.Np; i += gridDim.x * blockDim.x) {
+    double vv[3];
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      double xa = A.in.x[(size_t)a * A.Np + i];
+      mn[a] = fmin(mn[a], xa);
+      mx[a] = fmax(mx[a], xa);
+      vv[a] = A.in.v[(size_t)a * A.Np + i];
+    }
+    double s = __dadd_rn(__dmul_rn(vv[0], vv[0]), __dmul_rn(vv[1], vv[1]));
+    if constexpr (D == 3) s = __dadd_rn(s, __dmul_rn(vv[2], vv[2]));
+    v2 = fmax(v2, s);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      mn[a] = fmin(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], off));
+      mx[a] = fmax(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], off));
+    }
+    v2 = fmax(v2, __shfl_xor_sync(0xffffffffu, v2, off));
+  }
+  __shared__ BBoxPartial wp[8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      wp[warp].mn[a] = mn[a];
+      wp[warp].mx[a] = mx[a];
+    }
+    wp[warp].v2 = v2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    BBoxPartial r = wp[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        r.mn[a] = fmin(r.mn[a], wp[w].mn[a]);
+        r.mx[a] = fmax(r.mx[a], wp[w].mx[a]);
+      }
+      r.v2 = fmax(r.v2, wp[w].v2);
+    }
+    A.partials[blockIdx.x] = r;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2. step header: dt (update_dt.cpp:5-66) and grid (remesh.cpp:38-311)
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(32) k_header(StepArgs A) {
+  StepHeader* H = A.H;
+  const DevParams& P = *A.P;
+  if (step_inactive(H)) return;
+  const int lane = threadIdx.x;
+  double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300}, v2 = 0.0;
+  for (int b = lane; b < A.npartials; b += 32) {
+    const BBoxPartial& q = A.partials[b];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      mn[a] = fmin(mn[a], q.mn[a]);
+      mx[a] = fmax(mx[a], q.mx[a]);
+    }
+    v2 = fmax(v2, q.v2);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      mn[a] = fmin(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], off));
+      mx[a] = fmax(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], off));
+    }
+    v2 = fmax(v2, __shfl_xor_sync(0xffffffffu, v2, off));
+  }
+  __shared__ double s_low[3], s_high[3];
+  __shared__ int s_ok;
+  if (lane == 0) {
+    // updateDt
+    const double max_speed = sqrt(v2);
+    double dt;
+    if (fabs(max_speed) > 1e-10) {
+      double dt_cfl = P.cfl * P.dx / max_speed;
+      dt = dmin(dt_cfl, P.dt_max);
+    } else {
+      dt = P.dt_max;
+    }
+    dt = dmin(dt, __dsub_rn(__dmul_rn(P.frame_dt, (double)(H->frame + 1)), H->time));
+    dt = dmin(dt, __dsub_rn(P.final_time, H->time));
+    H->dt = dt;
+    if (P.gravity_special) {
+#pragma unroll
+      for (int a = 0; a < D; ++a)
+        H->gravity[a] = (H->time < P.gravity_time) ? P.gravity_final[a] * H->time / P.gravity_time : P.gravity_final[a];
+    }
+    // remesh
+    const double dx = P.dx;
+    if (H->step == 0) {  // remeshFixedInit(2,2,2)
+      if (P.grid_ref[0] < 1e10) {
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+          if (P.grid_ref[a] < mn[a])
+            mn[a] = P.grid_ref[a];
+          else if (P.grid_ref[a] > mx[a])
+            mx[a] = P.grid_ref[a];
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        H->max_init[a] = mx[a];
+        H->min_init[a] = mn[a];
+        H->low_init[a] = __dsub_rn(mn[a], __dmul_rn(dx, 2.0));
+        H->high_init[a] = __dadd_rn(mx[a], __dmul_rn(dx, 2.0));
+        s_low[a] = H->low_init[a];
+        s_high[a] = H->high_init[a];
+      }
+    } else {  // remeshFixedCont
+      // explicit roundings: each product and difference is rounded on its own,
+      // as in the host code this restates (no fused multiply-add)
+      const double tiny = __dmul_rn(1e-8, dx);
+      for (int a = 0; a < D; ++a) {
+        double hi, lo;
+        if (mx[a] < H->max_init[a]) {
+          unsigned int f = (unsigned int)floor(dmax(0.0, __dsub_rn(__ddiv_rn(__dsub_rn(H->max_init[a], mx[a]), dx), tiny)));
+          hi = __dsub_rn(H->high_init[a], __dmul_rn((double)f, dx));
+        } else {
+          unsigned int f = (unsigned int)floor(dmax(0.0, __dsub_rn(__ddiv_rn(__dsub_rn(mx[a], H->max_init[a]), dx), tiny)));
+          hi = __dadd_rn(H->high_init[a], __dmul_rn((double)f, dx));
+        }
+        if (mn[a] > H->min_init[a]) {
+          unsigned int f = (unsigned int)floor(dmax(0.0, __dsub_rn(__ddiv_rn(__dsub_rn(mn[a], H->min_init[a]), dx), tiny)));
+          lo = __dadd_rn(H->low_init[a], __dmul_rn((double)f, dx));
+        } else {
+          unsigned int f = (unsigned int)floor(dmax(0.0, __dsub_rn(__ddiv_rn(__dsub_rn(H->min_init[a], mn[a]), dx), tiny)));
+          lo = __dsub_rn(H->low_init[a], __dmul_rn((double)f, dx));
+        }
+        s_low[a] = lo;
+        s_high[a] = hi;
+      }
+    }
+    s_ok = 1;
+  }
+  __syncwarp();
+  // arange (tools.hpp:291-296): one lane per axis accumulates value += step
+  if (lane < D) {
+    const double dx = P.dx;
+    double* ax = lane == 0 ? A.gx : (lane == 1 ? A.gy : A.gz);
+    const uint32_t cap = A.cap_axis[lane];
+    const double stop = __dadd_rn(s_high[lane], dx);
+    uint32_t n = 0;
+    // counted exactly up to kMaxAxisNodes so the host can size the regrowth in
+    // one go; the bound also ends the loop for non-finite extents
+    for (double value = s_low[lane]; value < stop && n < kMaxAxisNodes; value = __dadd_rn(value, dx)) {
+      if (n < cap) ax[n] = value;
+      ++n;
+    }
+    H->N[lane] = n;
+    H->org[lane] = s_low[lane];
+    if (n > cap || n < 4 || n >= kMaxAxisNodes) atomicExch(&s_ok, 0);
+  }
+  __syncwarp();
+  if (lane == 0) {
+    if (D == 2) {
+      H->N[2] = 1;
+      H->org[2] = 0.0;
+    }
+    constexpr int TB = Tiling<D>::TB;
+    uint64_t G = (uint64_t)H->N[0] * H->N[1] * H->N[2];
+    H->T[0] = (H->N[0] + TB - 1) / TB;
+    H->T[1] = (H->N[1] + TB - 1) / TB;
+    H->T[2] = D == 3 ? (H->N[2] + TB - 1) / TB : 1;
+    uint64_t nt = (uint64_t)H->T[0] * H->T[1] * H->T[2];
+    if (!s_ok || G > A.cap_nodes || nt > A.cap_tiles) {
+      H->abort = 1;
+      atomicOr(&H->status, MTR_STATUS_GRID_OVERFLOW);
+    }
+    H->G = (uint32_t)G;
+    H->ntiles = (uint32_t)nt;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 3. stable LSD radix sort of (blocked cell key, input position)
+// ---------------------------------------------------------------------------
+template <int D>
+__device__ __forceinline__ uint32_t cell_key(const StepHeader* H, double ioh, const double (&x)[3]) {
+  constexpr int SH = Tiling<D>::SH, TB = Tiling<D>::TB;
+  int c[3] = {0, 0, 0};
+#pragma unroll
+  for (int a = 0; a < D; ++a) c[a] = (int)floor((x[a] - H->org[a]) * ioh);
+  uint32_t t, in;
+  if constexpr (D == 3) {
+    t = ((uint32_t)(c[0] >> SH) * H->T[1] + (uint32_t)(c[1] >> SH)) * H->T[2] + (uint32_t)(c[2] >> SH);
+    in = ((uint32_t)(c[0] & (TB - 1)) * TB + (uint32_t)(c[1] & (TB - 1))) * TB + (uint32_t)(c[2] & (TB - 1));
+  } else {
+    t = (uint32_t)(c[0] >> SH) * H->T[1] + (uint32_t)(c[1] >> SH);
+    in = (uint32_t)(c[0] & (TB - 1)) * TB + (uint32_t)(c[1] & (TB - 1));
+  }
+  return t * 64u + in;
+}
+
+// Per-block digit histogram.  The first pass computes the keys from x.
+template <int D, bool FIRST>
+__global__ void __launch_bounds__(kSortThreads) k_sort_hist(StepArgs A, const uint32_t* __restrict__ keys, int shift) {
+  if (step_inactive(A.H)) return;
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const uint32_t base = blockIdx.x * kSortTile;
+  const double ioh = A.P->one_over_dx;
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    uint32_t i = base + r * kSortThreads + threadIdx.x;
+    if (i < A.Np) {
+      uint32_t k;
+      if (FIRST) {
+        double x[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int a = 0; a < D; ++a) x[a] = A.in.x[(size_t)a * A.Np + i];
+        k = cell_key<D>(A.H, ioh, x);
+        A.keys0[i] = k;
+      } else {
+        k = keys[i];
+      }
+      atomicAdd(&h[(k >> shift) & 255u], 1u);
+    }
+  }
+  __syncthreads();
+  A.hist[threadIdx.x * A.sort_blocks + blockIdx.x] = h[threadIdx.x];
+}
+
+// Exclusive scan of each digit's row over the blocks; row totals to dtot.
+__global__ void __launch_bounds__(256) k_sort_scan(StepArgs A) {
+  if (step_inactive(A.H)) return;
+  const int dgt = blockIdx.x;
+  uint32_t* row = A.hist + (size_t)dgt * A.sort_blocks;
+  __shared__ uint32_t ws[8];
+  __shared__ uint32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int b0 = 0; b0 < A.sort_blocks; b0 += 256) {
+    int b = b0 + threadIdx.x;
+    uint32_t v = b < A.sort_blocks ? row[b] : 0u;
+    uint32_t incl = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      uint32_t t = __shfl_up_sync(0xffffffffu, incl, off);
+      if ((threadIdx.x & 31) >= off) incl += t;
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 31) ws[warp] = incl;
+    __syncthreads();
+    uint32_t wpre = 0;
+    for (int w = 0; w < warp; ++w) wpre += ws[w];
+    uint32_t total = 0;
+    for (int w = 0; w < 8; ++w) total += ws[w];
+    if (b < A.sort_blocks) row[b] = carry + wpre + incl - v;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) A.dtot[dgt] = carry;
+}
+
+// Stable scatter.  Elements are ranked round by round (256 at a time, in
+// index order) with warp match + per-warp digit counts, which keeps equal
+// digits in input order.
+__global__ void __launch_bounds__(kSortThreads) k_sort_scatter(StepArgs A, const uint32_t* __restrict__ ksrc,
+                                                               const uint32_t* __restrict__ vsrc, uint32_t* kdst,
+                                                               uint32_t* vdst, int shift) {
+  if (step_inactive(A.H)) return;
+  __shared__ uint32_t goff[256];
+  __shared__ uint32_t run[256];
+  __shared__ uint32_t wcnt[kSortThreads / 32][256];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  {  // digit base = exclusive prefix of digit totals, plus this block's row offset
+    uint32_t v = A.dtot[tid];
+    uint32_t incl = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      uint32_t t = __shfl_up_sync(0xffffffffu, incl, off);
+      if (lane >= off) incl += t;
+    }
+    __shared__ uint32_t ws[8];
+    if (lane == 31) ws[warp] = incl;
+    __syncthreads();
+    uint32_t wpre = 0;
+    for (int w = 0; w < warp; ++w) wpre += ws[w];
+    goff[tid] = wpre + incl - v + A.hist[(size_t)tid * A.sort_blocks + blockIdx.x];
+    run[tid] = 0;
+  }
+  const uint32_t base = blockIdx.x * kSortTile;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  for (int r = 0; r < kSortItems; ++r) {
+#pragma unroll
+    for (int w = 0; w < kSortThreads / 32; ++w) wcnt[w][tid] = 0;
+    __syncthreads();
+    const uint32_t i = base + r * kSortThreads + tid;
+    const bool valid = i < A.Np;
+    uint32_t k = 0, val = 0, dgt = 256;
+    if (valid) {
+      k = ksrc[i];
+      val = vsrc ? vsrc[i] : i;
+      dgt = (k >> shift) & 255u;
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, dgt);
+    const uint32_t rank = __popc(peers & lt_mask);
+    if (valid && rank == 0) wcnt[warp][dgt] = __popc(peers);
+    __syncthreads();
+    {  // exclusive prefix over warps per digit, on top of earlier rounds
+      uint32_t acc = run[tid];
+#pragma unroll
+      for (int w = 0; w < kSortThreads / 32; ++w) {
+        uint32_t c = wcnt[w][tid];
+        wcnt[w][tid] = acc;
+        acc += c;
+      }
+      run[tid] = acc;
+    }
+    __syncthreads();
+    if (valid) {
+      const uint32_t pos = goff[dgt] + wcnt[warp][dgt] + rank;
+      kdst[pos] = k;
+      vdst[pos] = val;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 4. tile ranges over the sorted keys
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_tile_ranges(StepArgs A, const uint32_t* __restrict__ skeys) {
+  if (step_inactive(A.H)) return;
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < A.Np; s += gridDim.x * blockDim.x) {
+    const uint32_t t = skeys[s] >> 6;
+    if (t >= A.cap_tiles) continue;
+    if (s == 0 || (skeys[s - 1] >> 6) != t) A.tile_begin[t] = s;
+    if (s == A.Np - 1 || (skeys[s + 1] >> 6) != t) A.tile_end[t] = s + 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// stencil weights of one particle along one axis
+// ---------------------------------------------------------------------------
+template <int DEG>
+__device__ __forceinline__ void axis_weights(double xp, const double* coords, double ioh, double (&w)[4],
+                                             double (&dw)[4]) {
+#pragma unroll
+  for (int o = 0; o < 4; ++o) {
+    const double u = (xp - coords[o]) * ioh;
+    w[o] = bspline_N<DEG>(u);
+    dw[o] = bspline_dN<DEG>(u);
+  }
+}
+
+template <int D>
+__device__ __forceinline__ void tile_coords(const StepHeader* H, uint32_t t, int (&tc)[3]) {
+  if constexpr (D == 3) {
+    tc[2] = (int)(t % H->T[2]);
+    uint32_t r = t / H->T[2];
+    tc[1] = (int)(r % H->T[1]);
+    tc[0] = (int)(r / H->T[1]);
+  } else {
+    tc[2] = 0;
+    tc[1] = (int)(t % H->T[1]);
+    tc[0] = (int)(t / H->T[1]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 5. P2G + stress force, one block per tile
+// ---------------------------------------------------------------------------
+template <int D, int DEG>
+__global__ void __launch_bounds__(128) k_p2g(StepArgs A, const uint32_t* __restrict__ perm) {
+  using TL = Tiling<D>;
+  constexpr int PN = TL::PN, NODES = TL::NODES, NCH = TL::NCH, TB = TL::TB;
+  const StepHeader* H = A.H;
+  if (step_inactive(H)) return;
+  const uint32_t t = blockIdx.x;
+  if (t >= H->ntiles) return;
+  const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
+  if (pb >= pe) return;
+  const DevParams& P = *A.P;
+  __shared__ double patch[NCH][NODES];
+  __shared__ double crd[3][PN];
+  int tc[3];
+  tile_coords<D>(H, t, tc);
+  int n0[3] = {tc[0] * TB - 1, tc[1] * TB - 1, D == 3 ? tc[2] * TB - 1 : 0};
+  for (int i = threadIdx.x; i < NCH * NODES; i += blockDim.x) (&patch[0][0])[i] = 0.0;
+  for (int i = threadIdx.x; i < D * PN; i += blockDim.x) {
+    const int a = i / PN, o = i % PN;
+    const int g = n0[a] + o;
+    const double* ax = a == 0 ? A.gx : (a == 1 ? A.gy : A.gz);
+    crd[a][o] = (g >= 0 && g < (int)H->N[a]) ? ax[g] : 0.0;
+  }
+  __syncthreads();
+  const uint32_t Np = A.Np;
+  const double ioh = P.one_over_dx;
+  const bool apic = P.flip_ratio < 0;
+  const bool mibf = P.use_mibf;
+  for (uint32_t s = pb + threadIdx.x; s < pe; s += blockDim.x) {
+    const uint32_t j = perm[s];
+    double xp[3] = {0, 0, 0}, vp[3] = {0, 0, 0}, tau[Sym<D>::n];
+    double Bm[D][D];
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      xp[a] = A.in.x[(size_t)a * Np + j];
+      vp[a] = A.in.v[(size_t)a * Np + j];
+    }
+    if (apic) {
+#pragma unroll
+      for (int r = 0; r < D; ++r)
+#pragma unroll
+        for (int c = 0; c < D; ++c) Bm[r][c] = A.in.B[(size_t)(r * D + c) * Np + j];
+    }
+#pragma unroll
+    for (int q = 0; q < Sym<D>::n; ++q) tau[q] = A.in.tau[(size_t)q * Np + j];
+    const double mui = mibf ? A.in.sc[(size_t)MTR_SCALAR_MUI * Np + j] : 0.0;
+    int lb[3] = {0, 0, 0};
+    bool oob = false;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      int b = (int)floor((xp[a] - H->org[a]) * ioh) - 1;
+      b = b < 0 ? 0 : b;  // p2g.cpp:21-24 clamps at zero
+      lb[a] = b - n0[a];
+      if (lb[a] < 0 || lb[a] > PN - 4 || b + 3 >= (int)H->N[a]) oob = true;
+    }
+    if (oob) {
+      raise_status(A.H, MTR_STATUS_STENCIL_OOB, A.in.id[j]);
+      continue;
+    }
+    double w[3][4], dw[3][4];
+#pragma unroll
+    for (int a = 0; a < D; ++a) axis_weights<DEG>(xp[a], &crd[a][lb[a]], ioh, w[a], dw[a]);
+    constexpr int KN = D == 3 ? 4 : 1;
+#pragma unroll
+    for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+        for (int kk = 0; kk < KN; ++kk) {
+          double wxy = w[0][ii] * w[1][jj];
+          const double weight = D == 3 ? wxy * w[2][kk] : wxy;
+          const int node = D == 3 ? ((lb[0] + ii) * PN + (lb[1] + jj)) * PN + (lb[2] + kk)
+                                  : (lb[0] + ii) * PN + (lb[1] + jj);
+          if (weight > 1e-25) {
+            atomicAdd(&patch[0][node], weight);
+            double pd[3] = {crd[0][lb[0] + ii] - xp[0], crd[1][lb[1] + jj] - xp[1],
+                            D == 3 ? crd[2][lb[2] + kk] - xp[2] : 0.0};
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+              double m = vp[a] * weight;
+              if (apic) {
+                double bv = Bm[a][0] * pd[0];
+#pragma unroll
+                for (int c = 1; c < D; ++c) bv += Bm[a][c] * pd[c];
+                m += bv * P.apicDinverse * weight;
+              }
+              atomicAdd(&patch[1 + a][node], m);
+            }
+            if (mibf) atomicAdd(&patch[1 + 2 * D][node], mui * weight);
+          }
+          double g[3];
+          if constexpr (D == 3) {
+            g[0] = dw[0][ii] * w[1][jj] * w[2][kk] * ioh;
+            g[1] = dw[1][jj] * w[0][ii] * w[2][kk] * ioh;
+            g[2] = dw[2][kk] * w[0][ii] * w[1][jj] * ioh;
+          } else {
+            g[0] = dw[0][ii] * w[1][jj] * ioh;
+            g[1] = dw[1][jj] * w[0][ii] * ioh;
+          }
+#pragma unroll
+          for (int a = 0; a < D; ++a) {
+            double f = sym_at<D>(tau, a, 0) * g[0];
+#pragma unroll
+            for (int c = 1; c < D; ++c) f += sym_at<D>(tau, a, c) * g[c];
+            if (f != 0.0) atomicAdd(&patch[1 + D + a][node], f);
+          }
+        }
+  }
+  __syncthreads();
+  const uint32_t cap = A.cap_nodes;
+  for (int n = threadIdx.x; n < NODES; n += blockDim.x) {
+    int li, lj, lk;
+    if constexpr (D == 3) {
+      lk = n % PN;
+      lj = (n / PN) % PN;
+      li = n / (PN * PN);
+    } else {
+      lk = 0;
+      lj = n % PN;
+      li = n / PN;
+    }
+    const int gi = n0[0] + li, gj = n0[1] + lj, gk = n0[2] + lk;
+    if (gi < 0 || gj < 0 || gk < 0 || gi >= (int)H->N[0] || gj >= (int)H->N[1] || gk >= (int)H->N[2]) continue;
+    const uint32_t l = node_index(H, gi, gj, gk);
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) {
+      const double val = patch[ch][n];
+      if (val != 0.0) atomicAdd(&A.acc[(size_t)ch * cap + l], val);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 6. grid update, one thread per node
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(256) k_grid(StepArgs A) {
+  StepHeader* H = A.H;
+  if (step_inactive(H)) return;
+  const DevParams& P = *A.P;
+  const uint32_t G = H->G, cap = A.cap_nodes;
+  const double dt = H->dt;
+  const double dtpv = dt * P.particle_volume;
+  double dtg[3];
+#pragma unroll
+  for (int a = 0; a < D; ++a) dtg[a] = dt * H->gravity[a];
+  __shared__ mtr_plate plates[MTR_MAXP];
+  for (int i = threadIdx.x; i < P.nplates; i += blockDim.x) plates[i] = H->plates[i];
+  __syncthreads();
+  constexpr int NCH = Tiling<D>::NCH;
+  for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < G; l += gridDim.x * blockDim.x) {
+    const double mraw = A.acc[l];
+    double v[3] = {0, 0, 0}, vold[3] = {0, 0, 0};
+    double fric = 0.0;
+    if (mraw > 0) {
+#pragma unroll
+      for (int a = 0; a < D; ++a) v[a] = A.acc[(size_t)(1 + a) * cap + l] / mraw;
+    }
+    if (P.use_mibf) fric = A.acc[(size_t)(1 + 2 * D) * cap + l] / mraw;
+    const double mi = mraw * P.particle_mass;
+    double fl[3] = {0, 0, 0};
+    if (mi > 0) {
+      uint32_t k = D == 3 ? l % H->N[2] : 0;
+      uint32_t r = D == 3 ? l / H->N[2] : l;
+      uint32_t jj = r % H->N[1], i = r / H->N[1];
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        double inc = -dtpv * A.acc[(size_t)(1 + D + a) * cap + l] / mi + dtg[a];
+        vold[a] = v[a];
+        v[a] = vold[a] + inc;
+      }
+      double Xi[3] = {A.gx[i], A.gy[jj], D == 3 ? A.gz[k] : 0.0};
+      if (!boundary_collision<D>(P, plates, fric, Xi, dt, v)) raise_status(H, MTR_STATUS_BAD_BC, 0xffffffffu);
+#pragma unroll
+      for (int a = 0; a < D; ++a) fl[a] = v[a] - vold[a];
+    }
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      A.nv[(size_t)a * cap + l] = v[a];
+      A.nflip[(size_t)a * cap + l] = fl[a];
+    }
+    A.nmass[l] = mi;
+    if (P.use_mibf) A.nfric[l] = fric;
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) A.acc[(size_t)ch * cap + l] = 0.0;  // ready for the next step
+  }
+}
+
+// ---------------------------------------------------------------------------
+// particle I/O helpers
+// ---------------------------------------------------------------------------
+template <int D>
+struct PLoad {
+  double x[3], v[3], F[D][D];
+  PScalars s;
+  uint32_t id;
+};
+
+template <int D>
+__device__ __forceinline__ void load_particle(const PBuf& b, uint32_t Np, uint32_t j, PLoad<D>& p) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) p.x[a] = p.v[a] = 0.0;
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    p.x[a] = b.x[(size_t)a * Np + j];
+    p.v[a] = b.v[(size_t)a * Np + j];
+  }
+#pragma unroll
+  for (int r = 0; r < D; ++r)
+#pragma unroll
+    for (int c = 0; c < D; ++c) p.F[r][c] = b.F[(size_t)(r * D + c) * Np + j];
+  p.s.eps_pl_dev = b.sc[(size_t)MTR_SCALAR_EPS_PL_DEV * Np + j];
+  p.s.eps_pl_vol = b.sc[(size_t)MTR_SCALAR_EPS_PL_VOL * Np + j];
+  p.s.eps_pl_vol_pradhana = b.sc[(size_t)MTR_SCALAR_EPS_PL_VOL_PRADHANA * Np + j];
+  p.s.delta_gamma = 0.0;  // deformation_update.cpp:13 zeroes it every step
+  p.s.viscosity = b.sc[(size_t)MTR_SCALAR_VISCOSITY * Np + j];
+  p.s.muI = b.sc[(size_t)MTR_SCALAR_MUI * Np + j];
+  p.id = b.id[j];
+}
+
+template <int D>
+__device__ __forceinline__ void store_defgrad(const PBuf& b, uint32_t Np, uint32_t s, const double (&F)[D][D],
+                                              const PScalars& sc, const double* tau) {
+#pragma unroll
+  for (int r = 0; r < D; ++r)
+#pragma unroll
+    for (int c = 0; c < D; ++c) b.F[(size_t)(r * D + c) * Np + s] = F[r][c];
+  b.sc[(size_t)MTR_SCALAR_EPS_PL_DEV * Np + s] = sc.eps_pl_dev;
+  b.sc[(size_t)MTR_SCALAR_EPS_PL_VOL * Np + s] = sc.eps_pl_vol;
+  b.sc[(size_t)MTR_SCALAR_EPS_PL_VOL_PRADHANA * Np + s] = sc.eps_pl_vol_pradhana;
+  b.sc[(size_t)MTR_SCALAR_DELTA_GAMMA * Np + s] = sc.delta_gamma;
+  b.sc[(size_t)MTR_SCALAR_VISCOSITY * Np + s] = sc.viscosity;
+  b.sc[(size_t)MTR_SCALAR_MUI * Np + s] = sc.muI;
+#pragma unroll
+  for (int q = 0; q < Sym<D>::n; ++q) b.tau[(size_t)q * Np + s] = tau[q];
+}
+
+// velocity blend of position_update.cpp:14-24 / musl.cpp:15-22
+__device__ __forceinline__ double blend_v(double fr, double v, double fl, double pic) {
+  if (fr < -1) return pic;
+  if (fr < 0) return (-fr) * (v + fl) + (1 - (-fr)) * pic;
+  return fr * (v + fl) + (1 - fr) * pic;
+}
+
+// Gathers pic, B, flip and grad v from the node arrays (g2p.cpp:24-77,
+// deformation_update.cpp:17-40).  The stencil base is not clamped (g2p.cpp:29).
+template <int D, int DEG, bool WANT_GRADV>
+__device__ __forceinline__ bool gather(const StepArgs& A, const StepHeader* H, const double* __restrict__ nv,
+                                       const double (&xp)[3], double (&pic)[3], double (&Bp)[D][D], double (&flp)[3],
+                                       double (&gv)[D][D], bool want_b, bool want_flip) {
+  const double ioh = A.P->one_over_dx;
+  const uint32_t cap = A.cap_nodes;
+  int base[3] = {0, 0, 0};
+  double w[3][4], dw[3][4], crd[3][4];
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    base[a] = (int)(floor((xp[a] - H->org[a]) * ioh) - 1);
+    if (base[a] < 0 || base[a] + 3 >= (int)H->N[a]) return false;
+    const double* ax = a == 0 ? A.gx : (a == 1 ? A.gy : A.gz);
+#pragma unroll
+    for (int o = 0; o < 4; ++o) crd[a][o] = ax[base[a] + o];
+    axis_weights<DEG>(xp[a], crd[a], ioh, w[a], dw[a]);
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) pic[a] = flp[a] = 0.0;
+#pragma unroll
+  for (int r = 0; r < D; ++r)
+#pragma unroll
+    for (int c = 0; c < D; ++c) Bp[r][c] = gv[r][c] = 0.0;
+  constexpr int KN = D == 3 ? 4 : 1;
+#pragma unroll
+  for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+      for (int kk = 0; kk < KN; ++kk) {
+        const uint32_t l = D == 3 ? node_index(H, base[0] + ii, base[1] + jj, base[2] + kk)
+                                  : node_index(H, base[0] + ii, base[1] + jj, 0);
+        const double wxy = w[0][ii] * w[1][jj];
+        const double weight = D == 3 ? wxy * w[2][kk] : wxy;
+        double vi[3] = {0, 0, 0};
+#pragma unroll
+        for (int a = 0; a < D; ++a) vi[a] = __ldg(&nv[(size_t)a * cap + l]);
+#pragma unroll
+        for (int a = 0; a < D; ++a) pic[a] += vi[a] * weight;
+        if (want_b) {
+          double pd[3] = {crd[0][ii] - xp[0], crd[1][jj] - xp[1], D == 3 ? crd[2][kk] - xp[2] : 0.0};
+#pragma unroll
+          for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) Bp[r][c] += vi[r] * pd[c] * weight;
+        }
+        if (want_flip) {
+#pragma unroll
+          for (int a = 0; a < D; ++a) flp[a] += __ldg(&A.nflip[(size_t)a * cap + l]) * weight;
+        }
+        if (WANT_GRADV) {
+          double g[3];
+          if constexpr (D == 3) {
+            g[0] = dw[0][ii] * w[1][jj] * w[2][kk] * ioh;
+            g[1] = dw[1][jj] * w[0][ii] * w[2][kk] * ioh;
+            g[2] = dw[2][kk] * w[0][ii] * w[1][jj] * ioh;
+          } else {
+            g[0] = dw[0][ii] * w[1][jj] * ioh;
+            g[1] = dw[1][jj] * w[0][ii] * ioh;
+          }
+#pragma unroll
+          for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) gv[r][c] += vi[r] * g[c];
+        }
+      }
+  return true;
+}
+
+// F_trial = F + dt * gradv * F (deformation_update.cpp:42-44), then the
+// return mapping; writes F, scalars and tau into the out buffer at slot s.
+template <int D>
+__device__ __forceinline__ void defgrad_and_store(const StepArgs& A, uint32_t s, double dt, PLoad<D>& p,
+                                                  const double (&gv)[D][D], uint32_t& flags, bool& plastic) {
+  double T1[D][D], T2[D][D];
+#pragma unroll
+  for (int r = 0; r < D; ++r)
+#pragma unroll
+    for (int c = 0; c < D; ++c) T1[r][c] = dt * gv[r][c];
+  mat_mul<D>(T1, p.F, T2);
+#pragma unroll
+  for (int r = 0; r < D; ++r)
+#pragma unroll
+    for (int c = 0; c < D; ++c) p.F[r][c] = p.F[r][c] + T2[r][c];
+  double tau[Sym<D>::n];
+  plastic = return_map<D>(*A.P, dt, p.F, p.s, tau, flags);
+  store_defgrad<D>(A.out, A.Np, s, p.F, p.s, tau);
+}
+
+__device__ __forceinline__ void count_plastic(StepHeader* H, bool plastic) {
+  const unsigned m = __ballot_sync(__activemask(), plastic);
+  if ((threadIdx.x & 31) == __ffs(__activemask()) - 1 && m) atomicAdd(&H->plastic_count, (unsigned long long)__popc(m));
+}
+
+// ---------------------------------------------------------------------------
+// 7a. USL: fused G2P + deformation update + return mapping + position update
+// ---------------------------------------------------------------------------
+template <int D, int DEG>
+__global__ void __launch_bounds__(128) k_g2p(StepArgs A, const uint32_t* __restrict__ perm) {
+  StepHeader* H = A.H;
+  if (step_inactive(H)) return;
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= A.Np) return;
+  const DevParams& P = *A.P;
+  const uint32_t Np = A.Np, j = perm[s];
+  const double dt = H->dt;
+  const double fr = P.flip_ratio;
+  PLoad<D> p;
+  load_particle<D>(A.in, Np, j, p);
+  double pic[3], flp[3], Bp[D][D], gv[D][D];
+  if (!gather<D, DEG, true>(A, H, A.nv, p.x, pic, Bp, flp, gv, fr < 0, fr >= -1)) {
+    raise_status(H, MTR_STATUS_STENCIL_OOB, p.id);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) pic[a] = flp[a] = 0.0;
+#pragma unroll
+    for (int r = 0; r < D; ++r)
+#pragma unroll
+      for (int c = 0; c < D; ++c) Bp[r][c] = gv[r][c] = 0.0;
+  }
+  uint32_t flags = 0;
+  bool plastic = false;
+  defgrad_and_store<D>(A, s, dt, p, gv, flags, plastic);
+  // positionUpdate (position_update.cpp:6-46)
+  double xn[3], vn[3];
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    xn[a] = p.x[a] + dt * pic[a];
+    vn[a] = blend_v(fr, p.v[a], flp[a], pic[a]);
+  }
+  if (P.change_particle_positions && xn[0] > 0.8) {  // position_update.cpp:35-41
+    xn[0] = -0.1;
+    xn[1] += 0.27;
+  }
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    A.out.x[(size_t)a * Np + s] = xn[a];
+    A.out.v[(size_t)a * Np + s] = vn[a];
+  }
+#pragma unroll
+  for (int r = 0; r < D; ++r)
+#pragma unroll
+    for (int c = 0; c < D; ++c) A.out.B[(size_t)(r * D + c) * Np + s] = (fr < 0) ? Bp[r][c] : 0.0;
+  A.out.id[s] = p.id;
+  if (P.store_pic_flip) {
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      A.pic[(size_t)a * Np + s] = pic[a];
+      A.flip[(size_t)a * Np + s] = (fr >= -1) ? flp[a] : 0.0;
+    }
+  }
+  if (flags) raise_status(H, flags, p.id);
+  count_plastic(H, plastic);
+}
+
+// ---------------------------------------------------------------------------
+// 7b. MUSL (musl.cpp:6-96): G2P, velocity blend and re-scatter of
+// v_p + B D^-1 (x_i - x_p), one block per tile
+// ---------------------------------------------------------------------------
+template <int D, int DEG>
+__global__ void __launch_bounds__(128) k_g2p_musl(StepArgs A, const uint32_t* __restrict__ perm) {
+  using TL = Tiling<D>;
+  constexpr int PN = TL::PN, NODES = TL::NODES, TB = TL::TB;
+  StepHeader* H = A.H;
+  if (step_inactive(H)) return;
+  const uint32_t t = blockIdx.x;
+  if (t >= H->ntiles) return;
+  const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
+  if (pb >= pe) return;
+  const DevParams& P = *A.P;
+  __shared__ double patch[D][NODES];
+  __shared__ double crd[3][PN];
+  int tc[3];
+  tile_coords<D>(H, t, tc);
+  int n0[3] = {tc[0] * TB - 1, tc[1] * TB - 1, D == 3 ? tc[2] * TB - 1 : 0};
+  for (int i = threadIdx.x; i < D * NODES; i += blockDim.x) (&patch[0][0])[i] = 0.0;
+  for (int i = threadIdx.x; i < D * PN; i += blockDim.x) {
+    const int a = i / PN, o = i % PN;
+    const int g = n0[a] + o;
+    const double* ax = a == 0 ? A.gx : (a == 1 ? A.gy : A.gz);
+    crd[a][o] = (g >= 0 && g < (int)H->N[a]) ? ax[g] : 0.0;
+  }
+  __syncthreads();
+  const uint32_t Np = A.Np;
+  const double dt = H->dt, fr = P.flip_ratio, ioh = P.one_over_dx;
+  for (uint32_t s = pb + threadIdx.x; s < pe; s += blockDim.x) {
+    const uint32_t j = perm[s];
+    double xp[3] = {0, 0, 0}, vp[3] = {0, 0, 0};
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      xp[a] = A.in.x[(size_t)a * Np + j];
+      vp[a] = A.in.v[(size_t)a * Np + j];
+    }
+    const uint32_t pid = A.in.id[j];
+    double pic[3], flp[3], Bp[D][D], gv[D][D];
+    if (!gather<D, DEG, false>(A, H, A.nv, xp, pic, Bp, flp, gv, fr < 0, fr >= -1)) {
+      raise_status(H, MTR_STATUS_STENCIL_OOB, pid);
+      continue;
+    }
+    double vn[3] = {0, 0, 0};
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      vn[a] = blend_v(fr, vp[a], flp[a], pic[a]);
+      A.out.x[(size_t)a * Np + s] = xp[a] + dt * pic[a];  // positionUpdate: x + dt pic
+      A.out.v[(size_t)a * Np + s] = vn[a];
+    }
+#pragma unroll
+    for (int r = 0; r < D; ++r)
+#pragma unroll
+      for (int c = 0; c < D; ++c) A.out.B[(size_t)(r * D + c) * Np + s] = (fr < 0) ? Bp[r][c] : 0.0;
+    A.out.id[s] = pid;
+    if (P.store_pic_flip) {
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        A.pic[(size_t)a * Np + s] = pic[a];
+        A.flip[(size_t)a * Np + s] = (fr >= -1) ? flp[a] : 0.0;
+      }
+    }
+    // re-scatter (musl.cpp:35-76), base clamped at zero like P2G
+    int lb[3] = {0, 0, 0};
+    bool oob = false;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      int b = (int)floor((xp[a] - H->org[a]) * ioh) - 1;
+      b = b < 0 ? 0 : b;
+      lb[a] = b - n0[a];
+      if (lb[a] < 0 || lb[a] > PN - 4) oob = true;
+    }
+    if (oob) {
+      raise_status(H, MTR_STATUS_STENCIL_OOB, pid);
+      continue;
+    }
+    double w[3][4], dw[3][4];
+#pragma unroll
+    for (int a = 0; a < D; ++a) axis_weights<DEG>(xp[a], &crd[a][lb[a]], ioh, w[a], dw[a]);
+    constexpr int KN = D == 3 ? 4 : 1;
+#pragma unroll
+    for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+        for (int kk = 0; kk < KN; ++kk) {
+          const double wxy = w[0][ii] * w[1][jj];
+          const double weight = D == 3 ? wxy * w[2][kk] : wxy;
+          if (!(weight > 1e-25)) continue;
+          const int node = D == 3 ? ((lb[0] + ii) * PN + (lb[1] + jj)) * PN + (lb[2] + kk)
+                                  : (lb[0] + ii) * PN + (lb[1] + jj);
+          double pd[3] = {crd[0][lb[0] + ii] - xp[0], crd[1][lb[1] + jj] - xp[1],
+                          D == 3 ? crd[2][lb[2] + kk] - xp[2] : 0.0};
+#pragma unroll
+          for (int a = 0; a < D; ++a) {
+            double m = vn[a] * weight;
+            if (fr < 0) {
+              double bv = Bp[a][0] * pd[0];
+#pragma unroll
+              for (int c = 1; c < D; ++c) bv += Bp[a][c] * pd[c];
+              m += bv * P.apicDinverse * weight;
+            }
+            atomicAdd(&patch[a][node], m);
+          }
+        }
+  }
+  __syncthreads();
+  const uint32_t cap = A.cap_nodes;
+  for (int n = threadIdx.x; n < NODES; n += blockDim.x) {
+    int li, lj, lk;
+    if constexpr (D == 3) {
+      lk = n % PN;
+      lj = (n / PN) % PN;
+      li = n / (PN * PN);
+    } else {
+      lk = 0;
+      lj = n % PN;
+      li = n / PN;
+    }
+    const int gi = n0[0] + li, gj = n0[1] + lj, gk = n0[2] + lk;
+    if (gi < 0 || gj < 0 || gk < 0 || gi >= (int)H->N[0] || gj >= (int)H->N[1] || gk >= (int)H->N[2]) continue;
+    const uint32_t l = node_index(H, gi, gj, gk);
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      const double val = patch[a][n];
+      if (val != 0.0) atomicAdd(&A.v2[(size_t)a * cap + l], val);
+    }
+  }
+}
+
+// musl.cpp:80-95: v2 /= (m_i / m_p) (zero where m_i == 0)
+template <int D>
+__global__ void __launch_bounds__(256) k_musl_norm(StepArgs A) {
+  StepHeader* H = A.H;
+  if (step_inactive(H)) return;
+  const uint32_t G = H->G, cap = A.cap_nodes;
+  const double mp = A.P->particle_mass;
+  for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < G; l += gridDim.x * blockDim.x) {
+    const double mi = A.nmass[l];
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      double* p = &A.v2[(size_t)a * cap + l];
+      *p = (mi > 0) ? *p / (mi / mp) : 0.0;
+    }
+  }
+}
+
+// MUSL: deformation update from the re-projected velocities and the OLD
+// positions (deformation_update.cpp:6), then the return mapping.
+template <int D, int DEG>
+__global__ void __launch_bounds__(128) k_defgrad(StepArgs A, const uint32_t* __restrict__ perm) {
+  StepHeader* H = A.H;
+  if (step_inactive(H)) return;
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= A.Np) return;
+  const uint32_t Np = A.Np, j = perm[s];
+  const double dt = H->dt;
+  PLoad<D> p;
+  load_particle<D>(A.in, Np, j, p);
+  double pic[3], flp[3], Bp[D][D], gv[D][D];
+  if (!gather<D, DEG, true>(A, H, A.v2, p.x, pic, Bp, flp, gv, false, false)) {
+    raise_status(H, MTR_STATUS_STENCIL_OOB, p.id);
+#pragma unroll
+    for (int r = 0; r < D; ++r)
+#pragma unroll
+      for (int c = 0; c < D; ++c) gv[r][c] = 0.0;
+  }
+  uint32_t flags = 0;
+  bool plastic = false;
+  defgrad_and_store<D>(A, s, dt, p, gv, flags, plastic);
+  if (flags) raise_status(H, flags, p.id);
+  count_plastic(H, plastic);
+}
+
+// ---------------------------------------------------------------------------
+// 8. end of step: moveObjects and the clock of simulate()
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void k_tail(StepArgs A, int out_parity) {
+  StepHeader* H = A.H;
+  if (step_inactive(H)) return;
+  const DevParams& P = *A.P;
+  if (threadIdx.x != 0) return;
+  const double dt = H->dt;
+  for (int i = 0; i < P.nplates; ++i) {  // ObjectPlate::move, object_plate.hpp:136-162
+    mtr_plate& o = H->plates[i];
+    double factor = (H->time < o.load_factor * P.frame_dt) ? (1.0 / o.vmin_factor) : 1.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) o.v_object[a] = (a < D) ? o.v_object_original[a] * factor : 0.0;
+    if (o.plate_type == MTR_PLATE_LEFT || o.plate_type == MTR_PLATE_RIGHT) {
+      o.pos_object += dt * o.v_object[0];
+      o.pos_upper += dt * o.v_object[1];
+      o.pos_lower += dt * o.v_object[1];
+    } else if (o.plate_type == MTR_PLATE_BOTTOM || o.plate_type == MTR_PLATE_TOP) {
+      o.pos_object += dt * o.v_object[1];
+      o.pos_upper += dt * o.v_object[0];
+      o.pos_lower += dt * o.v_object[0];
+    } else if (D == 3 && (o.plate_type == MTR_PLATE_BACK || o.plate_type == MTR_PLATE_FRONT)) {
+      o.pos_object += dt * o.v_object[2];
+    }
+  }
+  H->cur = out_parity;
+  if (H->status & kExitMask) {  // simulation.cpp:176-177: return before time += dt
+    H->done = 1;
+    return;
+  }
+  H->time += dt;
+  H->step += 1;
+  if (__dsub_rn(__dmul_rn(P.frame_dt, (double)(H->frame + 1)), H->time) < 1e-15) H->frame += 1;
+  if (fabs(__dsub_rn(P.final_time, H->time)) < 1e-15 || P.final_time < H->time || !(H->frame < P.end_frame)) H->done = 1;
+}
+
+// ---------------------------------------------------------------------------
+// set-up and download
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void k_init_state(StepArgs A, PBuf b) {  // tau of the uploaded F, id = index
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.Np) return;
+  double F[D][D];
+#pragma unroll
+  for (int r = 0; r < D; ++r)
+#pragma unroll
+    for (int c = 0; c < D; ++c) F[r][c] = b.F[(size_t)(r * D + c) * A.Np + i];
+  double tau[Sym<D>::n];
+  initial_tau<D>(*A.P, F, tau);
+#pragma unroll
+  for (int q = 0; q < Sym<D>::n; ++q) b.tau[(size_t)q * A.Np + i] = tau[q];
+  b.id[i] = i;
+}
+
+// AoS (host layout, column-major matrices) <-> SoA, in original particle order
+template <int D>
+__global__ void k_aos_to_soa(uint32_t Np, const double* __restrict__ src, double* dst, int kind) {
+  // kind 0: vector (D), 1: matrix (D*D, column-major src -> (r*D+c) dst), 2: scalars (6)
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= Np) return;
+  if (kind == 0) {
+#pragma unroll
+    for (int a = 0; a < D; ++a) dst[(size_t)a * Np + i] = src[(size_t)i * D + a];
+  } else if (kind == 1) {
+#pragma unroll
+    for (int r = 0; r < D; ++r)
+#pragma unroll
+      for (int c = 0; c < D; ++c) dst[(size_t)(r * D + c) * Np + i] = src[(size_t)i * D * D + c * D + r];
+  } else {
+#pragma unroll
+    for (int q = 0; q < MTR_NUM_SCALARS; ++q) dst[(size_t)q * Np + i] = src[(size_t)i * MTR_NUM_SCALARS + q];
+  }
+}
+
+template <int D>
+__global__ void k_soa_to_aos(uint32_t Np, const double* __restrict__ src, const uint32_t* __restrict__ id, double* dst,
+                             int kind) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= Np) return;
+  const uint32_t i = id[s];
+  if (kind == 0) {
+#pragma unroll
+    for (int a = 0; a < D; ++a) dst[(size_t)i * D + a] = src[(size_t)a * Np + s];
+  } else if (kind == 1) {
+#pragma unroll
+    for (int r = 0; r < D; ++r)
+#pragma unroll
+      for (int c = 0; c < D; ++c) dst[(size_t)i * D * D + c * D + r] = src[(size_t)(r * D + c) * Np + s];
+  } else {
+#pragma unroll
+    for (int q = 0; q < MTR_NUM_SCALARS; ++q) dst[(size_t)i * MTR_NUM_SCALARS + q] = src[(size_t)q * Np + s];
+  }
+}
+
+}  // namespace mtr

@@ -1,0 +1,216 @@
+"""ctypes binding of libmatter_gpu.so (include/matter_gpu.h).
+
+This is the only way Python reaches the CUDA step.  There is no fallback: if
+the library is missing or no CUDA device is visible, calls raise.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from .abi import MtrClock, MtrObject, MtrParams, MtrPlate, ERROR_NAMES, MTR_OK, SCALARS
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmatter_gpu.so")
+
+_P = C.POINTER(C.c_double)
+_U = C.POINTER(C.c_uint32)
+
+# every entry point declared in include/matter_gpu.h
+EXPORTS = (
+    "mtr_ctx_create", "mtr_upload", "mtr_set_objects", "mtr_step", "mtr_run", "mtr_download",
+    "mtr_download_pic_flip", "mtr_get_grid", "mtr_get_sort", "mtr_get_plates", "mtr_get_clock",
+    "mtr_status", "mtr_clear_status", "mtr_sync", "mtr_stream", "mtr_launch_count", "mtr_keep_pic_flip",
+    "mtr_use_graphs", "mtr_ctx_destroy", "mtr_last_error",
+)
+
+_lib = None
+
+
+class MtrFailure(RuntimeError):
+    def __init__(self, fn, rc, msg):
+        super().__init__(f"{fn} returned {ERROR_NAMES.get(rc, rc)}: {msg}")
+        self.rc = rc
+
+
+def load_library(path=LIB_PATH):
+    """Loads and types the library (raises if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m matter_tests_b200.build`")
+    lib = C.CDLL(path)
+    lib.mtr_ctx_create.argtypes = [C.POINTER(MtrParams), C.c_int, C.POINTER(C.c_void_p)]
+    lib.mtr_upload.argtypes = [C.c_void_p, _P, _P, _P, _P, _P, C.c_uint32]
+    lib.mtr_set_objects.argtypes = [C.c_void_p, C.POINTER(MtrPlate), C.c_int, C.POINTER(MtrObject), C.c_int]
+    lib.mtr_step.argtypes = [C.c_void_p, C.c_int]
+    lib.mtr_run.argtypes = [C.c_void_p]
+    lib.mtr_download.argtypes = [C.c_void_p, _P, _P, _P, _P, _P]
+    lib.mtr_download_pic_flip.argtypes = [C.c_void_p, _P, _P]
+    lib.mtr_get_grid.argtypes = [C.c_void_p, _U, _P, _P, _P, _P, _P, _P]
+    lib.mtr_get_sort.argtypes = [C.c_void_p, _U, _U, _U]
+    lib.mtr_get_plates.argtypes = [C.c_void_p, C.POINTER(MtrPlate), C.c_int]
+    lib.mtr_get_clock.argtypes = [C.c_void_p, C.POINTER(MtrClock)]
+    lib.mtr_status.argtypes = [C.c_void_p, _U, _U]
+    lib.mtr_clear_status.argtypes = [C.c_void_p]
+    lib.mtr_sync.argtypes = [C.c_void_p, C.c_double]
+    lib.mtr_stream.argtypes = [C.c_void_p]
+    lib.mtr_stream.restype = C.c_void_p
+    lib.mtr_launch_count.argtypes = [C.c_void_p]
+    lib.mtr_launch_count.restype = C.c_int64
+    lib.mtr_keep_pic_flip.argtypes = [C.c_void_p, C.c_int]
+    lib.mtr_use_graphs.argtypes = [C.c_void_p, C.c_int]
+    lib.mtr_ctx_destroy.argtypes = [C.c_void_p]
+    lib.mtr_ctx_destroy.restype = None
+    lib.mtr_last_error.restype = C.c_char_p
+    _lib = lib
+    return lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+def _check(lib, fn, rc):
+    if rc != MTR_OK:
+        raise MtrFailure(fn, rc, lib.mtr_last_error().decode())
+    return rc
+
+
+class GpuSim:
+    """One simulation context on one GPU (mtr_ctx)."""
+
+    def __init__(self, params, device=0):
+        self.lib = load_library()
+        self.params = params
+        self.dim = params.dim
+        h = C.c_void_p()
+        _check(self.lib, "mtr_ctx_create", self.lib.mtr_ctx_create(C.byref(params), device, C.byref(h)))
+        self.h = h
+        self.Np = 0
+        self.nplates = 0
+
+    # -- set-up ---------------------------------------------------------
+    def upload(self, x, v=None, F=None, B=None, scalars=None):
+        d = self.dim
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+        n = x.size // d
+        arrs = []
+        for a, w in ((v, d), (F, d * d), (B, d * d), (scalars, 6)):
+            if a is None:
+                arrs.append(None)
+            else:
+                a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+                assert a.size == n * w
+                arrs.append(a)
+        _check(self.lib, "mtr_upload", self.lib.mtr_upload(self.h, _ptr(x), *(_ptr(a) for a in arrs), n))
+        self.Np = n
+
+    def set_objects(self, plates=(), objects=()):
+        self.nplates = len(plates)
+        pa = (MtrPlate * max(1, len(plates)))(*plates)
+        oa = (MtrObject * max(1, len(objects)))(*objects)
+        _check(self.lib, "mtr_set_objects", self.lib.mtr_set_objects(self.h, pa, len(plates), oa, len(objects)))
+
+    def keep_pic_flip(self, on=True):
+        _check(self.lib, "mtr_keep_pic_flip", self.lib.mtr_keep_pic_flip(self.h, 1 if on else 0))
+
+    def use_graphs(self, on=True):
+        _check(self.lib, "mtr_use_graphs", self.lib.mtr_use_graphs(self.h, 1 if on else 0))
+
+    # -- stepping -------------------------------------------------------
+    def step(self, n=1, check=True):
+        rc = self.lib.mtr_step(self.h, n)
+        if check:
+            _check(self.lib, "mtr_step", rc)
+        return rc
+
+    def run(self, check=True):
+        rc = self.lib.mtr_run(self.h)
+        if check:
+            _check(self.lib, "mtr_run", rc)
+        return rc
+
+    def sync(self, timeout=600.0):
+        _check(self.lib, "mtr_sync", self.lib.mtr_sync(self.h, timeout))
+
+    @property
+    def stream(self):
+        return self.lib.mtr_stream(self.h)
+
+    def launch_count(self):
+        return self.lib.mtr_launch_count(self.h)
+
+    # -- read-back ------------------------------------------------------
+    def particles(self, pic_flip=False):
+        d, n = self.dim, self.Np
+        out = {"x": np.zeros(n * d), "v": np.zeros(n * d), "F": np.zeros(n * d * d), "B": np.zeros(n * d * d),
+               "scalars": np.zeros(n * 6)}
+        _check(self.lib, "mtr_download", self.lib.mtr_download(
+            self.h, *(_ptr(out[k]) for k in ("x", "v", "F", "B", "scalars"))))
+        if pic_flip:
+            out["pic"], out["flip"] = np.zeros(n * d), np.zeros(n * d)
+            _check(self.lib, "mtr_download_pic_flip",
+                   self.lib.mtr_download_pic_flip(self.h, _ptr(out["pic"]), _ptr(out["flip"])))
+            out["pic"] = out["pic"].reshape(n, d)
+            out["flip"] = out["flip"].reshape(n, d)
+        out["x"] = out["x"].reshape(n, d)
+        out["v"] = out["v"].reshape(n, d)
+        out["F"] = out["F"].reshape(n, d, d)
+        out["B"] = out["B"].reshape(n, d, d)
+        out["scalars"] = out["scalars"].reshape(n, 6)
+        return out
+
+    def grid(self):
+        d = self.dim
+        dims = (C.c_uint32 * 3)()
+        _check(self.lib, "mtr_get_grid", self.lib.mtr_get_grid(self.h, dims, None, None, None, None, None, None))
+        nx, ny, nz = dims[0], dims[1], dims[2]
+        G = nx * ny * nz
+        gx, gy, gz = np.zeros(nx), np.zeros(ny), np.zeros(max(nz, 1))
+        m, v, fl = np.zeros(G), np.zeros(G * d), np.zeros(G * d)
+        _check(self.lib, "mtr_get_grid", self.lib.mtr_get_grid(self.h, dims, _ptr(gx), _ptr(gy), _ptr(gz), _ptr(m),
+                                                               _ptr(v), _ptr(fl)))
+        return {"dims": (nx, ny, nz), "x": gx, "y": gy, "z": gz, "mass": m, "v": v.reshape(G, d),
+                "flip": fl.reshape(G, d)}
+
+    def sort_state(self):
+        n = self.Np
+        keys, perm, ids = (np.zeros(n, dtype=np.uint32) for _ in range(3))
+        _check(self.lib, "mtr_get_sort", self.lib.mtr_get_sort(
+            self.h, keys.ctypes.data_as(_U), perm.ctypes.data_as(_U), ids.ctypes.data_as(_U)))
+        return keys, perm, ids
+
+    def clock(self):
+        ck = MtrClock()
+        _check(self.lib, "mtr_get_clock", self.lib.mtr_get_clock(self.h, C.byref(ck)))
+        return {"time": ck.time, "dt": ck.dt, "step": ck.step, "frame": ck.frame, "done": ck.done}
+
+    def status(self):
+        f, b = C.c_uint32(), C.c_uint32()
+        _check(self.lib, "mtr_status", self.lib.mtr_status(self.h, C.byref(f), C.byref(b)))
+        return f.value, b.value
+
+    def clear_status(self):
+        _check(self.lib, "mtr_clear_status", self.lib.mtr_clear_status(self.h))
+
+    def plates(self):
+        arr = (MtrPlate * max(1, self.nplates))()
+        _check(self.lib, "mtr_get_plates", self.lib.mtr_get_plates(self.h, arr, self.nplates))
+        return list(arr)[: self.nplates]
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mtr_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def scalars_dict(sc):
+    return {k: sc[:, i] for i, k in enumerate(SCALARS)}

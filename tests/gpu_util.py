@@ -1,0 +1,82 @@
+"""Helpers for the GPU tests: run a scene on the CUDA path and on the oracle."""
+import numpy as np
+import pytest
+
+from oracle.checkers import Oracle
+
+
+def gpu_available():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+needs_gpu = pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")
+
+
+def run_gpu(scene, nsteps, keep_pic_flip=True, graphs=True):
+    from matter_tests_b200.gpu import GpuSim
+    g = GpuSim(scene.params)
+    g.upload(scene.x, scene.v, scene.F, scene.B, scene.scalars)
+    g.set_objects(scene.plates, scene.objects)
+    if keep_pic_flip:
+        g.keep_pic_flip(True)
+    if not graphs:
+        g.use_graphs(False)
+    rc = g.step(nsteps, check=False)
+    out = dict(rc=rc, p=g.particles(pic_flip=keep_pic_flip), g=g.grid(), c=g.clock(), status=g.status(),
+               plates=g.plates(), sort=g.sort_state())
+    g.close()
+    return out
+
+
+def run_oracle(scene, nsteps):
+    o = Oracle(scene.params)
+    o.set_particles(scene.x, scene.v, scene.F, scene.B, scene.scalars)
+    o.set_objects(scene.plates, scene.objects)
+    n = o.step(nsteps)
+    out = dict(n=n, p=o.particles(), g=o.grid(), c=o.clock(), keys=o.keys(), plates=o.plates())
+    o.close()
+    return out
+
+
+def rel_err(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    scale = np.abs(b).max(initial=0.0)
+    diff = np.abs(a - b).max(initial=0.0)
+    if scale == 0.0:
+        return diff
+    return diff / scale
+
+
+def assert_close(name, a, b, rel):
+    e = rel_err(a, b)
+    assert np.all(np.isfinite(a) == np.isfinite(b)), f"{name}: finiteness differs"
+    assert e <= rel, f"{name}: relative error {e:.3e} > {rel:.1e}"
+    return e
+
+
+def compare_states(gpu, orc, rel=1e-10, fields=("x", "v", "F", "B", "pic", "flip"), grid=True):
+    errs = {}
+    assert gpu["c"]["step"] == orc["c"]["step"], (gpu["c"], orc["c"])
+    assert gpu["c"]["frame"] == orc["c"]["frame"]
+    assert gpu["c"]["done"] == orc["c"]["done"]
+    errs["time"] = assert_close("time", gpu["c"]["time"], orc["c"]["time"], rel)
+    errs["dt"] = assert_close("dt", gpu["c"]["dt"], orc["c"]["dt"], rel)
+    for k in fields:
+        if k in gpu["p"]:
+            errs[k] = assert_close(k, gpu["p"][k], orc["p"][k], rel)
+    from matter_tests_b200.abi import SCALARS
+    for i, k in enumerate(SCALARS):
+        errs[k] = assert_close(k, gpu["p"]["scalars"][:, i], orc["p"]["scalars"][:, i], rel)
+    if grid:
+        assert tuple(gpu["g"]["dims"]) == tuple(orc["g"]["dims"])
+        for k in ("x", "y", "z"):
+            assert np.array_equal(gpu["g"][k], orc["g"][k]), f"grid axis {k} not bit-identical"
+        errs["grid_mass"] = assert_close("grid mass", gpu["g"]["mass"], orc["g"]["mass"], rel)
+        errs["grid_v"] = assert_close("grid v", gpu["g"]["v"], orc["g"]["v"], rel)
+        errs["grid_flip"] = assert_close("grid flip", gpu["g"]["flip"], orc["g"]["flip"], rel)
+    return errs

@@ -1,0 +1,124 @@
+"""Parity of the CUDA step (libmatter_gpu.so, through its C ABI) with the oracle.
+
+The oracle is the C restatement pinned bit-for-bit to the reference compiled
+from source (test_oracle_pin.py).  The plain FP64 GPU path must match it to
+1e-10 relative per field (grid mass, momentum/velocity, flip and every
+particle field) after one step; GPU atomics and fused multiply-adds change the
+summation order, which moves results by a few ulps, far inside that bound.
+The grid axes (arange, tools.hpp:291-296) are compared bit for bit.
+"""
+import numpy as np
+import pytest
+
+from matter_tests_b200 import scenes
+from matter_tests_b200.abi import BC
+
+import cases
+from gpu_util import compare_states, needs_gpu, run_gpu, run_oracle
+
+pytestmark = [pytest.mark.gpu, needs_gpu]
+
+REL_ONE_STEP = 1e-10
+
+
+@pytest.mark.parametrize("deg", [2, 3])
+@pytest.mark.parametrize("model", sorted(cases.MODEL_CASES))
+def test_models_one_step(model, deg):
+    sc = cases.apply(cases.block(3, deg, n=5), **cases.MODEL_CASES[model])
+    sc = cases.box_plates(sc, BC.SlipFree, 0.3)
+    g, o = run_gpu(sc, 1), run_oracle(sc, 1)
+    compare_states(g, o, REL_ONE_STEP)
+
+
+@pytest.mark.parametrize("model", ["dp", "dpmui", "mccvisc", "dpsoft", "noplast", "vmvisc_newton"])
+def test_models_2d_one_step(model):
+    sc = cases.apply(cases.block(2, 2, n=8), **cases.MODEL_CASES[model])
+    sc = cases.box_plates(sc, BC.SlipStick, 0.3)
+    g, o = run_gpu(sc, 1), run_oracle(sc, 1)
+    compare_states(g, o, REL_ONE_STEP)
+
+
+@pytest.mark.parametrize("dim,deg", [(2, 2), (2, 3), (3, 2), (3, 3)])
+@pytest.mark.parametrize("transfer", sorted(cases.TRANSFER_CASES))
+def test_transfers_one_step(transfer, dim, deg):
+    sc = cases.apply(cases.block(dim, deg, n=6 if dim == 3 else 10), plastic_model=cases.PM.DP, M=0.6,
+                     **cases.TRANSFER_CASES[transfer])
+    sc = cases.box_plates(sc, BC.SlipStick, 0.4)
+    g, o = run_gpu(sc, 1), run_oracle(sc, 1)
+    compare_states(g, o, REL_ONE_STEP)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("bc", [BC.NoSlip, BC.SlipStick, BC.SlipFree])
+@pytest.mark.parametrize("moving", [False, True])
+def test_plates(bc, moving, dim):
+    sc = cases.apply(cases.block(dim, 2, n=6 if dim == 3 else 10), plastic_model=cases.PM.NoPlasticity)
+    sc = cases.box_plates(sc, bc, 0.35, moving=moving)
+    g, o = run_gpu(sc, 3), run_oracle(sc, 3)
+    compare_states(g, o, 1e-9)
+    for pg, po in zip(g["plates"], o["plates"]):
+        assert abs(pg.pos_object - po.pos_object) <= 1e-12 * max(1.0, abs(po.pos_object))
+        assert abs(pg.pos_upper - po.pos_upper) <= 1e-9 * max(1.0, abs(po.pos_upper))
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("obj", ["bump", "ground", "ramp", "curve", "gate", "terrain", "two_objects", "box", "silo"])
+def test_objects(obj, dim):
+    oc = cases.object_cases(dim)
+    if obj not in oc:
+        pytest.skip("3D-only object")
+    sc = cases.apply(cases.block(dim, 2, n=5 if dim == 3 else 10), plastic_model=cases.PM.DPVisc, M=0.5, use_mibf=1)
+    sc.objects = oc[obj]
+    g, o = run_gpu(sc, 2), run_oracle(sc, 2)
+    compare_states(g, o, 1e-9)
+
+
+@pytest.mark.parametrize("builder,scale", [("collapse2d", 0.25), ("collapse3d_mui", 0.12), ("incline3d_mcc", 0.12)])
+def test_workloads_ten_steps(builder, scale):
+    sc = scenes.WORKLOADS[builder](scale=scale)
+    g, o = run_gpu(sc, 10), run_oracle(sc, 10)
+    compare_states(g, o, 1e-9)
+
+
+def test_graphs_match_direct_launches():
+    sc = cases.apply(cases.block(3, 3, n=5), plastic_model=cases.PM.DPMui, use_musl=1)
+    a = run_gpu(sc, 37, graphs=True)
+    b = run_gpu(sc, 37, graphs=False)
+    assert a["c"]["step"] == b["c"]["step"] == 37
+    for k in ("x", "v", "F"):
+        assert np.abs(a["p"][k] - b["p"][k]).max() <= 1e-12 * max(1.0, np.abs(b["p"][k]).max())
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_sort_keys_bitexact(dim):
+    """Cell keys equal the oracle's and the order is a stable sort of them."""
+    sc = cases.apply(cases.block(dim, 2, n=7 if dim == 3 else 12), plastic_model=cases.PM.DP, M=0.6)
+    for nsteps in (1, 4):
+        g, o = run_gpu(sc, nsteps), run_oracle(sc, nsteps)
+        keys_in, perm, ids_in = g["sort"]
+        # keys of the last step, in the order of that step's input, mapped to particle ids
+        k_orig = np.zeros_like(keys_in)
+        k_orig[ids_in] = keys_in
+        assert np.array_equal(k_orig, o["keys"]), "cell keys differ from the oracle's"
+        assert np.array_equal(perm, np.argsort(keys_in, kind="stable")), "not a stable sort"
+
+
+def test_end_of_simulation_clock():
+    sc = cases.apply(cases.block(3, 2, n=3), plastic_model=cases.PM.DP, M=0.6)
+    dt_max = 0.5 * sc.params.dx / np.sqrt(sc.params.E / sc.params.rho)
+    sc.params.fps = 1.0 / (3.5 * dt_max)
+    sc.params.end_frame = 1
+    g, o = run_gpu(sc, 10), run_oracle(sc, 10)
+    assert g["c"]["step"] == o["c"]["step"] == 4
+    assert g["c"]["done"] == 1
+    compare_states(g, o, 1e-9)
+
+
+def test_grid_regrowth():
+    """A block flying apart outgrows the first grid allocation; the step
+    aborts before touching state, the grid regrows and the run continues."""
+    sc = cases.apply(cases.block(3, 2, n=4), plastic_model=cases.PM.NoPlasticity)
+    sc.v = sc.v * 0 + np.array([8.0, 0.0, 0.0]) * np.sign(sc.x[:, :1] - sc.x[:, :1].mean())
+    g, o = run_gpu(sc, 60), run_oracle(sc, 60)
+    assert g["c"]["step"] == 60
+    compare_states(g, o, 1e-8)
