@@ -212,7 +212,29 @@ def reference_threads(Np):
     return max(1, min(n, int(0.5 * avail / per_thread)))
 
 
+class quiet_stdout:
+    """Silences fd 1 while the reference runs (Simulation prints banners)."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *exc):
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+        return False
+
+
 def run_cpu_reference(scene, budget_s, max_steps=None, warmup=1):
+    with quiet_stdout():
+        return _run_cpu_reference(scene, budget_s, max_steps, warmup)
+
+
+def _run_cpu_reference(scene, budget_s, max_steps=None, warmup=1):
     """Times the reference's own OpenMP step (oracle/_ref) on the workload.
     Returns (particle-steps/s, threads, kind, sample description)."""
     from oracle.checkers import Oracle, Reference, reference_available

@@ -189,6 +189,20 @@ void mark(mtr_ctx* c, const char* name) {
   c->marks.emplace_back(name, e);
 }
 
+template <int D, int DEG>
+void set_kernel_attributes_t() {
+  CK(cudaFuncSetAttribute(k_p2g_w<D, DEG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_smem_bytes<D>()));
+  CK(cudaFuncSetAttribute(k_g2p_musl_w<D, DEG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)musl_smem_bytes<D>()));
+}
+
+void set_kernel_attributes() {
+  set_kernel_attributes_t<2, 2>();
+  set_kernel_attributes_t<2, 3>();
+  set_kernel_attributes_t<3, 2>();
+  set_kernel_attributes_t<3, 3>();
+}
+
 StepArgs make_args(mtr_ctx* c, int parity) {
   StepArgs A{};
   A.P = c->dP;
@@ -268,7 +282,7 @@ int enqueue_step_t(mtr_ctx* c, int parity) {
   k_tile_ranges<<<std::min<uint32_t>((c->Np + 255) / 256, 148 * 8), 256, 0, st>>>(A, skeys);
   ++n;
   mark(c, "k_tile_ranges");
-  k_p2g<D, DEG><<<c->cap_tiles, 128, 0, st>>>(A, perm);
+  k_p2g_w<D, DEG><<<c->cap_tiles, kChunk, p2g_smem_bytes<D>(), st>>>(A, perm);
   ++n;
   mark(c, "k_p2g");
   const uint32_t gblocks = std::min<uint32_t>((c->cap_nodes + 255) / 256, 148 * 16);
@@ -278,7 +292,7 @@ int enqueue_step_t(mtr_ctx* c, int parity) {
   if (c->prm.use_musl) {
     CK(cudaMemsetAsync(c->v2, 0, sizeof(double) * D * c->cap_nodes, st));
     mark(c, "memset(v2)");
-    k_g2p_musl<D, DEG><<<c->cap_tiles, 128, 0, st>>>(A, perm);
+    k_g2p_musl_w<D, DEG><<<c->cap_tiles, kChunk, musl_smem_bytes<D>(), st>>>(A, perm);
     mark(c, "k_g2p_musl");
     k_musl_norm<D><<<gblocks, 256, 0, st>>>(A);
     mark(c, "k_musl_norm");
@@ -457,6 +471,7 @@ int mtr_ctx_create(const mtr_params* params, int device, mtr_ctx** out) {
       c->deg = p.spline_deg;
       CK(cudaSetDevice(device));
       CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+      set_kernel_attributes();
       derive_constants(c);
       c->dP = dalloc<DevParams>(1);
       c->dH = dalloc<StepHeader>(1);

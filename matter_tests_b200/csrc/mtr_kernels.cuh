@@ -600,6 +600,230 @@ __global__ void __launch_bounds__(128) k_p2g(StepArgs A, const uint32_t* __restr
 }
 
 // ---------------------------------------------------------------------------
+// 5'. P2G + stress force, warp-cooperative form (used for every launch).
+//
+// A tile block walks its sorted particles in chunks of kChunk.  Phase 1, one
+// thread per particle, loads the particle and stages its stencil weights and
+// gradients in shared memory.  Phase 2, one warp per run of 32 staged
+// particles: every lane owns fixed stencil nodes of a cell (3D: 2 of the 64,
+// 2D: 1 of the 16, a half warp per particle), accumulates all channels in
+// registers while consecutive particles share a cell, and adds them to the
+// shared patch once per cell.  Sorted particles share cells in runs of about
+// ppc, so this issues ~ppc times fewer shared atomics than one atomic per
+// particle and node, with no two lanes of a warp on one address.
+// ---------------------------------------------------------------------------
+constexpr int kChunk = 128;
+
+template <int D>
+struct PStage {
+  double x[D], v[D], B[D * D], tau[Sym<D>::n], w[D * 4], dw[D * 4];
+  double mui;
+  int lb;  // packed local stencil base (4 bits per axis); -1 marks an empty slot
+  int pad;
+};
+
+template <int D>
+constexpr size_t p2g_smem_bytes() {
+  return sizeof(double) * (Tiling<D>::NCH * Tiling<D>::NODES + 3 * Tiling<D>::PN) + sizeof(PStage<D>) * kChunk;
+}
+
+template <int D, int DEG>
+__global__ void __launch_bounds__(kChunk) k_p2g_w(StepArgs A, const uint32_t* __restrict__ perm) {
+  using TL = Tiling<D>;
+  constexpr int PN = TL::PN, NODES = TL::NODES, NCH = TL::NCH, TB = TL::TB;
+  constexpr int NS = Sym<D>::n;
+  const StepHeader* H = A.H;
+  if (step_inactive(H)) return;
+  const uint32_t t = blockIdx.x;
+  if (t >= H->ntiles) return;
+  const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
+  if (pb >= pe) return;
+  const DevParams& P = *A.P;
+  extern __shared__ double smem[];
+  double(*patch)[NODES] = reinterpret_cast<double(*)[NODES]>(smem);
+  double(*crd)[PN] = reinterpret_cast<double(*)[PN]>(smem + NCH * NODES);
+  PStage<D>* st = reinterpret_cast<PStage<D>*>(smem + NCH * NODES + 3 * PN);
+  int tc[3];
+  tile_coords<D>(H, t, tc);
+  const int n0[3] = {tc[0] * TB - 1, tc[1] * TB - 1, D == 3 ? tc[2] * TB - 1 : 0};
+  for (int i = threadIdx.x; i < NCH * NODES; i += blockDim.x) (&patch[0][0])[i] = 0.0;
+  for (int i = threadIdx.x; i < D * PN; i += blockDim.x) {
+    const int a = i / PN, o = i % PN;
+    const int g = n0[a] + o;
+    const double* ax = a == 0 ? A.gx : (a == 1 ? A.gy : A.gz);
+    crd[a][o] = (g >= 0 && g < (int)H->N[a]) ? ax[g] : 0.0;
+  }
+  __syncthreads();
+  const uint32_t Np = A.Np;
+  const double ioh = P.one_over_dx, apicD = P.apicDinverse;
+  const bool apic = P.flip_ratio < 0;
+  const bool mibf = P.use_mibf;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // the stencil nodes this lane owns
+  int ix0, iy, iz;
+  int kbeg, kend;
+  if constexpr (D == 3) {
+    ix0 = lane >> 4;  // nodes (ix0, iy, iz) and (ix0 + 2, iy, iz)
+    iy = (lane >> 2) & 3;
+    iz = lane & 3;
+    kbeg = warp * 32;
+    kend = kbeg + 32;
+  } else {
+    ix0 = (lane & 15) >> 2;  // one node (ix0, iy); a half warp per particle run
+    iy = lane & 3;
+    iz = 0;
+    kbeg = warp * 32 + (lane >> 4) * 16;
+    kend = kbeg + 16;
+  }
+  constexpr int NH = D == 3 ? 2 : 1;
+  for (uint32_t c0 = pb; c0 < pe; c0 += kChunk) {
+    {  // phase 1: stage one particle per thread
+      const uint32_t s = c0 + threadIdx.x;
+      PStage<D>& S = st[threadIdx.x];
+      int packed = -1;
+      if (s < pe) {
+        const uint32_t j = perm[s];
+        int lb[3] = {0, 0, 0};
+        bool oob = false;
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+          S.x[a] = A.in.x[(size_t)a * Np + j];
+          S.v[a] = A.in.v[(size_t)a * Np + j];
+          int b = (int)floor((S.x[a] - H->org[a]) * ioh) - 1;
+          b = b < 0 ? 0 : b;  // p2g.cpp:21-24 clamps at zero
+          lb[a] = b - n0[a];
+          if (lb[a] < 0 || lb[a] > PN - 4 || b + 3 >= (int)H->N[a]) oob = true;
+        }
+#pragma unroll
+        for (int q = 0; q < D * D; ++q) S.B[q] = apic ? A.in.B[(size_t)q * Np + j] : 0.0;
+#pragma unroll
+        for (int q = 0; q < NS; ++q) S.tau[q] = A.in.tau[(size_t)q * Np + j];
+        S.mui = mibf ? A.in.sc[(size_t)MTR_SCALAR_MUI * Np + j] : 0.0;
+        if (oob) {
+          raise_status(A.H, MTR_STATUS_STENCIL_OOB, A.in.id[j]);
+        } else {
+#pragma unroll
+          for (int a = 0; a < D; ++a) {
+#pragma unroll
+            for (int o = 0; o < 4; ++o) {
+              const double u = (S.x[a] - crd[a][lb[a] + o]) * ioh;
+              S.w[a * 4 + o] = bspline_N<DEG>(u);
+              S.dw[a * 4 + o] = bspline_dN<DEG>(u);
+            }
+          }
+          packed = lb[0] | (lb[1] << 4) | (lb[2] << 8);
+        }
+      }
+      S.lb = packed;
+    }
+    __syncthreads();
+    {  // phase 2: lanes own nodes, registers accumulate per cell
+      double acc[NH][NCH];
+#pragma unroll
+      for (int h = 0; h < NH; ++h)
+#pragma unroll
+        for (int ch = 0; ch < NCH; ++ch) acc[h][ch] = 0.0;
+      int cur = -1;
+      auto flush = [&]() {
+        const int lbx = cur & 15, lby = (cur >> 4) & 15, lbz = cur >> 8;
+#pragma unroll
+        for (int h = 0; h < NH; ++h) {
+          const int ix = ix0 + 2 * h;
+          const int node = D == 3 ? ((lbx + ix) * PN + (lby + iy)) * PN + (lbz + iz) : (lbx + ix) * PN + (lby + iy);
+#pragma unroll
+          for (int ch = 0; ch < NCH; ++ch) {
+            if (acc[h][ch] != 0.0) atomicAdd(&patch[ch][node], acc[h][ch]);
+            acc[h][ch] = 0.0;
+          }
+        }
+      };
+      for (int k = kbeg; k < kend; ++k) {
+        const PStage<D>& S = st[k];
+        const int lbp = S.lb;
+        if (lbp < 0) continue;
+        if (lbp != cur) {
+          if (cur >= 0) flush();
+          cur = lbp;
+        }
+        const int lbx = lbp & 15, lby = (lbp >> 4) & 15, lbz = lbp >> 8;
+        const double wy = S.w[4 + iy], dwy = S.dw[4 + iy];
+        const double wz = D == 3 ? S.w[8 + iz] : 1.0, dwz = D == 3 ? S.dw[8 + iz] : 0.0;
+        double xp[D], vp[D], tau[NS];
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+          xp[a] = S.x[a];
+          vp[a] = S.v[a];
+        }
+#pragma unroll
+        for (int q = 0; q < NS; ++q) tau[q] = S.tau[q];
+#pragma unroll
+        for (int h = 0; h < NH; ++h) {
+          const int ix = ix0 + 2 * h;
+          const double wx = S.w[ix], dwx = S.dw[ix];
+          const double wxy = wx * wy;
+          const double weight = D == 3 ? wxy * wz : wxy;
+          if (weight > 1e-25) {
+            acc[h][0] += weight;
+            double pd[3] = {crd[0][lbx + ix] - xp[0], crd[1][lby + iy] - xp[1], D == 3 ? crd[2][lbz + iz] - xp[D - 1] : 0.0};
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+              double m = vp[a] * weight;
+              if (apic) {
+                double bv = S.B[a * D] * pd[0];
+#pragma unroll
+                for (int c = 1; c < D; ++c) bv += S.B[a * D + c] * pd[c];
+                m += bv * apicD * weight;
+              }
+              acc[h][1 + a] += m;
+            }
+            if (mibf) acc[h][1 + 2 * D] += S.mui * weight;
+          }
+          double g[3];
+          if constexpr (D == 3) {
+            g[0] = dwx * wy * wz * ioh;
+            g[1] = dwy * wx * wz * ioh;
+            g[2] = dwz * wx * wy * ioh;
+          } else {
+            g[0] = dwx * wy * ioh;
+            g[1] = dwy * wx * ioh;
+          }
+#pragma unroll
+          for (int a = 0; a < D; ++a) {
+            double f = sym_at<D>(tau, a, 0) * g[0];
+#pragma unroll
+            for (int c = 1; c < D; ++c) f += sym_at<D>(tau, a, c) * g[c];
+            acc[h][1 + D + a] += f;
+          }
+        }
+      }
+      if (cur >= 0) flush();
+    }
+    __syncthreads();
+  }
+  const uint32_t cap = A.cap_nodes;
+  for (int n = threadIdx.x; n < NODES; n += blockDim.x) {
+    int li, lj, lk;
+    if constexpr (D == 3) {
+      lk = n % PN;
+      lj = (n / PN) % PN;
+      li = n / (PN * PN);
+    } else {
+      lk = 0;
+      lj = n % PN;
+      li = n / PN;
+    }
+    const int gi = n0[0] + li, gj = n0[1] + lj, gk = n0[2] + lk;
+    if (gi < 0 || gj < 0 || gk < 0 || gi >= (int)H->N[0] || gj >= (int)H->N[1] || gk >= (int)H->N[2]) continue;
+    const uint32_t l = node_index(H, gi, gj, gk);
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) {
+      const double val = patch[ch][n];
+      if (val != 0.0) atomicAdd(&A.acc[(size_t)ch * cap + l], val);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // 6. grid update, one thread per node
 // ---------------------------------------------------------------------------
 template <int D>
@@ -996,6 +1220,210 @@ __global__ void __launch_bounds__(128) k_g2p_musl(StepArgs A, const uint32_t* __
       if (val != 0.0) atomicAdd(&A.v2[(size_t)a * cap + l], val);
     }
   }
+}
+
+// MUSL G2P + re-scatter, two-phase form of k_g2p_musl: phase 1 (thread per
+// particle) gathers, blends and writes the particle and stages v_new, B_new
+// and the weights; phase 2 (warp per run, lanes owning stencil nodes)
+// accumulates v_p + B D^-1 (x_i - x_p) per cell in registers.
+template <int D, int DEG>
+__global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgs A, const uint32_t* __restrict__ perm) {
+  using TL = Tiling<D>;
+  constexpr int PN = TL::PN, NODES = TL::NODES, TB = TL::TB;
+  StepHeader* H = A.H;
+  if (step_inactive(H)) return;
+  const uint32_t t = blockIdx.x;
+  if (t >= H->ntiles) return;
+  const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
+  if (pb >= pe) return;
+  const DevParams& P = *A.P;
+  extern __shared__ double smem[];
+  double(*patch)[NODES] = reinterpret_cast<double(*)[NODES]>(smem);
+  double(*crd)[PN] = reinterpret_cast<double(*)[PN]>(smem + D * NODES);
+  PStage<D>* st = reinterpret_cast<PStage<D>*>(smem + D * NODES + 3 * PN);
+  int tc[3];
+  tile_coords<D>(H, t, tc);
+  const int n0[3] = {tc[0] * TB - 1, tc[1] * TB - 1, D == 3 ? tc[2] * TB - 1 : 0};
+  for (int i = threadIdx.x; i < D * NODES; i += blockDim.x) (&patch[0][0])[i] = 0.0;
+  for (int i = threadIdx.x; i < D * PN; i += blockDim.x) {
+    const int a = i / PN, o = i % PN;
+    const int g = n0[a] + o;
+    const double* ax = a == 0 ? A.gx : (a == 1 ? A.gy : A.gz);
+    crd[a][o] = (g >= 0 && g < (int)H->N[a]) ? ax[g] : 0.0;
+  }
+  __syncthreads();
+  const uint32_t Np = A.Np;
+  const double dt = H->dt, fr = P.flip_ratio, ioh = P.one_over_dx, apicD = P.apicDinverse;
+  const bool apic = fr < 0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int ix0, iy, iz, kbeg, kend;
+  if constexpr (D == 3) {
+    ix0 = lane >> 4;
+    iy = (lane >> 2) & 3;
+    iz = lane & 3;
+    kbeg = warp * 32;
+    kend = kbeg + 32;
+  } else {
+    ix0 = (lane & 15) >> 2;
+    iy = lane & 3;
+    iz = 0;
+    kbeg = warp * 32 + (lane >> 4) * 16;
+    kend = kbeg + 16;
+  }
+  constexpr int NH = D == 3 ? 2 : 1;
+  for (uint32_t c0 = pb; c0 < pe; c0 += kChunk) {
+    {  // phase 1
+      const uint32_t s = c0 + threadIdx.x;
+      PStage<D>& S = st[threadIdx.x];
+      int packed = -1;
+      if (s < pe) {
+        const uint32_t j = perm[s];
+        double xp[3] = {0, 0, 0}, vp[3] = {0, 0, 0};
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+          xp[a] = A.in.x[(size_t)a * Np + j];
+          vp[a] = A.in.v[(size_t)a * Np + j];
+        }
+        const uint32_t pid = A.in.id[j];
+        double pic[3], flp[3], Bp[D][D], gv[D][D];
+        if (!gather<D, DEG, false>(A, H, A.nv, xp, pic, Bp, flp, gv, apic, fr >= -1)) {
+          raise_status(H, MTR_STATUS_STENCIL_OOB, pid);
+#pragma unroll
+          for (int a = 0; a < 3; ++a) pic[a] = flp[a] = 0.0;
+#pragma unroll
+          for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) Bp[r][c] = 0.0;
+        }
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+          const double vn = blend_v(fr, vp[a], flp[a], pic[a]);
+          S.x[a] = xp[a];
+          S.v[a] = vn;
+          A.out.x[(size_t)a * Np + s] = xp[a] + dt * pic[a];  // positionUpdate: x + dt pic
+          A.out.v[(size_t)a * Np + s] = vn;
+        }
+#pragma unroll
+        for (int r = 0; r < D; ++r)
+#pragma unroll
+          for (int c = 0; c < D; ++c) {
+            const double b = apic ? Bp[r][c] : 0.0;
+            A.out.B[(size_t)(r * D + c) * Np + s] = b;
+            S.B[r * D + c] = b;
+          }
+        A.out.id[s] = pid;
+        if (P.store_pic_flip) {
+#pragma unroll
+          for (int a = 0; a < D; ++a) {
+            A.pic[(size_t)a * Np + s] = pic[a];
+            A.flip[(size_t)a * Np + s] = (fr >= -1) ? flp[a] : 0.0;
+          }
+        }
+        // re-scatter stencil, base clamped at zero like P2G (musl.cpp:35-40)
+        int lb[3] = {0, 0, 0};
+        bool oob = false;
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+          int b = (int)floor((xp[a] - H->org[a]) * ioh) - 1;
+          b = b < 0 ? 0 : b;
+          lb[a] = b - n0[a];
+          if (lb[a] < 0 || lb[a] > PN - 4) oob = true;
+        }
+        if (oob) {
+          raise_status(H, MTR_STATUS_STENCIL_OOB, pid);
+        } else {
+#pragma unroll
+          for (int a = 0; a < D; ++a)
+#pragma unroll
+            for (int o = 0; o < 4; ++o) S.w[a * 4 + o] = bspline_N<DEG>((xp[a] - crd[a][lb[a] + o]) * ioh);
+          packed = lb[0] | (lb[1] << 4) | (lb[2] << 8);
+        }
+      }
+      S.lb = packed;
+    }
+    __syncthreads();
+    {  // phase 2
+      double acc[NH][D];
+#pragma unroll
+      for (int h = 0; h < NH; ++h)
+#pragma unroll
+        for (int a = 0; a < D; ++a) acc[h][a] = 0.0;
+      int cur = -1;
+      auto flush = [&]() {
+        const int lbx = cur & 15, lby = (cur >> 4) & 15, lbz = cur >> 8;
+#pragma unroll
+        for (int h = 0; h < NH; ++h) {
+          const int ix = ix0 + 2 * h;
+          const int node = D == 3 ? ((lbx + ix) * PN + (lby + iy)) * PN + (lbz + iz) : (lbx + ix) * PN + (lby + iy);
+#pragma unroll
+          for (int a = 0; a < D; ++a) {
+            if (acc[h][a] != 0.0) atomicAdd(&patch[a][node], acc[h][a]);
+            acc[h][a] = 0.0;
+          }
+        }
+      };
+      for (int k = kbeg; k < kend; ++k) {
+        const PStage<D>& S = st[k];
+        const int lbp = S.lb;
+        if (lbp < 0) continue;
+        if (lbp != cur) {
+          if (cur >= 0) flush();
+          cur = lbp;
+        }
+        const int lbx = lbp & 15, lby = (lbp >> 4) & 15, lbz = lbp >> 8;
+        const double wy = S.w[4 + iy];
+        const double wz = D == 3 ? S.w[8 + iz] : 1.0;
+#pragma unroll
+        for (int h = 0; h < NH; ++h) {
+          const int ix = ix0 + 2 * h;
+          const double wxy = S.w[ix] * wy;
+          const double weight = D == 3 ? wxy * wz : wxy;
+          if (!(weight > 1e-25)) continue;
+          double pd[3] = {crd[0][lbx + ix] - S.x[0], crd[1][lby + iy] - S.x[1],
+                          D == 3 ? crd[2][lbz + iz] - S.x[D - 1] : 0.0};
+#pragma unroll
+          for (int a = 0; a < D; ++a) {
+            double m = S.v[a] * weight;
+            if (apic) {
+              double bv = S.B[a * D] * pd[0];
+#pragma unroll
+              for (int c = 1; c < D; ++c) bv += S.B[a * D + c] * pd[c];
+              m += bv * apicD * weight;
+            }
+            acc[h][a] += m;
+          }
+        }
+      }
+      if (cur >= 0) flush();
+    }
+    __syncthreads();
+  }
+  const uint32_t cap = A.cap_nodes;
+  for (int n = threadIdx.x; n < NODES; n += blockDim.x) {
+    int li, lj, lk;
+    if constexpr (D == 3) {
+      lk = n % PN;
+      lj = (n / PN) % PN;
+      li = n / (PN * PN);
+    } else {
+      lk = 0;
+      lj = n % PN;
+      li = n / PN;
+    }
+    const int gi = n0[0] + li, gj = n0[1] + lj, gk = n0[2] + lk;
+    if (gi < 0 || gj < 0 || gk < 0 || gi >= (int)H->N[0] || gj >= (int)H->N[1] || gk >= (int)H->N[2]) continue;
+    const uint32_t l = node_index(H, gi, gj, gk);
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      const double val = patch[a][n];
+      if (val != 0.0) atomicAdd(&A.v2[(size_t)a * cap + l], val);
+    }
+  }
+}
+
+template <int D>
+constexpr size_t musl_smem_bytes() {
+  return sizeof(double) * (D * Tiling<D>::NODES + 3 * Tiling<D>::PN) + sizeof(PStage<D>) * kChunk;
 }
 
 // musl.cpp:80-95: v2 /= (m_i / m_p) (zero where m_i == 0)

@@ -73,8 +73,12 @@ def rel_err(a, b):
     return diff / scale
 
 
-def assert_close(name, a, b, rel):
+def assert_close(name, a, b, rel, report=None):
     e = rel_err(a, b)
+    ok = bool(np.all(np.isfinite(a) == np.isfinite(b))) and e <= rel
+    if report is not None:
+        report.append((name, e, rel, ok))
+        return e
     assert np.all(np.isfinite(a) == np.isfinite(b)), f"{name}: finiteness differs"
     assert e <= rel, f"{name}: relative error {e:.3e} > {rel:.1e}"
     return e
@@ -91,25 +95,29 @@ def compare_states(gpu, orc, rel=1e-10, fields=("x", "v", "F", "B", "pic", "flip
     assert gpu["c"]["frame"] == orc["c"]["frame"]
     # the oracle reports the reference's exit flag apart from the end of time
     assert gpu["c"]["done"] == int(orc["c"]["done"] or orc["c"]["exit"])
-    errs["time"] = assert_close("time", gpu["c"]["time"], orc["c"]["time"], rel)
-    errs["dt"] = assert_close("dt", gpu["c"]["dt"], orc["c"]["dt"], rel)
+    rep = []
+    errs["time"] = assert_close("time", gpu["c"]["time"], orc["c"]["time"], rel, rep)
+    errs["dt"] = assert_close("dt", gpu["c"]["dt"], orc["c"]["dt"], rel, rep)
     for k in fields:
         if k in gpu["p"]:
-            errs[k] = assert_close(k, gpu["p"][k], orc["p"][k], rel)
+            errs[k] = assert_close(k, gpu["p"][k], orc["p"][k], rel, rep)
     from matter_tests_b200.abi import SCALARS
     for i, k in enumerate(SCALARS):
         a, b = gpu["p"]["scalars"][:, i], orc["p"]["scalars"][:, i]
         scale = np.abs(b).max(initial=0.0)
         tol = rel * scale + (sens_factor * sens[k] if sens is not None else 0.0)
         diff = np.abs(a - b).max(initial=0.0)
-        assert np.all(np.isfinite(a) == np.isfinite(b)), f"{k}: finiteness differs"
-        assert diff <= tol, f"{k}: |diff| {diff:.3e} > tol {tol:.3e} (scale {scale:.3e})"
+        ok = bool(np.all(np.isfinite(a) == np.isfinite(b))) and diff <= tol
+        rep.append((k + " (abs)", diff, tol, ok))
         errs[k] = diff / scale if scale > 0 else diff
     if grid:
         assert tuple(gpu["g"]["dims"]) == tuple(orc["g"]["dims"])
         for k in ("x", "y", "z"):
             assert np.array_equal(gpu["g"][k], orc["g"][k]), f"grid axis {k} not bit-identical"
-        errs["grid_mass"] = assert_close("grid mass", gpu["g"]["mass"], orc["g"]["mass"], rel)
-        errs["grid_v"] = assert_close("grid v", gpu["g"]["v"], orc["g"]["v"], rel)
-        errs["grid_flip"] = assert_close("grid flip", gpu["g"]["flip"], orc["g"]["flip"], rel)
+        errs["grid_mass"] = assert_close("grid mass", gpu["g"]["mass"], orc["g"]["mass"], rel, rep)
+        errs["grid_v"] = assert_close("grid v", gpu["g"]["v"], orc["g"]["v"], rel, rep)
+        errs["grid_flip"] = assert_close("grid flip", gpu["g"]["flip"], orc["g"]["flip"], rel, rep)
+    bad = [r for r in rep if not r[3]]
+    assert not bad, "parity failures: " + "; ".join(f"{n}: {e:.3e} > {t:.1e}" for n, e, t, _ in bad) + \
+        " | all: " + ", ".join(f"{n}={e:.1e}" for n, e, _, _ in rep)
     return errs
