@@ -59,8 +59,14 @@ def oracle_sensitivity(scene, nsteps, ulps=4.0, seed=11):
     if scene.B is not None:
         sc.B = scene.B * (1.0 + eps * rng.choice([-1.0, 1.0], size=scene.B.shape))
     a, b = run_oracle(scene, nsteps), run_oracle(sc, nsteps)
-    return {k: np.abs(a["p"]["scalars"][:, i] - b["p"]["scalars"][:, i]).max()
-            for i, k in enumerate(__import__("matter_tests_b200.abi", fromlist=["SCALARS"]).SCALARS)}
+    from matter_tests_b200.abi import SCALARS
+    out = {k: np.abs(a["p"]["scalars"][:, i] - b["p"]["scalars"][:, i]).max() for i, k in enumerate(SCALARS)}
+    for k in ("x", "v", "F", "B", "pic", "flip"):
+        out[k] = np.abs(a["p"][k] - b["p"][k]).max()
+    if tuple(a["g"]["dims"]) == tuple(b["g"]["dims"]):
+        for k in ("mass", "v", "flip"):
+            out["grid " + k] = np.abs(a["g"][k] - b["g"][k]).max()
+    return out
 
 
 def rel_err(a, b):
@@ -73,8 +79,11 @@ def rel_err(a, b):
     return diff / scale
 
 
-def assert_close(name, a, b, rel, report=None):
+def assert_close(name, a, b, rel, report=None, allowance=0.0):
     e = rel_err(a, b)
+    if allowance:
+        scale = np.abs(np.asarray(b, dtype=np.float64)).max(initial=0.0)
+        e = max(0.0, np.abs(np.asarray(a) - np.asarray(b)).max(initial=0.0) - allowance) / (scale or 1.0)
     ok = bool(np.all(np.isfinite(a) == np.isfinite(b))) and e <= rel
     if report is not None:
         report.append((name, e, rel, ok))
@@ -86,10 +95,12 @@ def assert_close(name, a, b, rel, report=None):
 
 def compare_states(gpu, orc, rel=1e-10, fields=("x", "v", "F", "B", "pic", "flip"), grid=True, sens=None,
                    sens_factor=100.0):
-    """State fields (x, v, F, B, pic, flip, grid mass/v/flip, clock) must agree
-    to `rel` of the field's scale.  The six plastic scalars must agree to
-    `rel` of the field's scale plus sens_factor times the oracle's own
-    sensitivity `sens` (oracle_sensitivity) when it is given."""
+    """Every field must agree to `rel` of its scale plus, when `sens` is given,
+    sens_factor times the oracle's own spread under a few-ulp input
+    perturbation (oracle_sensitivity).  One-step tests use rel = 1e-10, where
+    that spread is ~1e-15 for the state fields; over several steps friction
+    and yield thresholds make some grid nodes and plastic scalars
+    discontinuous in their inputs, and the allowance measures exactly that."""
     errs = {}
     assert gpu["c"]["step"] == orc["c"]["step"], (gpu["c"], orc["c"])
     assert gpu["c"]["frame"] == orc["c"]["frame"]
@@ -98,9 +109,10 @@ def compare_states(gpu, orc, rel=1e-10, fields=("x", "v", "F", "B", "pic", "flip
     rep = []
     errs["time"] = assert_close("time", gpu["c"]["time"], orc["c"]["time"], rel, rep)
     errs["dt"] = assert_close("dt", gpu["c"]["dt"], orc["c"]["dt"], rel, rep)
+    allow = (lambda k: sens_factor * sens.get(k, 0.0)) if sens is not None else (lambda k: 0.0)
     for k in fields:
         if k in gpu["p"]:
-            errs[k] = assert_close(k, gpu["p"][k], orc["p"][k], rel, rep)
+            errs[k] = assert_close(k, gpu["p"][k], orc["p"][k], rel, rep, allow(k))
     from matter_tests_b200.abi import SCALARS
     for i, k in enumerate(SCALARS):
         a, b = gpu["p"]["scalars"][:, i], orc["p"]["scalars"][:, i]
@@ -114,9 +126,9 @@ def compare_states(gpu, orc, rel=1e-10, fields=("x", "v", "F", "B", "pic", "flip
         assert tuple(gpu["g"]["dims"]) == tuple(orc["g"]["dims"])
         for k in ("x", "y", "z"):
             assert np.array_equal(gpu["g"][k], orc["g"][k]), f"grid axis {k} not bit-identical"
-        errs["grid_mass"] = assert_close("grid mass", gpu["g"]["mass"], orc["g"]["mass"], rel, rep)
-        errs["grid_v"] = assert_close("grid v", gpu["g"]["v"], orc["g"]["v"], rel, rep)
-        errs["grid_flip"] = assert_close("grid flip", gpu["g"]["flip"], orc["g"]["flip"], rel, rep)
+        errs["grid_mass"] = assert_close("grid mass", gpu["g"]["mass"], orc["g"]["mass"], rel, rep, allow("grid mass"))
+        errs["grid_v"] = assert_close("grid v", gpu["g"]["v"], orc["g"]["v"], rel, rep, allow("grid v"))
+        errs["grid_flip"] = assert_close("grid flip", gpu["g"]["flip"], orc["g"]["flip"], rel, rep, allow("grid flip"))
     bad = [r for r in rep if not r[3]]
     assert not bad, "parity failures: " + "; ".join(f"{n}: {e:.3e} > {t:.1e}" for n, e, t, _ in bad) + \
         " | all: " + ", ".join(f"{n}={e:.1e}" for n, e, _, _ in rep)
