@@ -296,11 +296,11 @@ int enqueue_step_t(mtr_ctx* c, int parity) {
     mark(c, "k_g2p_musl");
     k_musl_norm<D><<<gblocks, 256, 0, st>>>(A);
     mark(c, "k_musl_norm");
-    k_defgrad<D, DEG><<<pblocks, 128, 0, st>>>(A, perm);
+    k_defgrad_t<D, DEG><<<c->cap_tiles, kChunk, 0, st>>>(A, perm);
     mark(c, "k_defgrad");
     n += 3;
   } else {
-    k_g2p<D, DEG><<<pblocks, 128, 0, st>>>(A, perm);
+    k_g2p_t<D, DEG><<<c->cap_tiles, kChunk, 0, st>>>(A, perm);
     ++n;
     mark(c, "k_g2p");
   }

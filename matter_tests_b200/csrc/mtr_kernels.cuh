@@ -659,23 +659,14 @@ __global__ void __launch_bounds__(kChunk) k_p2g_w(StepArgs A, const uint32_t* __
   const bool apic = P.flip_ratio < 0;
   const bool mibf = P.use_mibf;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // the stencil nodes this lane owns
-  int ix0, iy, iz;
-  int kbeg, kend;
-  if constexpr (D == 3) {
-    ix0 = lane >> 4;  // nodes (ix0, iy, iz) and (ix0 + 2, iy, iz)
-    iy = (lane >> 2) & 3;
-    iz = lane & 3;
-    kbeg = warp * 32;
-    kend = kbeg + 32;
-  } else {
-    ix0 = (lane & 15) >> 2;  // one node (ix0, iy); a half warp per particle run
-    iy = lane & 3;
-    iz = 0;
-    kbeg = warp * 32 + (lane >> 4) * 16;
-    kend = kbeg + 16;
-  }
-  constexpr int NH = D == 3 ? 2 : 1;
+  // Lane groups: 3D, 16 lanes per particle (a lane owns the (iy, iz) column
+  // and its 4 ix nodes), two groups of 16 particles per warp and chunk; 2D,
+  // 4 lanes per particle (a lane owns iy and its 4 ix nodes), eight groups of 4.
+  constexpr int LPP = D == 3 ? 16 : 4;
+  const int q = lane % LPP;
+  const int iy = D == 3 ? (q >> 2) : q;
+  const int iz = D == 3 ? (q & 3) : 0;
+  const int kbeg = warp * 32 + (lane / LPP) * LPP, kend = kbeg + LPP;
   for (uint32_t c0 = pb; c0 < pe; c0 += kChunk) {
     {  // phase 1: stage one particle per thread
       const uint32_t s = c0 + threadIdx.x;
@@ -717,19 +708,18 @@ __global__ void __launch_bounds__(kChunk) k_p2g_w(StepArgs A, const uint32_t* __
       S.lb = packed;
     }
     __syncthreads();
-    {  // phase 2: lanes own nodes, registers accumulate per cell
-      double acc[NH][NCH];
+    {  // phase 2: a lane owns one (iy, iz) stencil column and its 4 ix nodes
+      double acc[4][NCH];
 #pragma unroll
-      for (int h = 0; h < NH; ++h)
+      for (int h = 0; h < 4; ++h)
 #pragma unroll
         for (int ch = 0; ch < NCH; ++ch) acc[h][ch] = 0.0;
       int cur = -1;
       auto flush = [&]() {
         const int lbx = cur & 15, lby = (cur >> 4) & 15, lbz = cur >> 8;
 #pragma unroll
-        for (int h = 0; h < NH; ++h) {
-          const int ix = ix0 + 2 * h;
-          const int node = D == 3 ? ((lbx + ix) * PN + (lby + iy)) * PN + (lbz + iz) : (lbx + ix) * PN + (lby + iy);
+        for (int h = 0; h < 4; ++h) {
+          const int node = D == 3 ? ((lbx + h) * PN + (lby + iy)) * PN + (lbz + iz) : (lbx + h) * PN + (lby + iy);
 #pragma unroll
           for (int ch = 0; ch < NCH; ++ch) {
             if (acc[h][ch] != 0.0) atomicAdd(&patch[ch][node], acc[h][ch]);
@@ -746,54 +736,59 @@ __global__ void __launch_bounds__(kChunk) k_p2g_w(StepArgs A, const uint32_t* __
           cur = lbp;
         }
         const int lbx = lbp & 15, lby = (lbp >> 4) & 15, lbz = lbp >> 8;
+        // tensor-product factors of this lane's column
         const double wy = S.w[4 + iy], dwy = S.dw[4 + iy];
-        const double wz = D == 3 ? S.w[8 + iz] : 1.0, dwz = D == 3 ? S.dw[8 + iz] : 0.0;
-        double xp[D], vp[D], tau[NS];
+        double wyz, G0, G1, G2 = 0.0;
+        if constexpr (D == 3) {
+          const double wz = S.w[8 + iz], dwz = S.dw[8 + iz];
+          wyz = wy * wz;
+          G0 = wyz * ioh;
+          G1 = dwy * wz * ioh;
+          G2 = wy * dwz * ioh;
+        } else {
+          wyz = wy;
+          G0 = wy * ioh;
+          G1 = dwy * ioh;
+        }
+        // force f_a = tau_a . grad w = dwx * Pf_a + wx * Qf_a
+        double Pf[D], Qf[D];
 #pragma unroll
         for (int a = 0; a < D; ++a) {
-          xp[a] = S.x[a];
-          vp[a] = S.v[a];
+          Pf[a] = sym_at<D>(S.tau, a, 0) * G0;
+          double q = sym_at<D>(S.tau, a, 1) * G1;
+          if constexpr (D == 3) q += sym_at<D>(S.tau, a, 2) * G2;
+          Qf[a] = q;
         }
+        // momentum per weight: v_a + apicD B_a . (x_i - x_p) = Tm_a + Sm_a * pdx
+        const double pdy = crd[1][lby + iy] - S.x[1];
+        const double pdz = D == 3 ? crd[2][lbz + iz] - S.x[D - 1] : 0.0;
+        double Tm[D], Sm[D];
 #pragma unroll
-        for (int q = 0; q < NS; ++q) tau[q] = S.tau[q];
-#pragma unroll
-        for (int h = 0; h < NH; ++h) {
-          const int ix = ix0 + 2 * h;
-          const double wx = S.w[ix], dwx = S.dw[ix];
-          const double wxy = wx * wy;
-          const double weight = D == 3 ? wxy * wz : wxy;
-          if (weight > 1e-25) {
-            acc[h][0] += weight;
-            double pd[3] = {crd[0][lbx + ix] - xp[0], crd[1][lby + iy] - xp[1], D == 3 ? crd[2][lbz + iz] - xp[D - 1] : 0.0};
-#pragma unroll
-            for (int a = 0; a < D; ++a) {
-              double m = vp[a] * weight;
-              if (apic) {
-                double bv = S.B[a * D] * pd[0];
-#pragma unroll
-                for (int c = 1; c < D; ++c) bv += S.B[a * D + c] * pd[c];
-                m += bv * apicD * weight;
-              }
-              acc[h][1 + a] += m;
-            }
-            if (mibf) acc[h][1 + 2 * D] += S.mui * weight;
-          }
-          double g[3];
-          if constexpr (D == 3) {
-            g[0] = dwx * wy * wz * ioh;
-            g[1] = dwy * wx * wz * ioh;
-            g[2] = dwz * wx * wy * ioh;
+        for (int a = 0; a < D; ++a) {
+          if (apic) {
+            double byz = S.B[a * D + 1] * pdy;
+            if constexpr (D == 3) byz += S.B[a * D + 2] * pdz;
+            Tm[a] = S.v[a] + apicD * byz;
+            Sm[a] = apicD * S.B[a * D];
           } else {
-            g[0] = dwx * wy * ioh;
-            g[1] = dwy * wx * ioh;
+            Tm[a] = S.v[a];
+            Sm[a] = 0.0;
+          }
+        }
+        const double xp0 = S.x[0], mui = S.mui;
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          const double wx = S.w[h], dwx = S.dw[h];
+          const double weight = wx * wyz;
+          if (weight > 1e-25) {
+            const double pdx = crd[0][lbx + h] - xp0;
+            acc[h][0] += weight;
+#pragma unroll
+            for (int a = 0; a < D; ++a) acc[h][1 + a] += weight * (Tm[a] + Sm[a] * pdx);
+            if (mibf) acc[h][1 + 2 * D] += mui * weight;
           }
 #pragma unroll
-          for (int a = 0; a < D; ++a) {
-            double f = sym_at<D>(tau, a, 0) * g[0];
-#pragma unroll
-            for (int c = 1; c < D; ++c) f += sym_at<D>(tau, a, c) * g[c];
-            acc[h][1 + D + a] += f;
-          }
+          for (int a = 0; a < D; ++a) acc[h][1 + D + a] += dwx * Pf[a] + wx * Qf[a];
         }
       }
       if (cur >= 0) flush();
@@ -1222,14 +1217,293 @@ __global__ void __launch_bounds__(128) k_g2p_musl(StepArgs A, const uint32_t* __
   }
 }
 
-// MUSL G2P + re-scatter, two-phase form of k_g2p_musl: phase 1 (thread per
-// particle) gathers, blends and writes the particle and stages v_new, B_new
-// and the weights; phase 2 (warp per run, lanes owning stencil nodes)
-// accumulates v_p + B D^-1 (x_i - x_p) per cell in registers.
+// ---------------------------------------------------------------------------
+// Tile-structured gathers.  A tile block first copies the node values its
+// particles' stencils can reach (the PN^D patch of the tile) from the node
+// arrays into shared memory, then every particle gathers from there.
+// ---------------------------------------------------------------------------
+template <int D>
+__device__ __forceinline__ void load_tile_setup(const StepArgs& A, const StepHeader* H, uint32_t t, int (&n0)[3],
+                                                double (*crd)[Tiling<D>::PN]) {
+  constexpr int PN = Tiling<D>::PN, TB = Tiling<D>::TB;
+  int tc[3];
+  tile_coords<D>(H, t, tc);
+  n0[0] = tc[0] * TB - 1;
+  n0[1] = tc[1] * TB - 1;
+  n0[2] = D == 3 ? tc[2] * TB - 1 : 0;
+  for (int i = threadIdx.x; i < D * PN; i += blockDim.x) {
+    const int a = i / PN, o = i % PN;
+    const int g = n0[a] + o;
+    const double* ax = a == 0 ? A.gx : (a == 1 ? A.gy : A.gz);
+    crd[a][o] = (g >= 0 && g < (int)H->N[a]) ? ax[g] : 0.0;
+  }
+}
+
+// copies NF fields of D components each, src[f] = [D][cap] node arrays
+template <int D, int NF>
+__device__ __forceinline__ void load_node_patch(const StepArgs& A, const StepHeader* H, const int (&n0)[3],
+                                                const double* const (&src)[NF], double* dst /*[NF*D][NODES]*/) {
+  constexpr int PN = Tiling<D>::PN, NODES = Tiling<D>::NODES;
+  const uint32_t cap = A.cap_nodes;
+  for (int n = threadIdx.x; n < NODES; n += blockDim.x) {
+    int li, lj, lk;
+    if constexpr (D == 3) {
+      lk = n % PN;
+      lj = (n / PN) % PN;
+      li = n / (PN * PN);
+    } else {
+      lk = 0;
+      lj = n % PN;
+      li = n / PN;
+    }
+    const int gi = n0[0] + li, gj = n0[1] + lj, gk = n0[2] + lk;
+    const bool in = gi >= 0 && gj >= 0 && gk >= 0 && gi < (int)H->N[0] && gj < (int)H->N[1] && gk < (int)H->N[2];
+    const uint32_t l = in ? node_index(H, gi, gj, gk) : 0u;
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+      for (int a = 0; a < D; ++a) dst[(f * D + a) * NODES + n] = in ? src[f][(size_t)a * cap + l] : 0.0;
+  }
+}
+
+// G2P gather (g2p.cpp:24-77) and velocity gradient (deformation_update.cpp:17-40)
+// from a shared node patch; lb = stencil base relative to the patch origin.
+// Sums are factorised over the tensor-product stencil.
+template <int D, int DEG, bool GRADV>
+__device__ __forceinline__ void gather_patch(const double* pv, const double* pf, const double (*crd)[Tiling<D>::PN],
+                                             const int (&lb)[3], const double (&xp)[3], double ioh, double (&pic)[3],
+                                             double (&Bp)[D][D], double (&flp)[3], double (&gv)[D][D], bool want_b,
+                                             bool want_flip) {
+  constexpr int PN = Tiling<D>::PN, NODES = Tiling<D>::NODES;
+  double w[3][4], dw[3][4], pd[3][4];
+#pragma unroll
+  for (int a = 0; a < D; ++a)
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+      const double c = crd[a][lb[a] + o];
+      const double u = (xp[a] - c) * ioh;
+      w[a][o] = bspline_N<DEG>(u);
+      dw[a][o] = GRADV ? bspline_dN<DEG>(u) : 0.0;
+      pd[a][o] = c - xp[a];
+    }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) pic[a] = flp[a] = 0.0;
+#pragma unroll
+  for (int r = 0; r < D; ++r)
+#pragma unroll
+    for (int c = 0; c < D; ++c) Bp[r][c] = gv[r][c] = 0.0;
+  constexpr int KN = D == 3 ? 4 : 1;
+#pragma unroll
+  for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const double wxy = w[0][ii] * w[1][jj];
+      const double gx_ = dw[0][ii] * w[1][jj], gy_ = w[0][ii] * dw[1][jj];
+#pragma unroll
+      for (int kk = 0; kk < KN; ++kk) {
+        const int node = D == 3 ? ((lb[0] + ii) * PN + (lb[1] + jj)) * PN + (lb[2] + kk) : (lb[0] + ii) * PN + (lb[1] + jj);
+        const double weight = D == 3 ? wxy * w[2][kk] : wxy;
+        double vi[D];
+#pragma unroll
+        for (int a = 0; a < D; ++a) vi[a] = pv[a * NODES + node];
+#pragma unroll
+        for (int a = 0; a < D; ++a) pic[a] += vi[a] * weight;
+        if (want_b) {
+          double wpd[3] = {weight * pd[0][ii], weight * pd[1][jj], D == 3 ? weight * pd[2][kk] : 0.0};
+#pragma unroll
+          for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) Bp[r][c] += vi[r] * wpd[c];
+        }
+        if (want_flip) {
+#pragma unroll
+          for (int a = 0; a < D; ++a) flp[a] += pf[a * NODES + node] * weight;
+        }
+        if (GRADV) {
+          double g[3];
+          if constexpr (D == 3) {
+            g[0] = gx_ * w[2][kk];
+            g[1] = gy_ * w[2][kk];
+            g[2] = wxy * dw[2][kk];
+          } else {
+            g[0] = gx_;
+            g[1] = gy_;
+          }
+#pragma unroll
+          for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) gv[r][c] += vi[r] * g[c];
+        }
+      }
+    }
+  if (GRADV) {
+#pragma unroll
+    for (int r = 0; r < D; ++r)
+#pragma unroll
+      for (int c = 0; c < D; ++c) gv[r][c] *= ioh;
+  }
+}
+
+// local stencil base of a particle in its tile patch; false if outside
+template <int D>
+__device__ __forceinline__ bool local_base(const StepHeader* H, const double (&xp)[3], double ioh, const int (&n0)[3],
+                                           bool clamp, int (&lb)[3]) {
+  constexpr int PN = Tiling<D>::PN;
+  bool ok = true;
+  lb[0] = lb[1] = lb[2] = 0;
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    int b = (int)floor((xp[a] - H->org[a]) * ioh) - 1;
+    if (clamp) b = b < 0 ? 0 : b;
+    lb[a] = b - n0[a];
+    if (b < 0 || lb[a] < 0 || lb[a] > PN - 4 || b + 3 >= (int)H->N[a]) ok = false;
+  }
+  return ok;
+}
+
+// USL: G2P + deformation update + return mapping + position update, one
+// block per tile, node patch in shared memory.
+template <int D, int DEG>
+__global__ void __launch_bounds__(kChunk) k_g2p_t(StepArgs A, const uint32_t* __restrict__ perm) {
+  using TL = Tiling<D>;
+  constexpr int PN = TL::PN, NODES = TL::NODES;
+  StepHeader* H = A.H;
+  if (step_inactive(H)) return;
+  const uint32_t t = blockIdx.x;
+  if (t >= H->ntiles) return;
+  const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
+  if (pb >= pe) return;
+  const DevParams& P = *A.P;
+  __shared__ double pv[2 * D * NODES];
+  __shared__ double crd[3][PN];
+  int n0[3];
+  load_tile_setup<D>(A, H, t, n0, crd);
+  const double* const src[2] = {A.nv, A.nflip};
+  load_node_patch<D, 2>(A, H, n0, src, pv);
+  __syncthreads();
+  const uint32_t Np = A.Np;
+  const double dt = H->dt, fr = P.flip_ratio, ioh = P.one_over_dx;
+  uint32_t flags = 0;
+  bool any_plastic = false;
+  for (uint32_t s = pb + threadIdx.x; s < pe; s += blockDim.x) {
+    const uint32_t j = perm[s];
+    PLoad<D> p;
+    load_particle<D>(A.in, Np, j, p);
+    double pic[3], flp[3], Bp[D][D], gv[D][D];
+    int lb[3];
+    if (local_base<D>(H, p.x, ioh, n0, false, lb)) {
+      gather_patch<D, DEG, true>(pv, pv + D * NODES, crd, lb, p.x, ioh, pic, Bp, flp, gv, fr < 0, fr >= -1);
+    } else {
+      raise_status(H, MTR_STATUS_STENCIL_OOB, p.id);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) pic[a] = flp[a] = 0.0;
+#pragma unroll
+      for (int r = 0; r < D; ++r)
+#pragma unroll
+        for (int c = 0; c < D; ++c) Bp[r][c] = gv[r][c] = 0.0;
+    }
+    uint32_t f = 0;
+    bool plastic = false;
+    defgrad_and_store<D>(A, s, dt, p, gv, f, plastic);
+    flags |= f;
+    if (f) raise_status(H, f, p.id);
+    any_plastic |= plastic;
+    if (plastic) atomicAdd(&H->plastic_count, 1ull);
+    double xn[3], vn[3];
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      xn[a] = p.x[a] + dt * pic[a];
+      vn[a] = blend_v(fr, p.v[a], flp[a], pic[a]);
+    }
+    if (P.change_particle_positions && xn[0] > 0.8) {  // position_update.cpp:35-41
+      xn[0] = -0.1;
+      xn[1] += 0.27;
+    }
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      A.out.x[(size_t)a * Np + s] = xn[a];
+      A.out.v[(size_t)a * Np + s] = vn[a];
+    }
+#pragma unroll
+    for (int r = 0; r < D; ++r)
+#pragma unroll
+      for (int c = 0; c < D; ++c) A.out.B[(size_t)(r * D + c) * Np + s] = (fr < 0) ? Bp[r][c] : 0.0;
+    A.out.id[s] = p.id;
+    if (P.store_pic_flip) {
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        A.pic[(size_t)a * Np + s] = pic[a];
+        A.flip[(size_t)a * Np + s] = (fr >= -1) ? flp[a] : 0.0;
+      }
+    }
+  }
+}
+
+// MUSL: deformation update from the normalised re-projected velocity v2 and
+// the old positions (deformation_update.cpp:6), then the return mapping.
+template <int D, int DEG>
+__global__ void __launch_bounds__(kChunk) k_defgrad_t(StepArgs A, const uint32_t* __restrict__ perm) {
+  using TL = Tiling<D>;
+  constexpr int PN = TL::PN, NODES = TL::NODES;
+  StepHeader* H = A.H;
+  if (step_inactive(H)) return;
+  const uint32_t t = blockIdx.x;
+  if (t >= H->ntiles) return;
+  const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
+  if (pb >= pe) return;
+  __shared__ double pv[D * NODES];
+  __shared__ double crd[3][PN];
+  int n0[3];
+  load_tile_setup<D>(A, H, t, n0, crd);
+  const double* const src[1] = {A.v2};
+  load_node_patch<D, 1>(A, H, n0, src, pv);
+  __syncthreads();
+  const uint32_t Np = A.Np;
+  const double dt = H->dt, ioh = A.P->one_over_dx;
+  for (uint32_t s = pb + threadIdx.x; s < pe; s += blockDim.x) {
+    const uint32_t j = perm[s];
+    PLoad<D> p;
+    load_particle<D>(A.in, Np, j, p);
+    double pic[3], flp[3], Bp[D][D], gv[D][D];
+    int lb[3];
+    if (local_base<D>(H, p.x, ioh, n0, false, lb)) {
+      gather_patch<D, DEG, true>(pv, nullptr, crd, lb, p.x, ioh, pic, Bp, flp, gv, false, false);
+    } else {
+      raise_status(H, MTR_STATUS_STENCIL_OOB, p.id);
+#pragma unroll
+      for (int r = 0; r < D; ++r)
+#pragma unroll
+        for (int c = 0; c < D; ++c) gv[r][c] = 0.0;
+    }
+    uint32_t f = 0;
+    bool plastic = false;
+    defgrad_and_store<D>(A, s, dt, p, gv, f, plastic);
+    if (f) raise_status(H, f, p.id);
+    if (plastic) atomicAdd(&H->plastic_count, 1ull);
+  }
+}
+
+// MUSL (musl.cpp:6-96), one block per tile.  Phase 1 (thread per particle):
+// gather pic/B/flip from the shared node patch, blend v, write x + dt pic, v,
+// B; stage v_new, B_new and the re-scatter weights.  Phase 2 (lane groups
+// owning stencil columns): accumulate v_p + B D^-1 (x_i - x_p) per cell in
+// registers, add once per cell to the shared re-projection patch.
+template <int D>
+struct MStage {
+  double x[D], v[D], B[D * D], w[D * 4];
+  int lb;
+  int pad;
+};
+
+template <int D>
+constexpr size_t musl_smem_bytes() {
+  return sizeof(double) * ((3 * D) * Tiling<D>::NODES + 3 * Tiling<D>::PN) + sizeof(MStage<D>) * kChunk;
+}
+
 template <int D, int DEG>
 __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgs A, const uint32_t* __restrict__ perm) {
   using TL = Tiling<D>;
-  constexpr int PN = TL::PN, NODES = TL::NODES, TB = TL::TB;
+  constexpr int PN = TL::PN, NODES = TL::NODES;
   StepHeader* H = A.H;
   if (step_inactive(H)) return;
   const uint32_t t = blockIdx.x;
@@ -1238,43 +1512,29 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgs A, const uint32_
   if (pb >= pe) return;
   const DevParams& P = *A.P;
   extern __shared__ double smem[];
-  double(*patch)[NODES] = reinterpret_cast<double(*)[NODES]>(smem);
-  double(*crd)[PN] = reinterpret_cast<double(*)[PN]>(smem + D * NODES);
-  PStage<D>* st = reinterpret_cast<PStage<D>*>(smem + D * NODES + 3 * PN);
-  int tc[3];
-  tile_coords<D>(H, t, tc);
-  const int n0[3] = {tc[0] * TB - 1, tc[1] * TB - 1, D == 3 ? tc[2] * TB - 1 : 0};
-  for (int i = threadIdx.x; i < D * NODES; i += blockDim.x) (&patch[0][0])[i] = 0.0;
-  for (int i = threadIdx.x; i < D * PN; i += blockDim.x) {
-    const int a = i / PN, o = i % PN;
-    const int g = n0[a] + o;
-    const double* ax = a == 0 ? A.gx : (a == 1 ? A.gy : A.gz);
-    crd[a][o] = (g >= 0 && g < (int)H->N[a]) ? ax[g] : 0.0;
-  }
+  double* pv = smem;                                              // [2D][NODES] node v, flip
+  double(*vsum)[NODES] = reinterpret_cast<double(*)[NODES]>(smem + 2 * D * NODES);  // [D][NODES]
+  double(*crd)[PN] = reinterpret_cast<double(*)[PN]>(smem + 3 * D * NODES);
+  MStage<D>* st = reinterpret_cast<MStage<D>*>(smem + 3 * D * NODES + 3 * PN);
+  int n0[3];
+  load_tile_setup<D>(A, H, t, n0, crd);
+  const double* const src[2] = {A.nv, A.nflip};
+  load_node_patch<D, 2>(A, H, n0, src, pv);
+  for (int i = threadIdx.x; i < D * NODES; i += blockDim.x) (&vsum[0][0])[i] = 0.0;
   __syncthreads();
   const uint32_t Np = A.Np;
   const double dt = H->dt, fr = P.flip_ratio, ioh = P.one_over_dx, apicD = P.apicDinverse;
   const bool apic = fr < 0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int ix0, iy, iz, kbeg, kend;
-  if constexpr (D == 3) {
-    ix0 = lane >> 4;
-    iy = (lane >> 2) & 3;
-    iz = lane & 3;
-    kbeg = warp * 32;
-    kend = kbeg + 32;
-  } else {
-    ix0 = (lane & 15) >> 2;
-    iy = lane & 3;
-    iz = 0;
-    kbeg = warp * 32 + (lane >> 4) * 16;
-    kend = kbeg + 16;
-  }
-  constexpr int NH = D == 3 ? 2 : 1;
+  constexpr int LPP = D == 3 ? 16 : 4;
+  const int q = lane % LPP;
+  const int iy = D == 3 ? (q >> 2) : q;
+  const int iz = D == 3 ? (q & 3) : 0;
+  const int kbeg = warp * 32 + (lane / LPP) * LPP, kend = kbeg + LPP;
   for (uint32_t c0 = pb; c0 < pe; c0 += kChunk) {
     {  // phase 1
       const uint32_t s = c0 + threadIdx.x;
-      PStage<D>& S = st[threadIdx.x];
+      MStage<D>& S = st[threadIdx.x];
       int packed = -1;
       if (s < pe) {
         const uint32_t j = perm[s];
@@ -1286,7 +1546,11 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgs A, const uint32_
         }
         const uint32_t pid = A.in.id[j];
         double pic[3], flp[3], Bp[D][D], gv[D][D];
-        if (!gather<D, DEG, false>(A, H, A.nv, xp, pic, Bp, flp, gv, apic, fr >= -1)) {
+        int lb[3];
+        const bool ok = local_base<D>(H, xp, ioh, n0, false, lb);
+        if (ok) {
+          gather_patch<D, DEG, false>(pv, pv + D * NODES, crd, lb, xp, ioh, pic, Bp, flp, gv, apic, fr >= -1);
+        } else {
           raise_status(H, MTR_STATUS_STENCIL_OOB, pid);
 #pragma unroll
           for (int a = 0; a < 3; ++a) pic[a] = flp[a] = 0.0;
@@ -1320,50 +1584,41 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgs A, const uint32_
           }
         }
         // re-scatter stencil, base clamped at zero like P2G (musl.cpp:35-40)
-        int lb[3] = {0, 0, 0};
-        bool oob = false;
-#pragma unroll
-        for (int a = 0; a < D; ++a) {
-          int b = (int)floor((xp[a] - H->org[a]) * ioh) - 1;
-          b = b < 0 ? 0 : b;
-          lb[a] = b - n0[a];
-          if (lb[a] < 0 || lb[a] > PN - 4) oob = true;
-        }
-        if (oob) {
-          raise_status(H, MTR_STATUS_STENCIL_OOB, pid);
-        } else {
+        int lbs[3];
+        if (ok && local_base<D>(H, xp, ioh, n0, true, lbs)) {
 #pragma unroll
           for (int a = 0; a < D; ++a)
 #pragma unroll
-            for (int o = 0; o < 4; ++o) S.w[a * 4 + o] = bspline_N<DEG>((xp[a] - crd[a][lb[a] + o]) * ioh);
-          packed = lb[0] | (lb[1] << 4) | (lb[2] << 8);
+            for (int o = 0; o < 4; ++o) S.w[a * 4 + o] = bspline_N<DEG>((xp[a] - crd[a][lbs[a] + o]) * ioh);
+          packed = lbs[0] | (lbs[1] << 4) | (lbs[2] << 8);
+        } else if (ok) {
+          raise_status(H, MTR_STATUS_STENCIL_OOB, pid);
         }
       }
       S.lb = packed;
     }
     __syncthreads();
     {  // phase 2
-      double acc[NH][D];
+      double acc[4][D];
 #pragma unroll
-      for (int h = 0; h < NH; ++h)
+      for (int h = 0; h < 4; ++h)
 #pragma unroll
         for (int a = 0; a < D; ++a) acc[h][a] = 0.0;
       int cur = -1;
       auto flush = [&]() {
         const int lbx = cur & 15, lby = (cur >> 4) & 15, lbz = cur >> 8;
 #pragma unroll
-        for (int h = 0; h < NH; ++h) {
-          const int ix = ix0 + 2 * h;
-          const int node = D == 3 ? ((lbx + ix) * PN + (lby + iy)) * PN + (lbz + iz) : (lbx + ix) * PN + (lby + iy);
+        for (int h = 0; h < 4; ++h) {
+          const int node = D == 3 ? ((lbx + h) * PN + (lby + iy)) * PN + (lbz + iz) : (lbx + h) * PN + (lby + iy);
 #pragma unroll
           for (int a = 0; a < D; ++a) {
-            if (acc[h][a] != 0.0) atomicAdd(&patch[a][node], acc[h][a]);
+            if (acc[h][a] != 0.0) atomicAdd(&vsum[a][node], acc[h][a]);
             acc[h][a] = 0.0;
           }
         }
       };
       for (int k = kbeg; k < kend; ++k) {
-        const PStage<D>& S = st[k];
+        const MStage<D>& S = st[k];
         const int lbp = S.lb;
         if (lbp < 0) continue;
         if (lbp != cur) {
@@ -1371,27 +1626,30 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgs A, const uint32_
           cur = lbp;
         }
         const int lbx = lbp & 15, lby = (lbp >> 4) & 15, lbz = lbp >> 8;
-        const double wy = S.w[4 + iy];
-        const double wz = D == 3 ? S.w[8 + iz] : 1.0;
+        const double wyz = D == 3 ? S.w[4 + iy] * S.w[8 + iz] : S.w[4 + iy];
+        const double pdy = crd[1][lby + iy] - S.x[1];
+        const double pdz = D == 3 ? crd[2][lbz + iz] - S.x[D - 1] : 0.0;
+        double Tm[D], Sm[D];
 #pragma unroll
-        for (int h = 0; h < NH; ++h) {
-          const int ix = ix0 + 2 * h;
-          const double wxy = S.w[ix] * wy;
-          const double weight = D == 3 ? wxy * wz : wxy;
-          if (!(weight > 1e-25)) continue;
-          double pd[3] = {crd[0][lbx + ix] - S.x[0], crd[1][lby + iy] - S.x[1],
-                          D == 3 ? crd[2][lbz + iz] - S.x[D - 1] : 0.0};
-#pragma unroll
-          for (int a = 0; a < D; ++a) {
-            double m = S.v[a] * weight;
-            if (apic) {
-              double bv = S.B[a * D] * pd[0];
-#pragma unroll
-              for (int c = 1; c < D; ++c) bv += S.B[a * D + c] * pd[c];
-              m += bv * apicD * weight;
-            }
-            acc[h][a] += m;
+        for (int a = 0; a < D; ++a) {
+          if (apic) {
+            double byz = S.B[a * D + 1] * pdy;
+            if constexpr (D == 3) byz += S.B[a * D + 2] * pdz;
+            Tm[a] = S.v[a] + apicD * byz;
+            Sm[a] = apicD * S.B[a * D];
+          } else {
+            Tm[a] = S.v[a];
+            Sm[a] = 0.0;
           }
+        }
+        const double xp0 = S.x[0];
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          const double weight = S.w[h] * wyz;
+          if (!(weight > 1e-25)) continue;
+          const double pdx = crd[0][lbx + h] - xp0;
+#pragma unroll
+          for (int a = 0; a < D; ++a) acc[h][a] += weight * (Tm[a] + Sm[a] * pdx);
         }
       }
       if (cur >= 0) flush();
@@ -1415,15 +1673,10 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgs A, const uint32_
     const uint32_t l = node_index(H, gi, gj, gk);
 #pragma unroll
     for (int a = 0; a < D; ++a) {
-      const double val = patch[a][n];
+      const double val = vsum[a][n];
       if (val != 0.0) atomicAdd(&A.v2[(size_t)a * cap + l], val);
     }
   }
-}
-
-template <int D>
-constexpr size_t musl_smem_bytes() {
-  return sizeof(double) * (D * Tiling<D>::NODES + 3 * Tiling<D>::PN) + sizeof(PStage<D>) * kChunk;
 }
 
 // musl.cpp:80-95: v2 /= (m_i / m_p) (zero where m_i == 0)
