@@ -666,6 +666,10 @@ __global__ void __launch_bounds__(kChunk) k_p2g_w(StepArgs A, const uint32_t* __
   const int q = lane % LPP;
   const int iy = D == 3 ? (q >> 2) : q;
   const int iz = D == 3 ? (q & 3) : 0;
+  // group g takes the consecutive staged particles [g*LPP, (g+1)*LPP) of the
+  // warp's 32, so groups work on different cells and their flushes rarely
+  // meet on one patch node (interleaving them made both groups flush the same
+  // cell at once, which measured slower despite fewer bank conflicts)
   const int kbeg = warp * 32 + (lane / LPP) * LPP, kend = kbeg + LPP;
   for (uint32_t c0 = pb; c0 < pe; c0 += kChunk) {
     {  // phase 1: stage one particle per thread
@@ -1530,6 +1534,10 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgs A, const uint32_
   const int q = lane % LPP;
   const int iy = D == 3 ? (q >> 2) : q;
   const int iz = D == 3 ? (q & 3) : 0;
+  // group g takes the consecutive staged particles [g*LPP, (g+1)*LPP) of the
+  // warp's 32, so groups work on different cells and their flushes rarely
+  // meet on one patch node (interleaving them made both groups flush the same
+  // cell at once, which measured slower despite fewer bank conflicts)
   const int kbeg = warp * 32 + (lane / LPP) * LPP, kend = kbeg + LPP;
   for (uint32_t c0 = pb; c0 < pe; c0 += kChunk) {
     {  // phase 1
