@@ -35,6 +35,7 @@ extern "C" {
 #define MTR_ERR_TIMEOUT          -5  /* bounded wait for the device expired  */
 #define MTR_ERR_NO_DEVICE        -6  /* no CUDA device is visible            */
 #define MTR_ERR_STATE            -7  /* call out of order (e.g. step before upload) */
+#define MTR_ERR_TOO_LARGE        -8  /* request exceeds a fixed capacity (mtr_p2g_noalloc) */
 
 /* ---- device status flags (mtr_status) ----------------------------------- */
 #define MTR_STATUS_GRID_OVERFLOW   0x0001u /* grid outgrew capacity; host regrows and retries */
@@ -210,6 +211,34 @@ int mtr_use_graphs(mtr_ctx* ctx, int on);
  * in the last step. */
 int mtr_profile(mtr_ctx* ctx, int nsteps, double* slot_ms, const char** slot_names, int max_slots, int* nslots);
 int mtr_active_nodes(mtr_ctx* ctx, uint64_t* active, uint64_t* total);
+
+/* mtr_p2g_noalloc — no counterpart in the reference.  The particle-to-grid
+ * transfer (the P2G of p2g.cpp: grid mass = particle mass * sum of weights,
+ * grid velocity = sum of w (v_p + B_p D^-1 (x_i - x_p)) / sum of w) of one
+ * particle set onto a grid the caller describes, for callers that cannot
+ * allocate device memory where they call it: code being captured into a CUDA
+ * graph, solvers living inside a framework that owns all device memory
+ * through its own pool, real-time loops that must not risk an allocation.
+ * Nothing is allocated: the sort, tile and accumulator scratch lives in one
+ * fixed device array (~10 MB, held by every GPU that loads the library until
+ * exit).  Inputs and outputs are device pointers the caller owns:
+ *   x, v  [dim][Np] component-major; B [dim*dim][Np], entry (r,c) at r*dim+c
+ *         (read only when params->flip_ratio < 0); gx, gy, gz the node
+ *         coordinates per axis (gz unused in 2D); dims = nodes per axis (host);
+ *   grid_mass [G], grid_v [dim][G] with G = dims product, node order
+ *         (i*Ny + j)*Nz + k.
+ * Uses params->dim, spline_deg, dx, flip_ratio, particle_mass.  Runs on
+ * `stream` (cudaStream_t; NULL = legacy default stream) and returns without
+ * synchronising.  More than MTR_NOALLOC_MAX_PARTICLES particles or
+ * MTR_NOALLOC_MAX_NODES nodes returns MTR_ERR_TOO_LARGE.  All calls share the
+ * scratch array: calls that overlap on the GPU race.  The first call on each
+ * device looks the array up (cudaGetSymbolAddress) and must not be inside a
+ * stream capture. */
+#define MTR_NOALLOC_MAX_PARTICLES (1u << 18)
+#define MTR_NOALLOC_MAX_NODES (1u << 17)
+int mtr_p2g_noalloc(const mtr_params* params, const double* x, const double* v, const double* B, uint32_t Np,
+                    const double* gx, const double* gy, const double* gz, const uint32_t dims[3], double* grid_mass,
+                    double* grid_v, void* stream);
 
 void mtr_ctx_destroy(mtr_ctx* ctx);
 

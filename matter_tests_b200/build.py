@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libmatter_gpu.so")
-SOURCES = [os.path.join(HERE, "csrc", "mtr_abi.cu")]
+SOURCES = [os.path.join(HERE, "csrc", "mtr_abi.cu"), os.path.join(HERE, "csrc", "mtr_noalloc.cu")]
 DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))] + \
     [os.path.join(ROOT, "include", "matter_gpu.h")]
 

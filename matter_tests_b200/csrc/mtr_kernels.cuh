@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_hist(StepArgs A, const ui
 }
 
 // Exclusive scan of each digit's row over the blocks; row totals to dtot.
-__global__ void __launch_bounds__(256) k_sort_scan(StepArgs A) {
+static __global__ void __launch_bounds__(256) k_sort_scan(StepArgs A) {
   if (step_inactive(A.H)) return;
   const int dgt = blockIdx.x;
   uint32_t* row = A.hist + (size_t)dgt * A.sort_blocks;
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(256) k_sort_scan(StepArgs A) {
 // Stable scatter.  Elements are ranked round by round (256 at a time, in
 // index order) with warp match + per-warp digit counts, which keeps equal
 // digits in input order.
-__global__ void __launch_bounds__(kSortThreads) k_sort_scatter(StepArgs A, const uint32_t* __restrict__ ksrc,
+static __global__ void __launch_bounds__(kSortThreads) k_sort_scatter(StepArgs A, const uint32_t* __restrict__ ksrc,
                                                                const uint32_t* __restrict__ vsrc, uint32_t* kdst,
                                                                uint32_t* vdst, int shift) {
   if (step_inactive(A.H)) return;
@@ -426,7 +426,7 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_scatter(StepArgs A, const
 // ---------------------------------------------------------------------------
 // 4. tile ranges over the sorted keys
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_tile_ranges(StepArgs A, const uint32_t* __restrict__ skeys) {
+static __global__ void __launch_bounds__(256) k_tile_ranges(StepArgs A, const uint32_t* __restrict__ skeys) {
   if (step_inactive(A.H)) return;
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < A.Np; s += gridDim.x * blockDim.x) {
     const uint32_t t = skeys[s] >> 6;

@@ -25,7 +25,7 @@ struct PScalars {
 };
 
 // MCCRMAExplicit (mcc_rma_explicit.hpp:8-96)
-__device__ bool mcc_rma_explicit(double& p_io, double& q_io, double M, double p0, double beta, double mu, double K,
+__device__ inline bool mcc_rma_explicit(double& p_io, double& q_io, double M, double p0, double beta, double mu, double K,
                                  double rma_prefac) {
   double p = p_io, q = q_io;
   double y = M * M * (p - p0) * (p + beta * p0) + (q * q);
@@ -188,7 +188,7 @@ __device__ bool mcc_rma_implicit(double& p_io, double& q_io, double M, double p0
 
 // Perzyna Newton loop of VMVisc / DPVisc / MCCVisc (plasticity.cpp:197-229,
 // 293-323, 558-588); VMVisc's yield stress depends on delta_gamma (is_vm).
-__device__ double perzyna_newton(const DevParams& P, double dt, double q_trial, double q_yield, bool is_vm,
+__device__ inline double perzyna_newton(const DevParams& P, double dt, double q_trial, double q_yield, bool is_vm,
                                  double eps_pl_dev, uint32_t& flags) {
   const double pe = P.perzyna_exp, pv = P.perzyna_visc, fm = P.f_mu_prefac;
   double delta_gamma = 0.01 * (q_trial - q_yield) / fm;

@@ -21,7 +21,7 @@ EXPORTS = (
     "mtr_ctx_create", "mtr_upload", "mtr_set_objects", "mtr_step", "mtr_run", "mtr_download",
     "mtr_download_pic_flip", "mtr_get_grid", "mtr_get_sort", "mtr_get_plates", "mtr_get_clock",
     "mtr_status", "mtr_clear_status", "mtr_sync", "mtr_stream", "mtr_launch_count", "mtr_keep_pic_flip",
-    "mtr_use_graphs", "mtr_profile", "mtr_active_nodes", "mtr_ctx_destroy", "mtr_last_error",
+    "mtr_use_graphs", "mtr_profile", "mtr_active_nodes", "mtr_ctx_destroy", "mtr_last_error", "mtr_p2g_noalloc",
 )
 
 _lib = None
@@ -63,6 +63,9 @@ def load_library(path=LIB_PATH):
     lib.mtr_use_graphs.argtypes = [C.c_void_p, C.c_int]
     lib.mtr_profile.argtypes = [C.c_void_p, C.c_int, _P, C.POINTER(C.c_char_p), C.c_int, C.POINTER(C.c_int)]
     lib.mtr_active_nodes.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    lib.mtr_p2g_noalloc.argtypes = [C.POINTER(MtrParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32), C.c_void_p,
+                                    C.c_void_p, C.c_void_p]
     lib.mtr_ctx_destroy.argtypes = [C.c_void_p]
     lib.mtr_ctx_destroy.restype = None
     lib.mtr_last_error.restype = C.c_char_p

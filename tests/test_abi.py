@@ -16,7 +16,7 @@ HEADER = os.path.join(ROOT, "include", "matter_gpu.h")
 def declared_functions():
     src = open(HEADER).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(mtr_[a-z_]+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(mtr_[a-z0-9_]+)\s*\(", src)))
 
 
 @pytest.fixture(scope="module")
