@@ -161,6 +161,11 @@ int mtr_step(mtr_ctx* ctx, int nsteps);
 /* Runs Simulation::simulate's loop (simulation.cpp:168-201) to the end. */
 int mtr_run(mtr_ctx* ctx);
 
+/* Runs steps until the frame counter advances (the point where simulate()
+ * saves a frame, simulation.cpp:180-190) or the simulation ends;
+ * *frame_done = 1 when a frame was completed. */
+int mtr_run_frame(mtr_ctx* ctx, int* frame_done);
+
 /* Copies the particle state back in the original particle order (any pointer
  * may be NULL).  Also returns pic and flip of the last step if requested. */
 int mtr_download(mtr_ctx* ctx, double* x, double* v, double* F, double* B, double* scalars);

@@ -573,6 +573,7 @@ int mtr_upload(mtr_ctx* c, const double* x, const double* v, const double* F, co
     // header
     std::memset(c->hH, 0, sizeof(StepHeader));
     c->hH->first_bad = 0xffffffffu;
+    c->hH->stop_frame = 0xffffffffu;
     for (int a = 0; a < 3; ++a) c->hH->gravity[a] = a < d ? c->prm.gravity[a] : 0.0;
     c->hH->done = (0 < c->prm.end_frame) ? 0 : 1;
     for (size_t i = 0; i < c->plates.size(); ++i) c->hH->plates[i] = c->plates[i];
@@ -626,6 +627,7 @@ int mtr_step(mtr_ctx* c, int nsteps) {
     CK(cudaSetDevice(c->device));
     read_header(c);
     if (c->hH->done) return (c->hH->status & kExitMask) ? MTR_ERR_DEVICE_STATUS : MTR_OK;
+    if (c->hH->frame >= c->hH->stop_frame) return MTR_OK;
     c->host_parity = c->hH->cur;
     int64_t launches = 0;
     int remaining = nsteps;
@@ -665,12 +667,44 @@ int mtr_step(mtr_ctx* c, int nsteps) {
         CK(cudaStreamSynchronize(c->stream));
         continue;
       }
-      if (H.done) break;
+      if (H.done || H.frame >= H.stop_frame) break;
     }
     c->launches_last = launches;
     if (c->hH->status & kExitMask) return MTR_ERR_DEVICE_STATUS;
     return MTR_OK;
   });
+}
+
+int mtr_run_frame(mtr_ctx* c, int* frame_done) {
+  int rc = guarded([&]() -> int {
+    if (!c || !c->uploaded) throw MtrError{MTR_ERR_STATE, "nothing uploaded"};
+    CK(cudaSetDevice(c->device));
+    read_header(c);
+    c->hH->stop_frame = c->hH->frame + 1;
+    write_header(c);
+    CK(cudaStreamSynchronize(c->stream));
+    return MTR_OK;
+  });
+  if (rc != MTR_OK) return rc;
+  mtr_clock ck{};
+  uint32_t f0 = 0;
+  rc = mtr_get_clock(c, &ck);
+  f0 = ck.frame;
+  while (rc == MTR_OK) {
+    rc = mtr_step(c, 128);
+    if (rc != MTR_OK) break;
+    rc = mtr_get_clock(c, &ck);
+    if (rc != MTR_OK || ck.done || ck.frame > f0) break;
+  }
+  int rc2 = guarded([&]() -> int {
+    read_header(c);
+    c->hH->stop_frame = 0xffffffffu;
+    write_header(c);
+    CK(cudaStreamSynchronize(c->stream));
+    return MTR_OK;
+  });
+  if (frame_done) *frame_done = (rc == MTR_OK && ck.frame > f0) ? 1 : 0;
+  return rc != MTR_OK ? rc : rc2;
 }
 
 int mtr_run(mtr_ctx* c) {

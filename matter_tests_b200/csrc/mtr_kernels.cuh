@@ -81,7 +81,9 @@ struct Tiling {
   static constexpr int NCH = 2 + 2 * D;         // mass, mom[D], force[D], friction
 };
 
-__device__ __forceinline__ bool step_inactive(const StepHeader* H) { return H->done || H->abort; }
+__device__ __forceinline__ bool step_inactive(const StepHeader* H) {
+  return H->done || H->abort || H->frame >= H->stop_frame;
+}
 
 __device__ __forceinline__ uint32_t node_index(const StepHeader* H, int i, int j, int k) {
   return ((uint32_t)i * H->N[1] + (uint32_t)j) * H->N[2] + (uint32_t)k;

@@ -18,7 +18,7 @@ _U = C.POINTER(C.c_uint32)
 
 # every entry point declared in include/matter_gpu.h
 EXPORTS = (
-    "mtr_ctx_create", "mtr_upload", "mtr_set_objects", "mtr_step", "mtr_run", "mtr_download",
+    "mtr_ctx_create", "mtr_upload", "mtr_set_objects", "mtr_step", "mtr_run", "mtr_run_frame", "mtr_download",
     "mtr_download_pic_flip", "mtr_get_grid", "mtr_get_sort", "mtr_get_plates", "mtr_get_clock",
     "mtr_status", "mtr_clear_status", "mtr_sync", "mtr_stream", "mtr_launch_count", "mtr_keep_pic_flip",
     "mtr_use_graphs", "mtr_profile", "mtr_active_nodes", "mtr_ctx_destroy", "mtr_last_error", "mtr_p2g_noalloc",
@@ -46,6 +46,7 @@ def load_library(path=LIB_PATH):
     lib.mtr_set_objects.argtypes = [C.c_void_p, C.POINTER(MtrPlate), C.c_int, C.POINTER(MtrObject), C.c_int]
     lib.mtr_step.argtypes = [C.c_void_p, C.c_int]
     lib.mtr_run.argtypes = [C.c_void_p]
+    lib.mtr_run_frame.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
     lib.mtr_download.argtypes = [C.c_void_p, _P, _P, _P, _P, _P]
     lib.mtr_download_pic_flip.argtypes = [C.c_void_p, _P, _P]
     lib.mtr_get_grid.argtypes = [C.c_void_p, _U, _P, _P, _P, _P, _P, _P]

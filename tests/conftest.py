@@ -25,6 +25,9 @@ def _ensure_oracle():
         # builds only where the reference tree is readable (oracle/Makefile REF)
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=False,
                        stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    if not os.path.exists(os.path.join(ref_dir, "kat", "kat")):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "kat"], check=False,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
 
 
 _ensure_oracle()
