@@ -6,12 +6,16 @@
 
 Workload (default): the 3D mu(I)-Drucker-Prager column collapse, MUSL, AFLIP,
 cubic B-splines, 1,024,000 particles (box 0.5 x 1.0 x 0.5 m, dx 0.0125 m,
-8 particles per cell), plain FP64, seeded synthetic jittered-lattice particles.
-A step is one Simulation::advanceStep of the whole scene.
+8 particles per cell), seeded synthetic jittered-lattice particles.  A step is
+one Simulation::advanceStep of the whole scene.  Both forms of the step run
+on the same scene: plain FP64 and mixed precision.
 
-value     particle-steps/s over K steps timed with CUDA events on the context's
-          stream, state resident in HBM (particle state 2 x 288 MB > 126 MB L2,
-          so every step streams it from HBM; no L2 flush is needed).
+value     mixed-precision particle-steps/s over K steps timed with CUDA events
+          on the context's stream, state resident in HBM (particle state
+          larger than the 126 MB L2 on both paths, so every step streams it
+          from HBM; no L2 flush is needed).  "fp64" holds the same figures for
+          the plain FP64 step, "mixed_error_vs_fp64" the state difference of
+          the two after the same W + K steps.
 e2e       the same metric through the C ABI with host buffers: mtr_upload from
           pinned host memory + mtr_step(K) + mtr_download, wall clock.
 roofline  the step's most expensive kernel: algorithmic bytes per launch
@@ -150,45 +154,48 @@ def hbm_peak():
 
 
 # ---------------------------------------------------------------------------
-# algorithmic bytes per launch (FP64): compulsory reads and writes of the
-# persistent particle state and of the grid nodes with mass.
-def kernel_bytes(name, p, Np, Ga, G):
+# algorithmic bytes per launch: compulsory reads and writes of the persistent
+# particle state and of the grid nodes with mass.  Positions are FP64 on both
+# paths (8 B); wr is the byte size of every other particle and grid value
+# (8 on the FP64 path, 4 on the mixed path).
+def kernel_bytes(name, p, Np, Ga, G, wr=8.0):
     d = p.dim
     dd = d * d
     ns = 6 if d == 3 else 3
-    w = 8.0
-    musl = bool(p.use_musl)
+    wx = 8.0
     nch = 2 + 2 * d
     if name == "k_p2g":
-        return Np * w * (2 * d + dd + ns + (1 if p.use_mibf else 0)) + Ga * w * (1 + 2 * d)
+        return Np * (wx * d + wr * (d + dd + ns + (1 if p.use_mibf else 0))) + Ga * wr * (1 + 2 * d)
     if name == "k_g2p":
-        return Np * w * (2 * d + dd + 5) + Ga * w * 2 * d + Np * (w * (2 * d + 2 * dd + 6 + ns) + 4)
+        return (Np * (wx * d + wr * (d + dd + 5)) + Ga * wr * 2 * d
+                + Np * (wx * d + wr * (d + 2 * dd + 6 + ns) + 4))
     if name == "k_g2p_musl":
-        return Np * w * (2 * d) + Ga * w * 2 * d + Np * (w * (2 * d + dd) + 4) + Ga * w * d
+        return Np * (wx * d + wr * d) + Ga * wr * 2 * d + Np * (wx * d + wr * (d + dd) + 4) + Ga * wr * d
     if name == "k_defgrad":
-        return Np * w * (d + dd + 5) + Ga * w * d + Np * w * (dd + 6 + ns)
+        return Np * (wx * d + wr * (dd + 5)) + Ga * wr * d + Np * wr * (dd + 6 + ns)
     if name == "k_grid":
-        return G * w * (nch + 2 * d + 1 + nch)
+        return G * wr * (nch + 2 * d + 1 + nch)
     if name == "k_musl_norm":
-        return G * w * (1 + 2 * d)
+        return G * wr * (1 + 2 * d)
     if name.startswith("k_sort_hist"):
-        return Np * (w * d + 4) if "keys" in name else Np * 4
+        return Np * (wx * d + 4) if "keys" in name else Np * 4
     if name == "k_sort_scatter":
         return Np * 16
     if name == "k_bbox":
-        return Np * w * 2 * d
+        return Np * (wx * d + wr * d)
     return None
 
 
-def step_bytes(p, Np, Ga):
+def step_bytes(p, Np, Ga, wr=8.0):
     """Whole-step algorithmic bytes: the persistent particle state read and
-    written once, plus the grid term (mass and momentum written and read,
+    written once (x v F B + 3 plastic scalars read; the same + 3 diagnostics
+    written), plus the grid term (mass and momentum written and read,
     velocity and flip written and read) per node with mass."""
     d = p.dim
     dd = d * d
-    per_particle = (2 * d + 2 * dd + 3) + (2 * d + 2 * dd + 6)  # read x v F B + 3 plastic; write + 3 diagnostics
+    per_particle = 2 * 8.0 * d + wr * ((d + 2 * dd + 3) + (d + 2 * dd + 6))
     per_node = (1 + d) * 2 + 2 * d * 2
-    return Np * 8.0 * per_particle + Ga * 8.0 * per_node
+    return Np * per_particle + Ga * wr * per_node
 
 
 # ---------------------------------------------------------------------------
@@ -274,10 +281,13 @@ def build_scene(args, rank):
 
 def config_of(args, sc):
     p = sc.params
+    sym = 6 if p.dim == 3 else 3
     return {"workload": f"{sc.name}: {args.workload} scale {args.scale}", "Np": sc.Np, "dim": p.dim,
             "spline_deg": p.spline_deg, "musl": bool(p.use_musl), "flip_ratio": p.flip_ratio,
             "plastic_model": int(p.plastic_model), "dx": p.dx, "precision": "fp64",
-            "l2": "inputs larger than L2 (particle state 2x%.0f MB)" % (sc.Np * 36 * 8 / 1e6),
+            "l2": "inputs larger than L2: particle state 2 x %.0f MB (FP64), 2 x %.0f MB (mixed)" % (
+                sc.Np * (8 * (2 * p.dim + 2 * p.dim ** 2 + 6 + sym)) / 1e6,
+                sc.Np * (8 * p.dim + 4 * (p.dim + 2 * p.dim ** 2 + 6 + sym)) / 1e6),
             "parallelism": "replicas"}
 
 
@@ -299,27 +309,26 @@ def reference_arm(args, world, rank):
     return 0
 
 
-def gpu_arm(args, world, rank, local):
+def measure(args, world, rank, local, sc, precision, sampler=None):
+    """Times one precision of the step on the scene: device-timed K steps,
+    per-kernel profile, roofline of the dominant kernel, and the end-to-end
+    run through the C ABI with pinned host buffers.  Returns a dict and the
+    particle state after warmup + K steps."""
+    import ctypes
+    import copy
     import numpy as np
     import torch
+    from matter_tests_b200.abi import PREC_MIXED
     from matter_tests_b200.gpu import GpuSim
 
-    torch.cuda.set_device(local)
-    sc = build_scene(args, rank)
-    p = sc.params
+    p = copy.copy(sc.params)
+    p.precision = precision
+    wr = 4.0 if precision == PREC_MIXED else 8.0
     g = GpuSim(p, device=local)
     g.upload(sc.x, sc.v, sc.F, sc.B, sc.scalars)
     g.set_objects(sc.plates, sc.objects)
     g.step(args.warmup)
     stream = torch.cuda.ExternalStream(g.stream, device=torch.device("cuda", local))
-    uuid = None
-    try:
-        uuid = str(torch.cuda.get_device_properties(local).uuid)
-        uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
-    except Exception:
-        pass
-    sampler = ClockSampler(uuid)
-    sampler.start()
     barrier(world)
     torch.cuda.synchronize(local)
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -330,10 +339,10 @@ def gpu_arm(args, world, rank, local):
     ev1.synchronize()
     torch.cuda.synchronize(local)
     barrier(world)
-    clocks = sampler.stop()
     ms = ev0.elapsed_time(ev1)
     launches = g.launch_count()
     ck = g.clock()
+    state = g.particles()
     ms_max = max_over_ranks(world, ms, local)
     value = sc.Np * args.steps * world / (ms_max / 1e3)
 
@@ -346,10 +355,10 @@ def gpu_arm(args, world, rank, local):
         agg[name] = agg.get(name, 0.0) + t
     dom = max((k for k in agg if k.startswith("k_")), key=lambda k: agg[k])
     dom_ms = agg[dom] / sum(1 for n, _ in slots if n == dom)
-    dom_bytes = kernel_bytes(dom, p, sc.Np, Ga, G)
+    dom_bytes = kernel_bytes(dom, p, sc.Np, Ga, G, wr)
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_bytes else None
     step_ms = sum(t for _, t in slots)
-    whole = step_bytes(p, sc.Np, Ga) / (ms / args.steps / 1e3) / 1e9
+    whole = step_bytes(p, sc.Np, Ga, wr) / (ms / args.steps / 1e3) / 1e9
 
     # end to end through the C ABI with pinned host buffers
     d = p.dim
@@ -361,7 +370,6 @@ def gpu_arm(args, world, rank, local):
     hB[:] = 0.0 if sc.B is None else sc.B.reshape(-1)
     hs[:] = 0.0 if sc.scalars is None else sc.scalars.reshape(-1)
     ox, ov, oF, oB, os_ = pin(sc.Np * d), pin(sc.Np * d), pin(sc.Np * d * d), pin(sc.Np * d * d), pin(sc.Np * 6)
-    import ctypes
     dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
     barrier(world)
     t0 = time.perf_counter()
@@ -378,6 +386,67 @@ def gpu_arm(args, world, rank, local):
            "timed": "mtr_upload (pinned host) + mtr_step(K) + mtr_download, wall clock"}
     status, _ = g.status()
     g.close()
+    out = {"value": value, "ms_per_step": ms_max / args.steps,
+           "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                        "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                        "traffic": None, "peak_source": peak_kind,
+                        "kernel_ms": dom_ms, "kernel_algorithmic_bytes": dom_bytes,
+                        "step_algorithmic_GBps": whole, "step_frac": whole / peak,
+                        "active_nodes": Ga, "grid_nodes": G},
+           "kernel_ms": {k: round(v / max(1, sum(1 for n, _ in slots if n == k)), 5) for k, v in agg.items()},
+           "profiled_step_ms": step_ms, "e2e": e2e, "gpu_launches": launches,
+           "sim_clock": {"step": ck["step"], "time": ck["time"]}, "status_flags": status}
+    return out, state
+
+
+def hencky_tau(F, E, nu):
+    """Kirchhoff stress of the Hencky model for a batch of F (n, d, d)."""
+    import numpy as np
+    lam = nu * E / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    U, S, _ = np.linalg.svd(F)
+    h = np.log(np.maximum(np.abs(S), 1e-300))
+    e = 2 * mu * h + lam * h.sum(axis=1, keepdims=True)
+    return np.einsum("nij,nj,nkj->nik", U, e, U)
+
+
+def mixed_error(sc, ref, got):
+    """Error of the mixed-precision state against the FP64 state after the
+    same steps: positions in units of dx, velocity and Kirchhoff stress
+    relative to their largest magnitude."""
+    import numpy as np
+    p = sc.params
+    dxp = np.abs(got["x"] - ref["x"]) / p.dx
+    vs = np.abs(ref["v"]).max()
+    Fr = np.transpose(ref["F"], (0, 2, 1))  # column-major host layout -> (n, r, c)
+    Fg = np.transpose(got["F"], (0, 2, 1))
+    tr, tg = hencky_tau(Fr, p.E, p.nu), hencky_tau(Fg, p.E, p.nu)
+    ts = np.abs(tr).max()
+    return {"x_max_over_dx": float(dxp.max()), "x_rms_over_dx": float(np.sqrt((dxp ** 2).mean())),
+            "v_max_rel": float(np.abs(got["v"] - ref["v"]).max() / vs) if vs > 0 else None,
+            "tau_max_rel": float(np.abs(tg - tr).max() / ts) if ts > 0 else None,
+            "F_max_abs": float(np.abs(got["F"] - ref["F"]).max())}
+
+
+def gpu_arm(args, world, rank, local):
+    import torch
+    from matter_tests_b200.abi import PREC_FP64, PREC_MIXED
+
+    torch.cuda.set_device(local)
+    sc = build_scene(args, rank)
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(local).uuid)
+        uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid)
+    sampler.start()
+    fp64, st64 = measure(args, world, rank, local, sc, PREC_FP64)
+    mixed, st32 = measure(args, world, rank, local, sc, PREC_MIXED)
+    clocks = sampler.stop()
+    err = mixed_error(sc, st64, st32)
+    err["steps"] = args.warmup + args.steps
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -385,20 +454,20 @@ def gpu_arm(args, world, rank, local):
         cpu = {"value": rate, "unit": METRIC, "cores": threads, "kind": kind, "sample": sample}
 
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic (seeded jittered lattice)", "config": config_of(args, sc),
-                "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                             "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                             "traffic": None, "peak_source": peak_kind,
-                             "kernel_ms": dom_ms, "kernel_algorithmic_bytes": dom_bytes,
-                             "step_algorithmic_GBps": whole, "step_frac": whole / peak,
-                             "active_nodes": Ga, "grid_nodes": G},
-                "kernel_ms": {k: round(v / max(1, sum(1 for n, _ in slots if n == k)), 5) for k, v in agg.items()},
-                "profiled_step_ms": step_ms,
-                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
-                "sim_clock": {"step": ck["step"], "time": ck["time"]}, "status_flags": status}
+        cfg = config_of(args, sc)
+        cfg["precision"] = "mixed (FP32 state and transfers, FP64 positions, SVD, return mapping, balances)"
+        line = {"metric": METRIC, "value": mixed["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": mixed["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+                "data": "synthetic (seeded jittered lattice)", "config": cfg,
+                "roofline": mixed["roofline"], "kernel_ms": mixed["kernel_ms"],
+                "profiled_step_ms": mixed["profiled_step_ms"], "cpu_baseline": cpu, "e2e": mixed["e2e"],
+                "gpu_launches": mixed["gpu_launches"] + fp64["gpu_launches"], "clocks": clocks,
+                "fp64": {k: fp64[k] for k in ("value", "ms_per_step", "roofline", "kernel_ms", "e2e",
+                                              "gpu_launches", "status_flags")},
+                "mixed_over_fp64": mixed["value"] / fp64["value"],
+                "mixed_error_vs_fp64": err,
+                "sim_clock": mixed["sim_clock"], "status_flags": mixed["status_flags"]}
         print(json.dumps(line), flush=True)
     return 0
 

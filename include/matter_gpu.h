@@ -78,6 +78,12 @@ enum mtr_object_kind {
 enum { MTR_SCALAR_EPS_PL_DEV = 0, MTR_SCALAR_EPS_PL_VOL, MTR_SCALAR_EPS_PL_VOL_PRADHANA,
        MTR_SCALAR_DELTA_GAMMA, MTR_SCALAR_VISCOSITY, MTR_SCALAR_MUI, MTR_NUM_SCALARS };
 
+/* MTR_PREC_FP64: the reference's double precision throughout.
+ * MTR_PREC_MIXED: particle velocity, deformation gradient (kept as F - I),
+ * affine matrix, stress and plastic scalars, the grid channels and the
+ * transfers in FP32; positions, the clock, the deformation update, the SVD,
+ * the Hencky log/exp, the return mapping and the balances in FP64.  The ABI
+ * is FP64 on both paths. */
 enum mtr_precision { MTR_PREC_FP64 = 0, MTR_PREC_MIXED = 1 };
 
 /* Public fields of Simulation (simulation.hpp:28-106) that the step reads,
@@ -216,6 +222,14 @@ int mtr_use_graphs(mtr_ctx* ctx, int on);
  * in the last step. */
 int mtr_profile(mtr_ctx* ctx, int nsteps, double* slot_ms, const char** slot_names, int max_slots, int* nslots);
 int mtr_active_nodes(mtr_ctx* ctx, uint64_t* active, uint64_t* total);
+
+/* Mass and momentum balance of the last step, in FP64 on both paths
+ * (Simulation::checkMassConservation / checkMomentumConservation,
+ * simulation.cpp:292-333): total grid mass and momentum right after P2G, and
+ * the particles' total mass and momentum (particle_mass * sum of v) before
+ * it.  Momenta are dim values. */
+int mtr_balance(mtr_ctx* ctx, double* grid_mass, double* grid_momentum, double* particle_mass,
+                double* particle_momentum);
 
 /* mtr_p2g_noalloc — no counterpart in the reference.  The particle-to-grid
  * transfer (the P2G of p2g.cpp: grid mass = particle mass * sum of weights,

@@ -70,15 +70,18 @@ struct mtr_ctx {
   StepHeader* hH = nullptr;  // pinned mirror
   uint32_t Np = 0;
   bool uploaded = false;
-  // particle buffers (two sets) and their backing allocations
-  PBuf buf[2]{};
+  // storage type of particle and grid state: double (MTR_PREC_FP64) or float (MTR_PREC_MIXED)
+  bool fp32 = false;
+  size_t rsize = sizeof(double);
+  // particle buffers (two sets, positions FP64, the rest of type R) and their backing allocations
+  PBufT<void> buf[2]{};
   std::vector<void*> pallocs;
-  double *pic = nullptr, *flip = nullptr;
-  // grid
+  void *pic = nullptr, *flip = nullptr;
+  // grid (axes FP64, node channels of type R)
   uint32_t cap_axis[3] = {0, 0, 0};
   uint32_t cap_nodes = 0, cap_tiles = 0;
   double *gx = nullptr, *gy = nullptr, *gz = nullptr;
-  double *acc = nullptr, *nv = nullptr, *nflip = nullptr, *nmass = nullptr, *nfric = nullptr, *v2 = nullptr;
+  void *acc = nullptr, *nv = nullptr, *nflip = nullptr, *nmass = nullptr, *nfric = nullptr, *v2 = nullptr;
   uint32_t *tile_begin = nullptr, *tile_end = nullptr;
   // sort
   uint32_t *keys0 = nullptr, *keysA = nullptr, *valsA = nullptr, *keysB = nullptr, *valsB = nullptr;
@@ -127,7 +130,8 @@ void free_grid(mtr_ctx* c) {
   for (void* p : {(void*)c->gx, (void*)c->gy, (void*)c->gz, (void*)c->acc, (void*)c->nv, (void*)c->nflip,
                   (void*)c->nmass, (void*)c->nfric, (void*)c->v2, (void*)c->tile_begin, (void*)c->tile_end})
     dfree(p);
-  c->gx = c->gy = c->gz = c->acc = c->nv = c->nflip = c->nmass = c->nfric = c->v2 = nullptr;
+  c->gx = c->gy = c->gz = nullptr;
+  c->acc = c->nv = c->nflip = c->nmass = c->nfric = c->v2 = nullptr;
   c->tile_begin = c->tile_end = nullptr;
 }
 
@@ -156,22 +160,23 @@ void alloc_grid(mtr_ctx* c, const uint32_t want[3]) {
   c->cap_nodes = (uint32_t)nodes;
   c->cap_tiles = (uint32_t)tiles;
   const int nch = 2 + 2 * d;
+  const size_t rs = c->rsize;
   c->gx = dalloc<double>(c->cap_axis[0]);
   c->gy = dalloc<double>(c->cap_axis[1]);
   c->gz = dalloc<double>(c->cap_axis[2]);
-  c->acc = dalloc<double>((size_t)nch * nodes);
-  c->nv = dalloc<double>((size_t)d * nodes);
-  c->nflip = dalloc<double>((size_t)d * nodes);
-  c->nmass = dalloc<double>(nodes);
-  c->nfric = dalloc<double>(nodes);
-  c->v2 = dalloc<double>((size_t)d * nodes);
+  c->acc = dalloc<unsigned char>(rs * nch * nodes);
+  c->nv = dalloc<unsigned char>(rs * d * nodes);
+  c->nflip = dalloc<unsigned char>(rs * d * nodes);
+  c->nmass = dalloc<unsigned char>(rs * nodes);
+  c->nfric = dalloc<unsigned char>(rs * nodes);
+  c->v2 = dalloc<unsigned char>(rs * d * nodes);
   c->tile_begin = dalloc<uint32_t>(tiles);
   c->tile_end = dalloc<uint32_t>(tiles);
-  CK(cudaMemsetAsync(c->acc, 0, sizeof(double) * nch * nodes, c->stream));
-  CK(cudaMemsetAsync(c->nv, 0, sizeof(double) * d * nodes, c->stream));
-  CK(cudaMemsetAsync(c->nflip, 0, sizeof(double) * d * nodes, c->stream));
-  CK(cudaMemsetAsync(c->nmass, 0, sizeof(double) * nodes, c->stream));
-  CK(cudaMemsetAsync(c->v2, 0, sizeof(double) * d * nodes, c->stream));
+  CK(cudaMemsetAsync(c->acc, 0, rs * nch * nodes, c->stream));
+  CK(cudaMemsetAsync(c->nv, 0, rs * d * nodes, c->stream));
+  CK(cudaMemsetAsync(c->nflip, 0, rs * d * nodes, c->stream));
+  CK(cudaMemsetAsync(c->nmass, 0, rs * nodes, c->stream));
+  CK(cudaMemsetAsync(c->v2, 0, rs * d * nodes, c->stream));
   uint64_t keybits = 1;
   while ((1ull << keybits) < tiles * 64ull) ++keybits;
   c->passes = (int)((keybits + 7) / 8);
@@ -189,22 +194,36 @@ void mark(mtr_ctx* c, const char* name) {
   c->marks.emplace_back(name, e);
 }
 
-template <int D, int DEG>
+template <int D, int DEG, typename R>
 void set_kernel_attributes_t() {
-  CK(cudaFuncSetAttribute(k_p2g_w<D, DEG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p2g_smem_bytes<D>()));
-  CK(cudaFuncSetAttribute(k_g2p_musl_w<D, DEG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)musl_smem_bytes<D>()));
+  CK(cudaFuncSetAttribute(k_p2g_w<D, DEG, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)p2g_smem_bytes<D, R>()));
+  CK(cudaFuncSetAttribute(k_g2p_musl_w<D, DEG, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)musl_smem_bytes<D, R>()));
 }
 
-void set_kernel_attributes() {
-  set_kernel_attributes_t<2, 2>();
-  set_kernel_attributes_t<2, 3>();
-  set_kernel_attributes_t<3, 2>();
-  set_kernel_attributes_t<3, 3>();
+void set_kernel_attributes(bool fp32) {
+  if (fp32) {
+    set_kernel_attributes_t<2, 2, float>();
+    set_kernel_attributes_t<2, 3, float>();
+    set_kernel_attributes_t<3, 2, float>();
+    set_kernel_attributes_t<3, 3, float>();
+  } else {
+    set_kernel_attributes_t<2, 2, double>();
+    set_kernel_attributes_t<2, 3, double>();
+    set_kernel_attributes_t<3, 2, double>();
+    set_kernel_attributes_t<3, 3, double>();
+  }
 }
 
-StepArgs make_args(mtr_ctx* c, int parity) {
-  StepArgs A{};
+template <typename R>
+PBufT<R> typed(const PBufT<void>& b) {
+  return PBufT<R>{b.x, (R*)b.v, (R*)b.F, (R*)b.B, (R*)b.sc, (R*)b.tau, b.id};
+}
+
+template <typename R>
+StepArgsT<R> make_args(mtr_ctx* c, int parity) {
+  StepArgsT<R> A{};
   A.P = c->dP;
   A.H = c->dH;
   A.partials = c->partials;
@@ -216,12 +235,13 @@ StepArgs make_args(mtr_ctx* c, int parity) {
   for (int a = 0; a < 3; ++a) A.cap_axis[a] = c->cap_axis[a];
   A.cap_nodes = c->cap_nodes;
   A.cap_tiles = c->cap_tiles;
-  A.acc = c->acc;
-  A.nv = c->nv;
-  A.nflip = c->nflip;
-  A.nmass = c->nmass;
-  A.nfric = c->nfric;
-  A.v2 = c->v2;
+  A.acc = (R*)c->acc;
+  A.nv = (R*)c->nv;
+  A.nflip = (R*)c->nflip;
+  A.nmass = (R*)c->nmass;
+  A.nfric = (R*)c->nfric;
+  A.v2 = (R*)c->v2;
+  A.xin = c->buf[parity].x;
   A.keys0 = c->keys0;
   A.keysA = c->keysA;
   A.valsA = c->valsA;
@@ -232,23 +252,23 @@ StepArgs make_args(mtr_ctx* c, int parity) {
   A.sort_blocks = c->sort_blocks;
   A.tile_begin = c->tile_begin;
   A.tile_end = c->tile_end;
-  A.in = c->buf[parity];
-  A.out = c->buf[1 - parity];
-  A.pic = c->pic;
-  A.flip = c->flip;
+  A.in = typed<R>(c->buf[parity]);
+  A.out = typed<R>(c->buf[1 - parity]);
+  A.pic = (R*)c->pic;
+  A.flip = (R*)c->flip;
   return A;
 }
 
 // Enqueues one step reading buffer `parity` and writing the other.  Returns
 // the number of kernels launched.
-template <int D, int DEG>
+template <int D, int DEG, typename R>
 int enqueue_step_t(mtr_ctx* c, int parity) {
   cudaStream_t st = c->stream;
-  StepArgs A = make_args(c, parity);
+  StepArgsT<R> A = make_args<R>(c, parity);
   int n = 0;
   const uint32_t pblocks = (c->Np + 127) / 128;
   mark(c, "start");
-  k_bbox<D><<<c->npartials, 256, 0, st>>>(A);
+  k_bbox<D, R><<<c->npartials, 256, 0, st>>>(A);
   ++n;
   mark(c, "k_bbox");
   k_header<D><<<1, 32, 0, st>>>(A);
@@ -282,25 +302,25 @@ int enqueue_step_t(mtr_ctx* c, int parity) {
   k_tile_ranges<<<std::min<uint32_t>((c->Np + 255) / 256, 148 * 8), 256, 0, st>>>(A, skeys);
   ++n;
   mark(c, "k_tile_ranges");
-  k_p2g_w<D, DEG><<<c->cap_tiles, kChunk, p2g_smem_bytes<D>(), st>>>(A, perm);
+  k_p2g_w<D, DEG, R><<<c->cap_tiles, kChunk, p2g_smem_bytes<D, R>(), st>>>(A, perm);
   ++n;
   mark(c, "k_p2g");
   const uint32_t gblocks = std::min<uint32_t>((c->cap_nodes + 255) / 256, 148 * 16);
-  k_grid<D><<<gblocks, 256, 0, st>>>(A);
+  k_grid<D, R><<<gblocks, 256, 0, st>>>(A);
   ++n;
   mark(c, "k_grid");
   if (c->prm.use_musl) {
-    CK(cudaMemsetAsync(c->v2, 0, sizeof(double) * D * c->cap_nodes, st));
+    CK(cudaMemsetAsync(c->v2, 0, sizeof(R) * D * c->cap_nodes, st));
     mark(c, "memset(v2)");
-    k_g2p_musl_w<D, DEG><<<c->cap_tiles, kChunk, musl_smem_bytes<D>(), st>>>(A, perm);
+    k_g2p_musl_w<D, DEG, R><<<c->cap_tiles, kChunk, musl_smem_bytes<D, R>(), st>>>(A, perm);
     mark(c, "k_g2p_musl");
-    k_musl_norm<D><<<gblocks, 256, 0, st>>>(A);
+    k_musl_norm<D, R><<<gblocks, 256, 0, st>>>(A);
     mark(c, "k_musl_norm");
-    k_defgrad_t<D, DEG><<<c->cap_tiles, kChunk, 0, st>>>(A, perm);
+    k_defgrad_t<D, DEG, R><<<c->cap_tiles, kChunk, 0, st>>>(A, perm);
     mark(c, "k_defgrad");
     n += 3;
   } else {
-    k_g2p_t<D, DEG><<<c->cap_tiles, kChunk, 0, st>>>(A, perm);
+    k_g2p_t<D, DEG, R><<<c->cap_tiles, kChunk, 0, st>>>(A, perm);
     ++n;
     mark(c, "k_g2p");
   }
@@ -311,9 +331,14 @@ int enqueue_step_t(mtr_ctx* c, int parity) {
   return n;
 }
 
+template <typename R>
+int enqueue_step_r(mtr_ctx* c, int parity) {
+  if (c->dim == 3) return c->deg == 3 ? enqueue_step_t<3, 3, R>(c, parity) : enqueue_step_t<3, 2, R>(c, parity);
+  return c->deg == 3 ? enqueue_step_t<2, 3, R>(c, parity) : enqueue_step_t<2, 2, R>(c, parity);
+}
+
 int enqueue_step(mtr_ctx* c, int parity) {
-  if (c->dim == 3) return c->deg == 3 ? enqueue_step_t<3, 3>(c, parity) : enqueue_step_t<3, 2>(c, parity);
-  return c->deg == 3 ? enqueue_step_t<2, 3>(c, parity) : enqueue_step_t<2, 2>(c, parity);
+  return c->fp32 ? enqueue_step_r<float>(c, parity) : enqueue_step_r<double>(c, parity);
 }
 
 void build_graphs(mtr_ctx* c) {
@@ -413,6 +438,7 @@ void derive_constants(mtr_ctx* c) {  // simulation.cpp:94-136
   h.p0 = p.p0;
   h.mu_1 = p.mu_1;
   h.mu_2 = p.mu_2;
+  h.mui0 = (p.plastic_model == MTR_PM_DPMUI || p.plastic_model == MTR_PM_MCCMUI) ? p.mu_1 : p.M;
 }
 
 // The first step's grid extents, as remeshFixedInit(2,2,2) will compute them
@@ -438,6 +464,39 @@ void initial_grid_extent(mtr_ctx* c, const double* x, uint32_t want[3]) {
   }
 }
 
+// SoA device array of the current particle order -> AoS host array in the
+// caller's order (kinds as k_soa_to_aos); f64 marks an FP64 array on either path.
+void get_soa(mtr_ctx* c, double* host, const void* src, const uint32_t* id, int width, int kind, bool f64) {
+  if (!host) return;
+  const uint32_t Np = c->Np, blocks = (Np + 255) / 256;
+  const int d = c->dim;
+  if (f64 || !c->fp32) {
+    if (d == 3)
+      k_soa_to_aos<3, double><<<blocks, 256, 0, c->stream>>>(Np, (const double*)src, id, c->staging, kind);
+    else
+      k_soa_to_aos<2, double><<<blocks, 256, 0, c->stream>>>(Np, (const double*)src, id, c->staging, kind);
+  } else {
+    if (d == 3)
+      k_soa_to_aos<3, float><<<blocks, 256, 0, c->stream>>>(Np, (const float*)src, id, c->staging, kind);
+    else
+      k_soa_to_aos<2, float><<<blocks, 256, 0, c->stream>>>(Np, (const float*)src, id, c->staging, kind);
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(host, c->staging, sizeof(double) * Np * width, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+}
+
+// n node values of the context's storage type -> FP64 host array
+void get_nodes(mtr_ctx* c, double* host, const void* src, size_t n) {
+  if (!c->fp32) {
+    CK(cudaMemcpy(host, src, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    return;
+  }
+  std::vector<float> tmp(n);
+  CK(cudaMemcpy(tmp.data(), src, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < n; ++i) host[i] = tmp[i];
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -452,7 +511,8 @@ int mtr_ctx_create(const mtr_params* params, int device, mtr_ctx** out) {
     const mtr_params& p = *params;
     if (p.dim != 2 && p.dim != 3) throw MtrError{MTR_ERR_INVALID, "dim must be 2 or 3"};
     if (p.spline_deg != 2 && p.spline_deg != 3) throw MtrError{MTR_ERR_INVALID, "spline_deg must be 2 or 3"};
-    if (p.precision != MTR_PREC_FP64) throw MtrError{MTR_ERR_INVALID, "only the FP64 path is built"};
+    if (p.precision != MTR_PREC_FP64 && p.precision != MTR_PREC_MIXED)
+      throw MtrError{MTR_ERR_INVALID, "precision must be MTR_PREC_FP64 or MTR_PREC_MIXED"};
     if (p.pbc) throw MtrError{MTR_ERR_INVALID, "periodic boundaries are not part of this path"};
     if (p.plastic_model < 0 || p.plastic_model > MTR_PM_SNOW) throw MtrError{MTR_ERR_INVALID, "invalid plastic model"};
     if (p.elastic_model != MTR_EL_HENCKY && p.elastic_model != MTR_EL_NEOHOOKEAN)
@@ -469,9 +529,11 @@ int mtr_ctx_create(const mtr_params* params, int device, mtr_ctx** out) {
       c->device = device;
       c->dim = p.dim;
       c->deg = p.spline_deg;
+      c->fp32 = p.precision == MTR_PREC_MIXED;
+      c->rsize = c->fp32 ? sizeof(float) : sizeof(double);
       CK(cudaSetDevice(device));
       CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-      set_kernel_attributes();
+      set_kernel_attributes(c->fp32);
       derive_constants(c);
       c->dP = dalloc<DevParams>(1);
       c->dH = dalloc<StepHeader>(1);
@@ -502,20 +564,23 @@ int mtr_upload(mtr_ctx* c, const double* x, const double* v, const double* F, co
       dfree(p);
     c->Np = Np;
     c->hp.Np = Np;
+    const size_t rs = c->rsize;
     for (int s = 0; s < 2; ++s) {
-      double* blk = dalloc<double>((size_t)Np * (2 * d + 2 * dd + MTR_NUM_SCALARS + ns));
+      double* xb = dalloc<double>((size_t)Np * d);
+      unsigned char* blk = dalloc<unsigned char>(rs * Np * (d + 2 * dd + MTR_NUM_SCALARS + ns));
+      c->pallocs.push_back(xb);
       c->pallocs.push_back(blk);
-      c->buf[s].x = blk;
-      c->buf[s].v = blk + (size_t)Np * d;
-      c->buf[s].F = blk + (size_t)Np * 2 * d;
-      c->buf[s].B = blk + (size_t)Np * (2 * d + dd);
-      c->buf[s].sc = blk + (size_t)Np * (2 * d + 2 * dd);
-      c->buf[s].tau = blk + (size_t)Np * (2 * d + 2 * dd + MTR_NUM_SCALARS);
+      c->buf[s].x = xb;
+      c->buf[s].v = blk;
+      c->buf[s].F = blk + rs * Np * d;
+      c->buf[s].B = blk + rs * Np * (d + dd);
+      c->buf[s].sc = blk + rs * Np * (d + 2 * dd);
+      c->buf[s].tau = blk + rs * Np * (d + 2 * dd + MTR_NUM_SCALARS);
       c->buf[s].id = dalloc<uint32_t>(Np);
       c->pallocs.push_back(c->buf[s].id);
     }
-    c->pic = dalloc<double>((size_t)Np * d);
-    c->flip = dalloc<double>((size_t)Np * d);
+    c->pic = dalloc<unsigned char>(rs * Np * d);
+    c->flip = dalloc<unsigned char>(rs * Np * d);
     c->pallocs.push_back(c->pic);
     c->pallocs.push_back(c->flip);
     c->sort_blocks = (int)((Np + kSortTile - 1) / kSortTile);
@@ -531,7 +596,7 @@ int mtr_upload(mtr_ctx* c, const double* x, const double* v, const double* F, co
     c->staging = dalloc<double>((size_t)Np * std::max<int>(dd, (int)MTR_NUM_SCALARS));
     // state -> buffer 0 (AoS host layout -> SoA)
     const uint32_t blocks = (Np + 255) / 256;
-    auto put = [&](const double* host, double* dst, int width, int kind, const double* fill) {
+    auto put = [&](const double* host, void* dst, int width, int kind, const double* fill) {
       if (host) {
         CK(cudaMemcpyAsync(c->staging, host, sizeof(double) * Np * width, cudaMemcpyHostToDevice, c->stream));
       } else {
@@ -542,10 +607,22 @@ int mtr_upload(mtr_ctx* c, const double* x, const double* v, const double* F, co
         CK(cudaMemcpyAsync(c->staging, tmp.data(), sizeof(double) * tmp.size(), cudaMemcpyHostToDevice, c->stream));
         CK(cudaStreamSynchronize(c->stream));
       }
-      if (d == 3)
-        k_aos_to_soa<3><<<blocks, 256, 0, c->stream>>>(Np, c->staging, dst, kind);
-      else
-        k_aos_to_soa<2><<<blocks, 256, 0, c->stream>>>(Np, c->staging, dst, kind);
+      if (kind == 0 && dst == c->buf[0].x) {  // positions stay FP64
+        if (d == 3)
+          k_aos_to_soa<3, double><<<blocks, 256, 0, c->stream>>>(Np, c->staging, (double*)dst, kind);
+        else
+          k_aos_to_soa<2, double><<<blocks, 256, 0, c->stream>>>(Np, c->staging, (double*)dst, kind);
+      } else if (c->fp32) {
+        if (d == 3)
+          k_aos_to_soa<3, float><<<blocks, 256, 0, c->stream>>>(Np, c->staging, (float*)dst, kind);
+        else
+          k_aos_to_soa<2, float><<<blocks, 256, 0, c->stream>>>(Np, c->staging, (float*)dst, kind);
+      } else {
+        if (d == 3)
+          k_aos_to_soa<3, double><<<blocks, 256, 0, c->stream>>>(Np, c->staging, (double*)dst, kind);
+        else
+          k_aos_to_soa<2, double><<<blocks, 256, 0, c->stream>>>(Np, c->staging, (double*)dst, kind);
+      }
       CK(cudaGetLastError());
       CK(cudaStreamSynchronize(c->stream));
     };
@@ -553,7 +630,7 @@ int mtr_upload(mtr_ctx* c, const double* x, const double* v, const double* F, co
     for (int i = 0; i < d; ++i) eye[i * d + i] = 1.0;
     put(x, c->buf[0].x, d, 0, nullptr);
     put(v, c->buf[0].v, d, 0, nullptr);
-    put(F, c->buf[0].F, dd, 1, eye);
+    put(F, c->buf[0].F, dd, c->fp32 ? 3 : 1, eye);  // FP32 keeps F - I
     put(B, c->buf[0].B, dd, 1, nullptr);
     std::vector<double> sc;
     const double* scp = scalars;
@@ -579,11 +656,19 @@ int mtr_upload(mtr_ctx* c, const double* x, const double* v, const double* F, co
     for (size_t i = 0; i < c->plates.size(); ++i) c->hH->plates[i] = c->plates[i];
     write_header(c);
     upload_params(c);
-    StepArgs A = make_args(c, 0);
-    if (d == 3)
-      k_init_state<3><<<blocks, 256, 0, c->stream>>>(A, c->buf[0]);
-    else
-      k_init_state<2><<<blocks, 256, 0, c->stream>>>(A, c->buf[0]);
+    if (c->fp32) {
+      StepArgsT<float> A = make_args<float>(c, 0);
+      if (d == 3)
+        k_init_state<3, float><<<blocks, 256, 0, c->stream>>>(A, A.in);
+      else
+        k_init_state<2, float><<<blocks, 256, 0, c->stream>>>(A, A.in);
+    } else {
+      StepArgsT<double> A = make_args<double>(c, 0);
+      if (d == 3)
+        k_init_state<3, double><<<blocks, 256, 0, c->stream>>>(A, A.in);
+      else
+        k_init_state<2, double><<<blocks, 256, 0, c->stream>>>(A, A.in);
+    }
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(c->stream));
     c->host_parity = 0;
@@ -724,23 +809,12 @@ int mtr_download(mtr_ctx* c, double* x, double* v, double* F, double* B, double*
     CK(cudaSetDevice(c->device));
     read_header(c);
     const int d = c->dim, dd = d * d;
-    const PBuf& b = c->buf[c->hH->cur];
-    const uint32_t Np = c->Np, blocks = (Np + 255) / 256;
-    auto get = [&](double* host, const double* src, int width, int kind) {
-      if (!host) return;
-      if (d == 3)
-        k_soa_to_aos<3><<<blocks, 256, 0, c->stream>>>(Np, src, b.id, c->staging, kind);
-      else
-        k_soa_to_aos<2><<<blocks, 256, 0, c->stream>>>(Np, src, b.id, c->staging, kind);
-      CK(cudaGetLastError());
-      CK(cudaMemcpyAsync(host, c->staging, sizeof(double) * Np * width, cudaMemcpyDeviceToHost, c->stream));
-      CK(cudaStreamSynchronize(c->stream));
-    };
-    get(x, b.x, d, 0);
-    get(v, b.v, d, 0);
-    get(F, b.F, dd, 1);
-    get(B, b.B, dd, 1);
-    get(scalars, b.sc, MTR_NUM_SCALARS, 2);
+    const PBufT<void>& b = c->buf[c->hH->cur];
+    get_soa(c, x, b.x, b.id, d, 0, true);
+    get_soa(c, v, b.v, b.id, d, 0, false);
+    get_soa(c, F, b.F, b.id, dd, c->fp32 ? 3 : 1, false);
+    get_soa(c, B, b.B, b.id, dd, 1, false);
+    get_soa(c, scalars, b.sc, b.id, MTR_NUM_SCALARS, 2, false);
     return MTR_OK;
   });
 }
@@ -751,21 +825,9 @@ int mtr_download_pic_flip(mtr_ctx* c, double* pic, double* flip) {
     if (!c->hp.store_pic_flip) throw MtrError{MTR_ERR_STATE, "pic/flip are kept only after mtr_keep_pic_flip(ctx, 1)"};
     CK(cudaSetDevice(c->device));
     read_header(c);
-    const int d = c->dim;
-    const PBuf& b = c->buf[c->hH->cur];
-    const uint32_t Np = c->Np, blocks = (Np + 255) / 256;
-    for (int w = 0; w < 2; ++w) {
-      double* host = w == 0 ? pic : flip;
-      if (!host) continue;
-      const double* src = w == 0 ? c->pic : c->flip;
-      if (d == 3)
-        k_soa_to_aos<3><<<blocks, 256, 0, c->stream>>>(Np, src, b.id, c->staging, 0);
-      else
-        k_soa_to_aos<2><<<blocks, 256, 0, c->stream>>>(Np, src, b.id, c->staging, 0);
-      CK(cudaGetLastError());
-      CK(cudaMemcpyAsync(host, c->staging, sizeof(double) * Np * d, cudaMemcpyDeviceToHost, c->stream));
-      CK(cudaStreamSynchronize(c->stream));
-    }
+    const PBufT<void>& b = c->buf[c->hH->cur];
+    get_soa(c, pic, c->pic, b.id, c->dim, 0, false);
+    get_soa(c, flip, c->flip, b.id, c->dim, 0, false);
     return MTR_OK;
   });
 }
@@ -797,14 +859,14 @@ int mtr_get_grid(mtr_ctx* c, uint32_t dims[3], double* gx, double* gy, double* g
     if (gx) CK(cudaMemcpy(gx, c->gx, sizeof(double) * H.N[0], cudaMemcpyDeviceToHost));
     if (gy) CK(cudaMemcpy(gy, c->gy, sizeof(double) * H.N[1], cudaMemcpyDeviceToHost));
     if (gz && d == 3) CK(cudaMemcpy(gz, c->gz, sizeof(double) * H.N[2], cudaMemcpyDeviceToHost));
-    if (mass) CK(cudaMemcpy(mass, c->nmass, sizeof(double) * G, cudaMemcpyDeviceToHost));
+    if (mass) get_nodes(c, mass, c->nmass, G);
     std::vector<double> tmp((size_t)G);
     for (int w = 0; w < 2; ++w) {
       double* host = w == 0 ? v : flip;
       if (!host) continue;
-      const double* src = w == 0 ? (c->prm.use_musl ? c->v2 : c->nv) : c->nflip;
+      const unsigned char* src = (const unsigned char*)(w == 0 ? (c->prm.use_musl ? c->v2 : c->nv) : c->nflip);
       for (int a = 0; a < d; ++a) {
-        CK(cudaMemcpy(tmp.data(), src + (size_t)a * c->cap_nodes, sizeof(double) * G, cudaMemcpyDeviceToHost));
+        get_nodes(c, tmp.data(), src + c->rsize * a * c->cap_nodes, G);
         for (uint32_t l = 0; l < G; ++l) host[(size_t)l * d + a] = tmp[l];
       }
     }
@@ -967,11 +1029,28 @@ int mtr_active_nodes(mtr_ctx* c, uint64_t* active, uint64_t* total) {
     CK(cudaSetDevice(c->device));
     read_header(c);
     std::vector<double> m(c->hH->G);
-    CK(cudaMemcpy(m.data(), c->nmass, sizeof(double) * m.size(), cudaMemcpyDeviceToHost));
+    get_nodes(c, m.data(), c->nmass, m.size());
     uint64_t a = 0;
     for (double v : m) a += v > 0;
     if (active) *active = a;
     if (total) *total = m.size();
+    return MTR_OK;
+  });
+}
+
+int mtr_balance(mtr_ctx* c, double* grid_mass, double* grid_momentum, double* particle_mass,
+                double* particle_momentum) {
+  return guarded([&]() -> int {
+    if (!c || !c->uploaded) throw MtrError{MTR_ERR_STATE, "nothing uploaded"};
+    CK(cudaSetDevice(c->device));
+    read_header(c);
+    const StepHeader& H = *c->hH;
+    if (grid_mass) *grid_mass = H.grid_mass;
+    if (particle_mass) *particle_mass = c->prm.particle_mass * (double)c->Np;
+    for (int a = 0; a < c->dim; ++a) {
+      if (grid_momentum) grid_momentum[a] = H.grid_mom[a];
+      if (particle_momentum) particle_momentum[a] = H.part_mom[a];
+    }
     return MTR_OK;
   });
 }

@@ -1,6 +1,8 @@
 // mtr_device.cuh — device-side types and math shared by the MPM step kernels.
 //
-// Everything here is written for sm_100a and FP64 (the plain-precision path).
+// Everything here is written for sm_100a.  The return mapping, the SVD and
+// every projection are FP64 on both paths; the spline weights are templated on
+// the arithmetic type so the mixed-precision path can evaluate them in FP32.
 // Small matrices are register arrays indexed with compile-time indices only
 // (all loops over DIM are unrolled), so nothing spills to local memory.
 #pragma once
@@ -29,6 +31,7 @@ struct DevParams {
   double gravity_final[3], gravity_time, grid_ref[3];
   double E, nu, stress_tolerance, xi, q_max, q_min, p_min, M, q_cohesion, perzyna_exp, perzyna_visc, beta, p0,
       mu_1, mu_2;
+  double mui0;  // muI every particle starts from when use_mibf (simulation.cpp:138-145)
   mtr_object objects[MTR_MAXO];
 };
 
@@ -50,6 +53,9 @@ struct StepHeader {
   uint32_t ntiles;
   double min_init[3], max_init[3], low_init[3], high_init[3];
   unsigned long long plastic_count;
+  // FP64 balances of the last step (simulation.cpp:292-333): grid mass and
+  // momentum right after P2G, particle mass and momentum before it
+  double grid_mass, grid_mom[3], part_mom[3];
   mtr_plate plates[MTR_MAXP];
 };
 
@@ -57,7 +63,7 @@ struct StepHeader {
 // remesh.cpp:42-83): min and max of x per axis and max |v|^2.
 struct BBoxPartial {
   double mn[3], mx[3], v2;
-  double pad;
+  double vsum[3];  // sum of particle velocities (for the momentum balance)
 };
 
 // ---------------------------------------------------------------------------
@@ -147,8 +153,8 @@ __device__ __forceinline__ void usu_packed(const double (&U)[D][D], const double
   }
 }
 
-template <int D>
-__device__ __forceinline__ double sym_at(const double* t, int i, int j) {
+template <int D, typename T>
+__device__ __forceinline__ T sym_at(const T* t, int i, int j) {
   if constexpr (D == 3) {
     if (i == j) return t[i];
     int s = i + j;  // (0,1)->1, (0,2)->2, (1,2)->3
@@ -161,31 +167,34 @@ __device__ __forceinline__ double sym_at(const double* t, int i, int j) {
 // ---------------------------------------------------------------------------
 // B-spline basis (tools.hpp:108-188): quadratic (DEG 2) and cubic (DEG 3)
 // ---------------------------------------------------------------------------
-template <int DEG>
-__device__ __forceinline__ double bspline_N(double u) {
-  double a = fabs(u);
+// R is the arithmetic type: double on the FP64 path, float for the FP32
+// weights of the mixed-precision path (same expressions, same order).
+template <int DEG, typename R>
+__device__ __forceinline__ R bspline_N(R u) {
+  R a = fabs(u);
   if constexpr (DEG == 3) {
-    if (a < 1.0) return 0.5 * a * a * a - a * a + 2.0 / 3.0;
-    if (a < 2.0) return (1.0 / 6.0) * (2.0 - a) * (2.0 - a) * (2.0 - a);
-    return 0.0;
+    if (a < R(1.0)) return R(0.5) * a * a * a - a * a + R(2.0 / 3.0);
+    if (a < R(2.0)) return R(1.0 / 6.0) * (R(2.0) - a) * (R(2.0) - a) * (R(2.0) - a);
+    return R(0.0);
   } else {
-    if (a < 0.5) return 0.75 - a * a;
-    if (a < 1.5) return 0.5 * (1.5 - a) * (1.5 - a);
-    return 0.0;
+    if (a < R(0.5)) return R(0.75) - a * a;
+    if (a < R(1.5)) return R(0.5) * (R(1.5) - a) * (R(1.5) - a);
+    return R(0.0);
   }
 }
 
-template <int DEG>
-__device__ __forceinline__ double bspline_dN(double u) {
-  double a = fabs(u);
+template <int DEG, typename R>
+__device__ __forceinline__ R bspline_dN(R u) {
+  R a = fabs(u);
+  const R sg = R((R(0.0) < u) - (u < R(0.0)));  // tools.hpp:90-92
   if constexpr (DEG == 3) {
-    if (a < 1.0) return u * (1.5 * a - 2.0);
-    if (a < 2.0) return -0.5 * sgn(u) * (2.0 - a) * (2.0 - a);
-    return 0.0;
+    if (a < R(1.0)) return u * (R(1.5) * a - R(2.0));
+    if (a < R(2.0)) return R(-0.5) * sg * (R(2.0) - a) * (R(2.0) - a);
+    return R(0.0);
   } else {
-    if (a < 0.5) return -2 * u;
-    if (a < 1.5) return u - 1.5 * sgn(u);
-    return 0.0;
+    if (a < R(0.5)) return R(-2) * u;
+    if (a < R(1.5)) return u - R(1.5) * sg;
+    return R(0.0);
   }
 }
 

@@ -1,20 +1,20 @@
 // mtr_kernels.cuh — the sm_100a kernels of one explicit MPM step
-// (Simulation::advanceStep, simulation.cpp:219-273), FP64.
+// (Simulation::advanceStep, simulation.cpp:219-273).
 //
 // Step pipeline (all on one stream, no host round trip, CUDA-graph capturable):
-//   k_bbox        per-block min/max x and max |v|^2          update_dt.cpp, remesh.cpp
+//   k_bbox        per-block min/max x, max |v|^2 and sum v    update_dt.cpp, remesh.cpp
 //   k_header      dt, gravity ramp, remesh + arange axes      update_dt.cpp:5-66, remesh.cpp:38-311
 //   k_sort_*      stable LSD radix sort by blocked cell key   (new: locality for P2G)
 //   k_tile_ranges particle range of every 4^3 (2D: 8^2) tile
-//   k_p2g         tile block -> shared grid patch -> one global atomic per node and channel
+//   k_p2g_w       tile block -> shared grid patch -> one global atomic per node and channel
 //                 (mass, momentum with APIC, force tau.grad w, MIBF friction)
 //                                                              p2g.cpp:6-100, explicit_euler_update.cpp:15-77
-//   k_grid        normalise, v += -dt V0 f/m + dt g, boundary collision, flip
+//   k_grid        normalise, v += -dt V0 f/m + dt g, boundary collision, flip, FP64 balances
 //                                                              p2g.cpp:84-98, explicit_euler_update.cpp:83-132
-//   USL:  k_g2p   gather pic/B/flip/grad v, F update, return mapping, tau, x/v update, coalesced stores
+//   USL:  k_g2p_t gather pic/B/flip/grad v, F update, return mapping, tau, x/v update, coalesced stores
 //                                                              g2p.cpp, deformation_update.cpp, plasticity.cpp,
 //                                                              position_update.cpp
-//   MUSL: k_g2p_musl (gather + v blend + re-scatter), k_musl_norm, k_defgrad
+//   MUSL: k_g2p_musl_w (gather + v blend + re-scatter), k_musl_norm, k_defgrad_t
 //                                                              musl.cpp:6-96
 //   k_tail        plate motion, clock, frame and end test     object_plate.hpp:136-162, simulation.cpp:176-200
 //
@@ -22,24 +22,39 @@
 // the step reads the `in` set through the sort permutation and writes the
 // `out` set in sorted order, so the particle order follows the cell order and
 // every later read of the same data is nearly coalesced.
+//
+// Precision.  Every kernel that touches particle or grid state is templated
+// on the storage type R.  R = double is the reference's FP64 arithmetic,
+// operation for operation.  R = float is the mixed-precision form: particle
+// v, F, B, stress and plastic scalars, the grid channels, the spline weights,
+// the P2G/MUSL accumulation and the G2P gathers are FP32; positions, the
+// clock and the grid axes stay FP64, and so do the deformation update, the
+// SVD, the Hencky log/exp, the return mapping with its projections, and the
+// mass and momentum balances.  F is stored as F - I in FP32, so its rounding
+// is relative to the strain (about 1e-3) rather than to 1.
 #pragma once
+#include <type_traits>
+
 #include "mtr_boundary.cuh"
 #include "mtr_device.cuh"
 #include "mtr_plasticity.cuh"
 
 namespace mtr {
 
-struct PBuf {
-  double* x;     // [D][Np]
-  double* v;     // [D][Np]
-  double* F;     // [D*D][Np], entry (r,c) at (r*D + c)
-  double* B;     // [D*D][Np]
-  double* sc;    // [6][Np] MTR_SCALAR_* order
-  double* tau;   // [Sym<D>::n][Np]
+template <typename R>
+struct PBufT {
+  double* x;     // [D][Np] positions, FP64 on both paths
+  R* v;          // [D][Np]
+  R* F;          // [D*D][Np], entry (r,c) at (r*D + c); FP32 path: F - I
+  R* B;          // [D*D][Np]
+  R* sc;         // [6][Np] MTR_SCALAR_* order
+  R* tau;        // [Sym<D>::n][Np] Kirchhoff stress carried to the next P2G
   uint32_t* id;  // original particle index
 };
+using PBuf = PBufT<double>;
 
-struct StepArgs {
+// What every kernel of a step shares, whatever the storage type.
+struct StepCommon {
   const DevParams* P;
   StepHeader* H;
   BBoxPartial* partials;
@@ -49,23 +64,32 @@ struct StepArgs {
   uint32_t cap_axis[3];
   uint32_t cap_nodes;
   uint32_t cap_tiles;
-  double* acc;    // [NCH][cap_nodes] P2G accumulators: mass, mom[D], force[D], friction
-  double* nv;     // [D][cap_nodes]  node velocity after the update (MUSL: after re-projection)
-  double* nflip;  // [D][cap_nodes]
-  double* nmass;  // [cap_nodes]
-  double* nfric;  // [cap_nodes]
-  double* v2;     // [D][cap_nodes]  MUSL re-projection accumulator
-  uint32_t* keys0;  // cell key of each particle in input order
+  const double* xin;  // positions of the step's input buffer (sort keys)
+  uint32_t* keys0;    // cell key of each particle in input order
   uint32_t *keysA, *valsA, *keysB, *valsB;
-  uint32_t* hist;   // [256][sort_blocks]
-  uint32_t* dtot;   // [256]
+  uint32_t* hist;  // [256][sort_blocks]
+  uint32_t* dtot;  // [256]
   int sort_blocks;
   uint32_t* tile_begin;
   uint32_t* tile_end;
-  PBuf in, out;
-  double* pic;   // optional [D][Np] in output order
-  double* flip;  // optional [D][Np]
 };
+
+template <typename R>
+struct StepArgsT : StepCommon {
+  R* acc;    // [NCH][cap_nodes] P2G accumulators: mass, mom[D], force[D], friction
+  R* nv;     // [D][cap_nodes]  node velocity after the update (MUSL: after re-projection)
+  R* nflip;  // [D][cap_nodes]
+  R* nmass;  // [cap_nodes]
+  R* nfric;  // [cap_nodes]
+  R* v2;     // [D][cap_nodes]  MUSL re-projection accumulator
+  PBufT<R> in, out;
+  R* pic;   // optional [D][Np] in output order
+  R* flip;  // optional [D][Np]
+};
+using StepArgs = StepArgsT<double>;
+
+template <typename R>
+constexpr bool kFP64 = std::is_same<R, double>::value;
 
 constexpr uint32_t kMaxAxisNodes = 1u << 22;
 constexpr int kSortThreads = 256;
@@ -81,6 +105,8 @@ struct Tiling {
   static constexpr int NCH = 2 + 2 * D;         // mass, mom[D], force[D], friction
 };
 
+constexpr size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
+
 __device__ __forceinline__ bool step_inactive(const StepHeader* H) {
   return H->done || H->abort || H->frame >= H->stop_frame;
 }
@@ -89,13 +115,40 @@ __device__ __forceinline__ uint32_t node_index(const StepHeader* H, int i, int j
   return ((uint32_t)i * H->N[1] + (uint32_t)j) * H->N[2] + (uint32_t)k;
 }
 
+// sum over the block of a per-thread value, added once to *dst (all threads call)
+__device__ __forceinline__ void block_add(double v, double* dst) {
+  __shared__ double red[32];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += red[w];
+    if (s != 0.0) atomicAdd(dst, s);
+  }
+}
+
+// plastic particles of the block, one global atomic per block
+__device__ __forceinline__ void block_count(unsigned n, unsigned long long* dst) {
+  __shared__ unsigned cnt;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  n = __reduce_add_sync(0xffffffffu, n);
+  if ((threadIdx.x & 31) == 0 && n) atomicAdd(&cnt, n);
+  __syncthreads();
+  if (threadIdx.x == 0 && cnt) atomicAdd(dst, (unsigned long long)cnt);
+}
+
 // ---------------------------------------------------------------------------
-// 1. bbox / vmax partials
+// 1. bbox / vmax / sum v partials
 // ---------------------------------------------------------------------------
-template <int D>
-__global__ void __launch_bounds__(256) k_bbox(StepArgs A) {
+template <int D, typename R>
+__global__ void __launch_bounds__(256) k_bbox(StepArgsT<R> A) {
   if (step_inactive(A.H)) return;
-  double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300}, v2 = 0.0;
+  double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300}, v2 = 0.0, vs[3] = {0.0, 0.0, 0.0};
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < A.Np; i += gridDim.x * blockDim.x) {
     double vv[3];
 #pragma unroll
@@ -104,6 +157,7 @@ __global__ void __launch_bounds__(256) k_bbox(StepArgs A) {
       mn[a] = fmin(mn[a], xa);
       mx[a] = fmax(mx[a], xa);
       vv[a] = A.in.v[(size_t)a * A.Np + i];
+      vs[a] += vv[a];
     }
     double s = __dadd_rn(__dmul_rn(vv[0], vv[0]), __dmul_rn(vv[1], vv[1]));
     if constexpr (D == 3) s = __dadd_rn(s, __dmul_rn(vv[2], vv[2]));
@@ -115,6 +169,7 @@ __global__ void __launch_bounds__(256) k_bbox(StepArgs A) {
     for (int a = 0; a < D; ++a) {
       mn[a] = fmin(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], off));
       mx[a] = fmax(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], off));
+      vs[a] += __shfl_xor_sync(0xffffffffu, vs[a], off);
     }
     v2 = fmax(v2, __shfl_xor_sync(0xffffffffu, v2, off));
   }
@@ -125,6 +180,7 @@ __global__ void __launch_bounds__(256) k_bbox(StepArgs A) {
     for (int a = 0; a < 3; ++a) {
       wp[warp].mn[a] = mn[a];
       wp[warp].mx[a] = mx[a];
+      wp[warp].vsum[a] = vs[a];
     }
     wp[warp].v2 = v2;
   }
@@ -136,6 +192,7 @@ __global__ void __launch_bounds__(256) k_bbox(StepArgs A) {
       for (int a = 0; a < 3; ++a) {
         r.mn[a] = fmin(r.mn[a], wp[w].mn[a]);
         r.mx[a] = fmax(r.mx[a], wp[w].mx[a]);
+        r.vsum[a] += wp[w].vsum[a];
       }
       r.v2 = fmax(r.v2, wp[w].v2);
     }
@@ -147,18 +204,19 @@ __global__ void __launch_bounds__(256) k_bbox(StepArgs A) {
 // 2. step header: dt (update_dt.cpp:5-66) and grid (remesh.cpp:38-311)
 // ---------------------------------------------------------------------------
 template <int D>
-__global__ void __launch_bounds__(32) k_header(StepArgs A) {
+__global__ void __launch_bounds__(32) k_header(StepCommon A) {
   StepHeader* H = A.H;
   const DevParams& P = *A.P;
   if (step_inactive(H)) return;
   const int lane = threadIdx.x;
-  double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300}, v2 = 0.0;
+  double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300}, v2 = 0.0, vs[3] = {0.0, 0.0, 0.0};
   for (int b = lane; b < A.npartials; b += 32) {
     const BBoxPartial& q = A.partials[b];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       mn[a] = fmin(mn[a], q.mn[a]);
       mx[a] = fmax(mx[a], q.mx[a]);
+      vs[a] += q.vsum[a];
     }
     v2 = fmax(v2, q.v2);
   }
@@ -168,12 +226,20 @@ __global__ void __launch_bounds__(32) k_header(StepArgs A) {
     for (int a = 0; a < 3; ++a) {
       mn[a] = fmin(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], off));
       mx[a] = fmax(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], off));
+      vs[a] += __shfl_xor_sync(0xffffffffu, vs[a], off);
     }
     v2 = fmax(v2, __shfl_xor_sync(0xffffffffu, v2, off));
   }
   __shared__ double s_low[3], s_high[3];
   __shared__ int s_ok;
   if (lane == 0) {
+    // balances of this step (read back by mtr_balance)
+    H->grid_mass = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      H->grid_mom[a] = 0.0;
+      H->part_mom[a] = P.particle_mass * vs[a];
+    }
     // updateDt
     const double max_speed = sqrt(v2);
     double dt;
@@ -299,7 +365,8 @@ __device__ __forceinline__ uint32_t cell_key(const StepHeader* H, double ioh, co
 
 // Per-block digit histogram.  The first pass computes the keys from x.
 template <int D, bool FIRST>
-__global__ void __launch_bounds__(kSortThreads) k_sort_hist(StepArgs A, const uint32_t* __restrict__ keys, int shift) {
+__global__ void __launch_bounds__(kSortThreads) k_sort_hist(StepCommon A, const uint32_t* __restrict__ keys,
+                                                            int shift) {
   if (step_inactive(A.H)) return;
   __shared__ uint32_t h[256];
   h[threadIdx.x] = 0;
@@ -314,7 +381,7 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_hist(StepArgs A, const ui
       if (FIRST) {
         double x[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-        for (int a = 0; a < D; ++a) x[a] = A.in.x[(size_t)a * A.Np + i];
+        for (int a = 0; a < D; ++a) x[a] = A.xin[(size_t)a * A.Np + i];
         k = cell_key<D>(A.H, ioh, x);
         A.keys0[i] = k;
       } else {
@@ -328,7 +395,7 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_hist(StepArgs A, const ui
 }
 
 // Exclusive scan of each digit's row over the blocks; row totals to dtot.
-static __global__ void __launch_bounds__(256) k_sort_scan(StepArgs A) {
+static __global__ void __launch_bounds__(256) k_sort_scan(StepCommon A) {
   if (step_inactive(A.H)) return;
   const int dgt = blockIdx.x;
   uint32_t* row = A.hist + (size_t)dgt * A.sort_blocks;
@@ -363,7 +430,7 @@ static __global__ void __launch_bounds__(256) k_sort_scan(StepArgs A) {
 // Stable scatter.  Elements are ranked round by round (256 at a time, in
 // index order) with warp match + per-warp digit counts, which keeps equal
 // digits in input order.
-static __global__ void __launch_bounds__(kSortThreads) k_sort_scatter(StepArgs A, const uint32_t* __restrict__ ksrc,
+static __global__ void __launch_bounds__(kSortThreads) k_sort_scatter(StepCommon A, const uint32_t* __restrict__ ksrc,
                                                                const uint32_t* __restrict__ vsrc, uint32_t* kdst,
                                                                uint32_t* vdst, int shift) {
   if (step_inactive(A.H)) return;
@@ -428,27 +495,13 @@ static __global__ void __launch_bounds__(kSortThreads) k_sort_scatter(StepArgs A
 // ---------------------------------------------------------------------------
 // 4. tile ranges over the sorted keys
 // ---------------------------------------------------------------------------
-static __global__ void __launch_bounds__(256) k_tile_ranges(StepArgs A, const uint32_t* __restrict__ skeys) {
+static __global__ void __launch_bounds__(256) k_tile_ranges(StepCommon A, const uint32_t* __restrict__ skeys) {
   if (step_inactive(A.H)) return;
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < A.Np; s += gridDim.x * blockDim.x) {
     const uint32_t t = skeys[s] >> 6;
     if (t >= A.cap_tiles) continue;
     if (s == 0 || (skeys[s - 1] >> 6) != t) A.tile_begin[t] = s;
     if (s == A.Np - 1 || (skeys[s + 1] >> 6) != t) A.tile_end[t] = s + 1;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// stencil weights of one particle along one axis
-// ---------------------------------------------------------------------------
-template <int DEG>
-__device__ __forceinline__ void axis_weights(double xp, const double* coords, double ioh, double (&w)[4],
-                                             double (&dw)[4]) {
-#pragma unroll
-  for (int o = 0; o < 4; ++o) {
-    const double u = (xp - coords[o]) * ioh;
-    w[o] = bspline_N<DEG>(u);
-    dw[o] = bspline_dN<DEG>(u);
   }
 }
 
@@ -466,770 +519,10 @@ __device__ __forceinline__ void tile_coords(const StepHeader* H, uint32_t t, int
   }
 }
 
-// ---------------------------------------------------------------------------
-// 5. P2G + stress force, one block per tile
-// ---------------------------------------------------------------------------
-template <int D, int DEG>
-__global__ void __launch_bounds__(128) k_p2g(StepArgs A, const uint32_t* __restrict__ perm) {
-  using TL = Tiling<D>;
-  constexpr int PN = TL::PN, NODES = TL::NODES, NCH = TL::NCH, TB = TL::TB;
-  const StepHeader* H = A.H;
-  if (step_inactive(H)) return;
-  const uint32_t t = blockIdx.x;
-  if (t >= H->ntiles) return;
-  const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
-  if (pb >= pe) return;
-  const DevParams& P = *A.P;
-  __shared__ double patch[NCH][NODES];
-  __shared__ double crd[3][PN];
-  int tc[3];
-  tile_coords<D>(H, t, tc);
-  int n0[3] = {tc[0] * TB - 1, tc[1] * TB - 1, D == 3 ? tc[2] * TB - 1 : 0};
-  for (int i = threadIdx.x; i < NCH * NODES; i += blockDim.x) (&patch[0][0])[i] = 0.0;
-  for (int i = threadIdx.x; i < D * PN; i += blockDim.x) {
-    const int a = i / PN, o = i % PN;
-    const int g = n0[a] + o;
-    const double* ax = a == 0 ? A.gx : (a == 1 ? A.gy : A.gz);
-    crd[a][o] = (g >= 0 && g < (int)H->N[a]) ? ax[g] : 0.0;
-  }
-  __syncthreads();
-  const uint32_t Np = A.Np;
-  const double ioh = P.one_over_dx;
-  const bool apic = P.flip_ratio < 0;
-  const bool mibf = P.use_mibf;
-  for (uint32_t s = pb + threadIdx.x; s < pe; s += blockDim.x) {
-    const uint32_t j = perm[s];
-    double xp[3] = {0, 0, 0}, vp[3] = {0, 0, 0}, tau[Sym<D>::n];
-    double Bm[D][D];
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      xp[a] = A.in.x[(size_t)a * Np + j];
-      vp[a] = A.in.v[(size_t)a * Np + j];
-    }
-    if (apic) {
-#pragma unroll
-      for (int r = 0; r < D; ++r)
-#pragma unroll
-        for (int c = 0; c < D; ++c) Bm[r][c] = A.in.B[(size_t)(r * D + c) * Np + j];
-    }
-#pragma unroll
-    for (int q = 0; q < Sym<D>::n; ++q) tau[q] = A.in.tau[(size_t)q * Np + j];
-    const double mui = mibf ? A.in.sc[(size_t)MTR_SCALAR_MUI * Np + j] : 0.0;
-    int lb[3] = {0, 0, 0};
-    bool oob = false;
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      int b = (int)floor((xp[a] - H->org[a]) * ioh) - 1;
-      b = b < 0 ? 0 : b;  // p2g.cpp:21-24 clamps at zero
-      lb[a] = b - n0[a];
-      if (lb[a] < 0 || lb[a] > PN - 4 || b + 3 >= (int)H->N[a]) oob = true;
-    }
-    if (oob) {
-      raise_status(A.H, MTR_STATUS_STENCIL_OOB, A.in.id[j]);
-      continue;
-    }
-    double w[3][4], dw[3][4];
-#pragma unroll
-    for (int a = 0; a < D; ++a) axis_weights<DEG>(xp[a], &crd[a][lb[a]], ioh, w[a], dw[a]);
-    constexpr int KN = D == 3 ? 4 : 1;
-#pragma unroll
-    for (int ii = 0; ii < 4; ++ii)
-#pragma unroll
-      for (int jj = 0; jj < 4; ++jj)
-#pragma unroll
-        for (int kk = 0; kk < KN; ++kk) {
-          double wxy = w[0][ii] * w[1][jj];
-          const double weight = D == 3 ? wxy * w[2][kk] : wxy;
-          const int node = D == 3 ? ((lb[0] + ii) * PN + (lb[1] + jj)) * PN + (lb[2] + kk)
-                                  : (lb[0] + ii) * PN + (lb[1] + jj);
-          if (weight > 1e-25) {
-            atomicAdd(&patch[0][node], weight);
-            double pd[3] = {crd[0][lb[0] + ii] - xp[0], crd[1][lb[1] + jj] - xp[1],
-                            D == 3 ? crd[2][lb[2] + kk] - xp[2] : 0.0};
-#pragma unroll
-            for (int a = 0; a < D; ++a) {
-              double m = vp[a] * weight;
-              if (apic) {
-                double bv = Bm[a][0] * pd[0];
-#pragma unroll
-                for (int c = 1; c < D; ++c) bv += Bm[a][c] * pd[c];
-                m += bv * P.apicDinverse * weight;
-              }
-              atomicAdd(&patch[1 + a][node], m);
-            }
-            if (mibf) atomicAdd(&patch[1 + 2 * D][node], mui * weight);
-          }
-          double g[3];
-          if constexpr (D == 3) {
-            g[0] = dw[0][ii] * w[1][jj] * w[2][kk] * ioh;
-            g[1] = dw[1][jj] * w[0][ii] * w[2][kk] * ioh;
-            g[2] = dw[2][kk] * w[0][ii] * w[1][jj] * ioh;
-          } else {
-            g[0] = dw[0][ii] * w[1][jj] * ioh;
-            g[1] = dw[1][jj] * w[0][ii] * ioh;
-          }
-#pragma unroll
-          for (int a = 0; a < D; ++a) {
-            double f = sym_at<D>(tau, a, 0) * g[0];
-#pragma unroll
-            for (int c = 1; c < D; ++c) f += sym_at<D>(tau, a, c) * g[c];
-            if (f != 0.0) atomicAdd(&patch[1 + D + a][node], f);
-          }
-        }
-  }
-  __syncthreads();
-  const uint32_t cap = A.cap_nodes;
-  for (int n = threadIdx.x; n < NODES; n += blockDim.x) {
-    int li, lj, lk;
-    if constexpr (D == 3) {
-      lk = n % PN;
-      lj = (n / PN) % PN;
-      li = n / (PN * PN);
-    } else {
-      lk = 0;
-      lj = n % PN;
-      li = n / PN;
-    }
-    const int gi = n0[0] + li, gj = n0[1] + lj, gk = n0[2] + lk;
-    if (gi < 0 || gj < 0 || gk < 0 || gi >= (int)H->N[0] || gj >= (int)H->N[1] || gk >= (int)H->N[2]) continue;
-    const uint32_t l = node_index(H, gi, gj, gk);
-#pragma unroll
-    for (int ch = 0; ch < NCH; ++ch) {
-      const double val = patch[ch][n];
-      if (val != 0.0) atomicAdd(&A.acc[(size_t)ch * cap + l], val);
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// 5'. P2G + stress force, warp-cooperative form (used for every launch).
-//
-// A tile block walks its sorted particles in chunks of kChunk.  Phase 1, one
-// thread per particle, loads the particle and stages its stencil weights and
-// gradients in shared memory.  Phase 2, one warp per run of 32 staged
-// particles: every lane owns fixed stencil nodes of a cell (3D: 2 of the 64,
-// 2D: 1 of the 16, a half warp per particle), accumulates all channels in
-// registers while consecutive particles share a cell, and adds them to the
-// shared patch once per cell.  Sorted particles share cells in runs of about
-// ppc, so this issues ~ppc times fewer shared atomics than one atomic per
-// particle and node, with no two lanes of a warp on one address.
-// ---------------------------------------------------------------------------
-constexpr int kChunk = 128;
-
+// Sets the patch origin n0 of tile t and copies the grid coordinates its
+// stencils can reach into crd.
 template <int D>
-struct PStage {
-  double x[D], v[D], B[D * D], tau[Sym<D>::n], w[D * 4], dw[D * 4];
-  double mui;
-  int lb;  // packed local stencil base (4 bits per axis); -1 marks an empty slot
-  int pad;
-};
-
-template <int D>
-constexpr size_t p2g_smem_bytes() {
-  return sizeof(double) * (Tiling<D>::NCH * Tiling<D>::NODES + 3 * Tiling<D>::PN) + sizeof(PStage<D>) * kChunk;
-}
-
-template <int D, int DEG>
-__global__ void __launch_bounds__(kChunk) k_p2g_w(StepArgs A, const uint32_t* __restrict__ perm) {
-  using TL = Tiling<D>;
-  constexpr int PN = TL::PN, NODES = TL::NODES, NCH = TL::NCH, TB = TL::TB;
-  constexpr int NS = Sym<D>::n;
-  const StepHeader* H = A.H;
-  if (step_inactive(H)) return;
-  const uint32_t t = blockIdx.x;
-  if (t >= H->ntiles) return;
-  const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
-  if (pb >= pe) return;
-  const DevParams& P = *A.P;
-  extern __shared__ double smem[];
-  double(*patch)[NODES] = reinterpret_cast<double(*)[NODES]>(smem);
-  double(*crd)[PN] = reinterpret_cast<double(*)[PN]>(smem + NCH * NODES);
-  PStage<D>* st = reinterpret_cast<PStage<D>*>(smem + NCH * NODES + 3 * PN);
-  int tc[3];
-  tile_coords<D>(H, t, tc);
-  const int n0[3] = {tc[0] * TB - 1, tc[1] * TB - 1, D == 3 ? tc[2] * TB - 1 : 0};
-  for (int i = threadIdx.x; i < NCH * NODES; i += blockDim.x) (&patch[0][0])[i] = 0.0;
-  for (int i = threadIdx.x; i < D * PN; i += blockDim.x) {
-    const int a = i / PN, o = i % PN;
-    const int g = n0[a] + o;
-    const double* ax = a == 0 ? A.gx : (a == 1 ? A.gy : A.gz);
-    crd[a][o] = (g >= 0 && g < (int)H->N[a]) ? ax[g] : 0.0;
-  }
-  __syncthreads();
-  const uint32_t Np = A.Np;
-  const double ioh = P.one_over_dx, apicD = P.apicDinverse;
-  const bool apic = P.flip_ratio < 0;
-  const bool mibf = P.use_mibf;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // Lane groups: 3D, 16 lanes per particle (a lane owns the (iy, iz) column
-  // and its 4 ix nodes), two groups of 16 particles per warp and chunk; 2D,
-  // 4 lanes per particle (a lane owns iy and its 4 ix nodes), eight groups of 4.
-  constexpr int LPP = D == 3 ? 16 : 4;
-  const int q = lane % LPP;
-  const int iy = D == 3 ? (q >> 2) : q;
-  const int iz = D == 3 ? (q & 3) : 0;
-  // group g takes the consecutive staged particles [g*LPP, (g+1)*LPP) of the
-  // warp's 32, so groups work on different cells and their flushes rarely
-  // meet on one patch node (interleaving them made both groups flush the same
-  // cell at once, which measured slower despite fewer bank conflicts)
-  const int kbeg = warp * 32 + (lane / LPP) * LPP, kend = kbeg + LPP;
-  for (uint32_t c0 = pb; c0 < pe; c0 += kChunk) {
-    {  // phase 1: stage one particle per thread
-      const uint32_t s = c0 + threadIdx.x;
-      PStage<D>& S = st[threadIdx.x];
-      int packed = -1;
-      if (s < pe) {
-        const uint32_t j = perm[s];
-        int lb[3] = {0, 0, 0};
-        bool oob = false;
-#pragma unroll
-        for (int a = 0; a < D; ++a) {
-          S.x[a] = A.in.x[(size_t)a * Np + j];
-          S.v[a] = A.in.v[(size_t)a * Np + j];
-          int b = (int)floor((S.x[a] - H->org[a]) * ioh) - 1;
-          b = b < 0 ? 0 : b;  // p2g.cpp:21-24 clamps at zero
-          lb[a] = b - n0[a];
-          if (lb[a] < 0 || lb[a] > PN - 4 || b + 3 >= (int)H->N[a]) oob = true;
-        }
-#pragma unroll
-        for (int q = 0; q < D * D; ++q) S.B[q] = apic ? A.in.B[(size_t)q * Np + j] : 0.0;
-#pragma unroll
-        for (int q = 0; q < NS; ++q) S.tau[q] = A.in.tau[(size_t)q * Np + j];
-        S.mui = mibf ? A.in.sc[(size_t)MTR_SCALAR_MUI * Np + j] : 0.0;
-        if (oob) {
-          raise_status(A.H, MTR_STATUS_STENCIL_OOB, A.in.id[j]);
-        } else {
-#pragma unroll
-          for (int a = 0; a < D; ++a) {
-#pragma unroll
-            for (int o = 0; o < 4; ++o) {
-              const double u = (S.x[a] - crd[a][lb[a] + o]) * ioh;
-              S.w[a * 4 + o] = bspline_N<DEG>(u);
-              S.dw[a * 4 + o] = bspline_dN<DEG>(u);
-            }
-          }
-          packed = lb[0] | (lb[1] << 4) | (lb[2] << 8);
-        }
-      }
-      S.lb = packed;
-    }
-    __syncthreads();
-    {  // phase 2: a lane owns one (iy, iz) stencil column and its 4 ix nodes
-      double acc[4][NCH];
-#pragma unroll
-      for (int h = 0; h < 4; ++h)
-#pragma unroll
-        for (int ch = 0; ch < NCH; ++ch) acc[h][ch] = 0.0;
-      int cur = -1;
-      auto flush = [&]() {
-        const int lbx = cur & 15, lby = (cur >> 4) & 15, lbz = cur >> 8;
-#pragma unroll
-        for (int h = 0; h < 4; ++h) {
-          const int node = D == 3 ? ((lbx + h) * PN + (lby + iy)) * PN + (lbz + iz) : (lbx + h) * PN + (lby + iy);
-#pragma unroll
-          for (int ch = 0; ch < NCH; ++ch) {
-            if (acc[h][ch] != 0.0) atomicAdd(&patch[ch][node], acc[h][ch]);
-            acc[h][ch] = 0.0;
-          }
-        }
-      };
-      for (int k = kbeg; k < kend; ++k) {
-        const PStage<D>& S = st[k];
-        const int lbp = S.lb;
-        if (lbp < 0) continue;
-        if (lbp != cur) {
-          if (cur >= 0) flush();
-          cur = lbp;
-        }
-        const int lbx = lbp & 15, lby = (lbp >> 4) & 15, lbz = lbp >> 8;
-        // tensor-product factors of this lane's column
-        const double wy = S.w[4 + iy], dwy = S.dw[4 + iy];
-        double wyz, G0, G1, G2 = 0.0;
-        if constexpr (D == 3) {
-          const double wz = S.w[8 + iz], dwz = S.dw[8 + iz];
-          wyz = wy * wz;
-          G0 = wyz * ioh;
-          G1 = dwy * wz * ioh;
-          G2 = wy * dwz * ioh;
-        } else {
-          wyz = wy;
-          G0 = wy * ioh;
-          G1 = dwy * ioh;
-        }
-        // force f_a = tau_a . grad w = dwx * Pf_a + wx * Qf_a
-        double Pf[D], Qf[D];
-#pragma unroll
-        for (int a = 0; a < D; ++a) {
-          Pf[a] = sym_at<D>(S.tau, a, 0) * G0;
-          double q = sym_at<D>(S.tau, a, 1) * G1;
-          if constexpr (D == 3) q += sym_at<D>(S.tau, a, 2) * G2;
-          Qf[a] = q;
-        }
-        // momentum per weight: v_a + apicD B_a . (x_i - x_p) = Tm_a + Sm_a * pdx
-        const double pdy = crd[1][lby + iy] - S.x[1];
-        const double pdz = D == 3 ? crd[2][lbz + iz] - S.x[D - 1] : 0.0;
-        double Tm[D], Sm[D];
-#pragma unroll
-        for (int a = 0; a < D; ++a) {
-          if (apic) {
-            double byz = S.B[a * D + 1] * pdy;
-            if constexpr (D == 3) byz += S.B[a * D + 2] * pdz;
-            Tm[a] = S.v[a] + apicD * byz;
-            Sm[a] = apicD * S.B[a * D];
-          } else {
-            Tm[a] = S.v[a];
-            Sm[a] = 0.0;
-          }
-        }
-        const double xp0 = S.x[0], mui = S.mui;
-#pragma unroll
-        for (int h = 0; h < 4; ++h) {
-          const double wx = S.w[h], dwx = S.dw[h];
-          const double weight = wx * wyz;
-          if (weight > 1e-25) {
-            const double pdx = crd[0][lbx + h] - xp0;
-            acc[h][0] += weight;
-#pragma unroll
-            for (int a = 0; a < D; ++a) acc[h][1 + a] += weight * (Tm[a] + Sm[a] * pdx);
-            if (mibf) acc[h][1 + 2 * D] += mui * weight;
-          }
-#pragma unroll
-          for (int a = 0; a < D; ++a) acc[h][1 + D + a] += dwx * Pf[a] + wx * Qf[a];
-        }
-      }
-      if (cur >= 0) flush();
-    }
-    __syncthreads();
-  }
-  const uint32_t cap = A.cap_nodes;
-  for (int n = threadIdx.x; n < NODES; n += blockDim.x) {
-    int li, lj, lk;
-    if constexpr (D == 3) {
-      lk = n % PN;
-      lj = (n / PN) % PN;
-      li = n / (PN * PN);
-    } else {
-      lk = 0;
-      lj = n % PN;
-      li = n / PN;
-    }
-    const int gi = n0[0] + li, gj = n0[1] + lj, gk = n0[2] + lk;
-    if (gi < 0 || gj < 0 || gk < 0 || gi >= (int)H->N[0] || gj >= (int)H->N[1] || gk >= (int)H->N[2]) continue;
-    const uint32_t l = node_index(H, gi, gj, gk);
-#pragma unroll
-    for (int ch = 0; ch < NCH; ++ch) {
-      const double val = patch[ch][n];
-      if (val != 0.0) atomicAdd(&A.acc[(size_t)ch * cap + l], val);
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// 6. grid update, one thread per node
-// ---------------------------------------------------------------------------
-template <int D>
-__global__ void __launch_bounds__(256) k_grid(StepArgs A) {
-  StepHeader* H = A.H;
-  if (step_inactive(H)) return;
-  const DevParams& P = *A.P;
-  const uint32_t G = H->G, cap = A.cap_nodes;
-  const double dt = H->dt;
-  const double dtpv = dt * P.particle_volume;
-  double dtg[3];
-#pragma unroll
-  for (int a = 0; a < D; ++a) dtg[a] = dt * H->gravity[a];
-  __shared__ mtr_plate plates[MTR_MAXP];
-  for (int i = threadIdx.x; i < P.nplates; i += blockDim.x) plates[i] = H->plates[i];
-  __syncthreads();
-  constexpr int NCH = Tiling<D>::NCH;
-  for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < G; l += gridDim.x * blockDim.x) {
-    const double mraw = A.acc[l];
-    double v[3] = {0, 0, 0}, vold[3] = {0, 0, 0};
-    double fric = 0.0;
-    if (mraw > 0) {
-#pragma unroll
-      for (int a = 0; a < D; ++a) v[a] = A.acc[(size_t)(1 + a) * cap + l] / mraw;
-    }
-    if (P.use_mibf) fric = A.acc[(size_t)(1 + 2 * D) * cap + l] / mraw;
-    const double mi = mraw * P.particle_mass;
-    double fl[3] = {0, 0, 0};
-    if (mi > 0) {
-      uint32_t k = D == 3 ? l % H->N[2] : 0;
-      uint32_t r = D == 3 ? l / H->N[2] : l;
-      uint32_t jj = r % H->N[1], i = r / H->N[1];
-#pragma unroll
-      for (int a = 0; a < D; ++a) {
-        double inc = -dtpv * A.acc[(size_t)(1 + D + a) * cap + l] / mi + dtg[a];
-        vold[a] = v[a];
-        v[a] = vold[a] + inc;
-      }
-      double Xi[3] = {A.gx[i], A.gy[jj], D == 3 ? A.gz[k] : 0.0};
-      if (!boundary_collision<D>(P, plates, fric, Xi, dt, v)) raise_status(H, MTR_STATUS_BAD_BC, 0xffffffffu);
-#pragma unroll
-      for (int a = 0; a < D; ++a) fl[a] = v[a] - vold[a];
-    }
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      A.nv[(size_t)a * cap + l] = v[a];
-      A.nflip[(size_t)a * cap + l] = fl[a];
-    }
-    A.nmass[l] = mi;
-    if (P.use_mibf) A.nfric[l] = fric;
-#pragma unroll
-    for (int ch = 0; ch < NCH; ++ch) A.acc[(size_t)ch * cap + l] = 0.0;  // ready for the next step
-  }
-}
-
-// ---------------------------------------------------------------------------
-// particle I/O helpers
-// ---------------------------------------------------------------------------
-template <int D>
-struct PLoad {
-  double x[3], v[3], F[D][D];
-  PScalars s;
-  uint32_t id;
-};
-
-template <int D>
-__device__ __forceinline__ void load_particle(const PBuf& b, uint32_t Np, uint32_t j, PLoad<D>& p) {
-#pragma unroll
-  for (int a = 0; a < 3; ++a) p.x[a] = p.v[a] = 0.0;
-#pragma unroll
-  for (int a = 0; a < D; ++a) {
-    p.x[a] = b.x[(size_t)a * Np + j];
-    p.v[a] = b.v[(size_t)a * Np + j];
-  }
-#pragma unroll
-  for (int r = 0; r < D; ++r)
-#pragma unroll
-    for (int c = 0; c < D; ++c) p.F[r][c] = b.F[(size_t)(r * D + c) * Np + j];
-  p.s.eps_pl_dev = b.sc[(size_t)MTR_SCALAR_EPS_PL_DEV * Np + j];
-  p.s.eps_pl_vol = b.sc[(size_t)MTR_SCALAR_EPS_PL_VOL * Np + j];
-  p.s.eps_pl_vol_pradhana = b.sc[(size_t)MTR_SCALAR_EPS_PL_VOL_PRADHANA * Np + j];
-  p.s.delta_gamma = 0.0;  // deformation_update.cpp:13 zeroes it every step
-  p.s.viscosity = b.sc[(size_t)MTR_SCALAR_VISCOSITY * Np + j];
-  p.s.muI = b.sc[(size_t)MTR_SCALAR_MUI * Np + j];
-  p.id = b.id[j];
-}
-
-template <int D>
-__device__ __forceinline__ void store_defgrad(const PBuf& b, uint32_t Np, uint32_t s, const double (&F)[D][D],
-                                              const PScalars& sc, const double* tau) {
-#pragma unroll
-  for (int r = 0; r < D; ++r)
-#pragma unroll
-    for (int c = 0; c < D; ++c) b.F[(size_t)(r * D + c) * Np + s] = F[r][c];
-  b.sc[(size_t)MTR_SCALAR_EPS_PL_DEV * Np + s] = sc.eps_pl_dev;
-  b.sc[(size_t)MTR_SCALAR_EPS_PL_VOL * Np + s] = sc.eps_pl_vol;
-  b.sc[(size_t)MTR_SCALAR_EPS_PL_VOL_PRADHANA * Np + s] = sc.eps_pl_vol_pradhana;
-  b.sc[(size_t)MTR_SCALAR_DELTA_GAMMA * Np + s] = sc.delta_gamma;
-  b.sc[(size_t)MTR_SCALAR_VISCOSITY * Np + s] = sc.viscosity;
-  b.sc[(size_t)MTR_SCALAR_MUI * Np + s] = sc.muI;
-#pragma unroll
-  for (int q = 0; q < Sym<D>::n; ++q) b.tau[(size_t)q * Np + s] = tau[q];
-}
-
-// velocity blend of position_update.cpp:14-24 / musl.cpp:15-22
-__device__ __forceinline__ double blend_v(double fr, double v, double fl, double pic) {
-  if (fr < -1) return pic;
-  if (fr < 0) return (-fr) * (v + fl) + (1 - (-fr)) * pic;
-  return fr * (v + fl) + (1 - fr) * pic;
-}
-
-// Gathers pic, B, flip and grad v from the node arrays (g2p.cpp:24-77,
-// deformation_update.cpp:17-40).  The stencil base is not clamped (g2p.cpp:29).
-template <int D, int DEG, bool WANT_GRADV>
-__device__ __forceinline__ bool gather(const StepArgs& A, const StepHeader* H, const double* __restrict__ nv,
-                                       const double (&xp)[3], double (&pic)[3], double (&Bp)[D][D], double (&flp)[3],
-                                       double (&gv)[D][D], bool want_b, bool want_flip) {
-  const double ioh = A.P->one_over_dx;
-  const uint32_t cap = A.cap_nodes;
-  int base[3] = {0, 0, 0};
-  double w[3][4], dw[3][4], crd[3][4];
-#pragma unroll
-  for (int a = 0; a < D; ++a) {
-    base[a] = (int)(floor((xp[a] - H->org[a]) * ioh) - 1);
-    if (base[a] < 0 || base[a] + 3 >= (int)H->N[a]) return false;
-    const double* ax = a == 0 ? A.gx : (a == 1 ? A.gy : A.gz);
-#pragma unroll
-    for (int o = 0; o < 4; ++o) crd[a][o] = ax[base[a] + o];
-    axis_weights<DEG>(xp[a], crd[a], ioh, w[a], dw[a]);
-  }
-#pragma unroll
-  for (int a = 0; a < 3; ++a) pic[a] = flp[a] = 0.0;
-#pragma unroll
-  for (int r = 0; r < D; ++r)
-#pragma unroll
-    for (int c = 0; c < D; ++c) Bp[r][c] = gv[r][c] = 0.0;
-  constexpr int KN = D == 3 ? 4 : 1;
-#pragma unroll
-  for (int ii = 0; ii < 4; ++ii)
-#pragma unroll
-    for (int jj = 0; jj < 4; ++jj)
-#pragma unroll
-      for (int kk = 0; kk < KN; ++kk) {
-        const uint32_t l = D == 3 ? node_index(H, base[0] + ii, base[1] + jj, base[2] + kk)
-                                  : node_index(H, base[0] + ii, base[1] + jj, 0);
-        const double wxy = w[0][ii] * w[1][jj];
-        const double weight = D == 3 ? wxy * w[2][kk] : wxy;
-        double vi[3] = {0, 0, 0};
-#pragma unroll
-        for (int a = 0; a < D; ++a) vi[a] = __ldg(&nv[(size_t)a * cap + l]);
-#pragma unroll
-        for (int a = 0; a < D; ++a) pic[a] += vi[a] * weight;
-        if (want_b) {
-          double pd[3] = {crd[0][ii] - xp[0], crd[1][jj] - xp[1], D == 3 ? crd[2][kk] - xp[2] : 0.0};
-#pragma unroll
-          for (int r = 0; r < D; ++r)
-#pragma unroll
-            for (int c = 0; c < D; ++c) Bp[r][c] += vi[r] * pd[c] * weight;
-        }
-        if (want_flip) {
-#pragma unroll
-          for (int a = 0; a < D; ++a) flp[a] += __ldg(&A.nflip[(size_t)a * cap + l]) * weight;
-        }
-        if (WANT_GRADV) {
-          double g[3];
-          if constexpr (D == 3) {
-            g[0] = dw[0][ii] * w[1][jj] * w[2][kk] * ioh;
-            g[1] = dw[1][jj] * w[0][ii] * w[2][kk] * ioh;
-            g[2] = dw[2][kk] * w[0][ii] * w[1][jj] * ioh;
-          } else {
-            g[0] = dw[0][ii] * w[1][jj] * ioh;
-            g[1] = dw[1][jj] * w[0][ii] * ioh;
-          }
-#pragma unroll
-          for (int r = 0; r < D; ++r)
-#pragma unroll
-            for (int c = 0; c < D; ++c) gv[r][c] += vi[r] * g[c];
-        }
-      }
-  return true;
-}
-
-// F_trial = F + dt * gradv * F (deformation_update.cpp:42-44), then the
-// return mapping; writes F, scalars and tau into the out buffer at slot s.
-template <int D>
-__device__ __forceinline__ void defgrad_and_store(const StepArgs& A, uint32_t s, double dt, PLoad<D>& p,
-                                                  const double (&gv)[D][D], uint32_t& flags, bool& plastic) {
-  double T1[D][D], T2[D][D];
-#pragma unroll
-  for (int r = 0; r < D; ++r)
-#pragma unroll
-    for (int c = 0; c < D; ++c) T1[r][c] = dt * gv[r][c];
-  mat_mul<D>(T1, p.F, T2);
-#pragma unroll
-  for (int r = 0; r < D; ++r)
-#pragma unroll
-    for (int c = 0; c < D; ++c) p.F[r][c] = p.F[r][c] + T2[r][c];
-  double tau[Sym<D>::n];
-  plastic = return_map<D>(*A.P, dt, p.F, p.s, tau, flags);
-  store_defgrad<D>(A.out, A.Np, s, p.F, p.s, tau);
-}
-
-__device__ __forceinline__ void count_plastic(StepHeader* H, bool plastic) {
-  const unsigned m = __ballot_sync(__activemask(), plastic);
-  if ((threadIdx.x & 31) == __ffs(__activemask()) - 1 && m) atomicAdd(&H->plastic_count, (unsigned long long)__popc(m));
-}
-
-// ---------------------------------------------------------------------------
-// 7a. USL: fused G2P + deformation update + return mapping + position update
-// ---------------------------------------------------------------------------
-template <int D, int DEG>
-__global__ void __launch_bounds__(128) k_g2p(StepArgs A, const uint32_t* __restrict__ perm) {
-  StepHeader* H = A.H;
-  if (step_inactive(H)) return;
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= A.Np) return;
-  const DevParams& P = *A.P;
-  const uint32_t Np = A.Np, j = perm[s];
-  const double dt = H->dt;
-  const double fr = P.flip_ratio;
-  PLoad<D> p;
-  load_particle<D>(A.in, Np, j, p);
-  double pic[3], flp[3], Bp[D][D], gv[D][D];
-  if (!gather<D, DEG, true>(A, H, A.nv, p.x, pic, Bp, flp, gv, fr < 0, fr >= -1)) {
-    raise_status(H, MTR_STATUS_STENCIL_OOB, p.id);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) pic[a] = flp[a] = 0.0;
-#pragma unroll
-    for (int r = 0; r < D; ++r)
-#pragma unroll
-      for (int c = 0; c < D; ++c) Bp[r][c] = gv[r][c] = 0.0;
-  }
-  uint32_t flags = 0;
-  bool plastic = false;
-  defgrad_and_store<D>(A, s, dt, p, gv, flags, plastic);
-  // positionUpdate (position_update.cpp:6-46)
-  double xn[3], vn[3];
-#pragma unroll
-  for (int a = 0; a < D; ++a) {
-    xn[a] = p.x[a] + dt * pic[a];
-    vn[a] = blend_v(fr, p.v[a], flp[a], pic[a]);
-  }
-  if (P.change_particle_positions && xn[0] > 0.8) {  // position_update.cpp:35-41
-    xn[0] = -0.1;
-    xn[1] += 0.27;
-  }
-#pragma unroll
-  for (int a = 0; a < D; ++a) {
-    A.out.x[(size_t)a * Np + s] = xn[a];
-    A.out.v[(size_t)a * Np + s] = vn[a];
-  }
-#pragma unroll
-  for (int r = 0; r < D; ++r)
-#pragma unroll
-    for (int c = 0; c < D; ++c) A.out.B[(size_t)(r * D + c) * Np + s] = (fr < 0) ? Bp[r][c] : 0.0;
-  A.out.id[s] = p.id;
-  if (P.store_pic_flip) {
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      A.pic[(size_t)a * Np + s] = pic[a];
-      A.flip[(size_t)a * Np + s] = (fr >= -1) ? flp[a] : 0.0;
-    }
-  }
-  if (flags) raise_status(H, flags, p.id);
-  count_plastic(H, plastic);
-}
-
-// ---------------------------------------------------------------------------
-// 7b. MUSL (musl.cpp:6-96): G2P, velocity blend and re-scatter of
-// v_p + B D^-1 (x_i - x_p), one block per tile
-// ---------------------------------------------------------------------------
-template <int D, int DEG>
-__global__ void __launch_bounds__(128) k_g2p_musl(StepArgs A, const uint32_t* __restrict__ perm) {
-  using TL = Tiling<D>;
-  constexpr int PN = TL::PN, NODES = TL::NODES, TB = TL::TB;
-  StepHeader* H = A.H;
-  if (step_inactive(H)) return;
-  const uint32_t t = blockIdx.x;
-  if (t >= H->ntiles) return;
-  const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
-  if (pb >= pe) return;
-  const DevParams& P = *A.P;
-  __shared__ double patch[D][NODES];
-  __shared__ double crd[3][PN];
-  int tc[3];
-  tile_coords<D>(H, t, tc);
-  int n0[3] = {tc[0] * TB - 1, tc[1] * TB - 1, D == 3 ? tc[2] * TB - 1 : 0};
-  for (int i = threadIdx.x; i < D * NODES; i += blockDim.x) (&patch[0][0])[i] = 0.0;
-  for (int i = threadIdx.x; i < D * PN; i += blockDim.x) {
-    const int a = i / PN, o = i % PN;
-    const int g = n0[a] + o;
-    const double* ax = a == 0 ? A.gx : (a == 1 ? A.gy : A.gz);
-    crd[a][o] = (g >= 0 && g < (int)H->N[a]) ? ax[g] : 0.0;
-  }
-  __syncthreads();
-  const uint32_t Np = A.Np;
-  const double dt = H->dt, fr = P.flip_ratio, ioh = P.one_over_dx;
-  for (uint32_t s = pb + threadIdx.x; s < pe; s += blockDim.x) {
-    const uint32_t j = perm[s];
-    double xp[3] = {0, 0, 0}, vp[3] = {0, 0, 0};
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      xp[a] = A.in.x[(size_t)a * Np + j];
-      vp[a] = A.in.v[(size_t)a * Np + j];
-    }
-    const uint32_t pid = A.in.id[j];
-    double pic[3], flp[3], Bp[D][D], gv[D][D];
-    if (!gather<D, DEG, false>(A, H, A.nv, xp, pic, Bp, flp, gv, fr < 0, fr >= -1)) {
-      raise_status(H, MTR_STATUS_STENCIL_OOB, pid);
-      continue;
-    }
-    double vn[3] = {0, 0, 0};
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      vn[a] = blend_v(fr, vp[a], flp[a], pic[a]);
-      A.out.x[(size_t)a * Np + s] = xp[a] + dt * pic[a];  // positionUpdate: x + dt pic
-      A.out.v[(size_t)a * Np + s] = vn[a];
-    }
-#pragma unroll
-    for (int r = 0; r < D; ++r)
-#pragma unroll
-      for (int c = 0; c < D; ++c) A.out.B[(size_t)(r * D + c) * Np + s] = (fr < 0) ? Bp[r][c] : 0.0;
-    A.out.id[s] = pid;
-    if (P.store_pic_flip) {
-#pragma unroll
-      for (int a = 0; a < D; ++a) {
-        A.pic[(size_t)a * Np + s] = pic[a];
-        A.flip[(size_t)a * Np + s] = (fr >= -1) ? flp[a] : 0.0;
-      }
-    }
-    // re-scatter (musl.cpp:35-76), base clamped at zero like P2G
-    int lb[3] = {0, 0, 0};
-    bool oob = false;
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      int b = (int)floor((xp[a] - H->org[a]) * ioh) - 1;
-      b = b < 0 ? 0 : b;
-      lb[a] = b - n0[a];
-      if (lb[a] < 0 || lb[a] > PN - 4) oob = true;
-    }
-    if (oob) {
-      raise_status(H, MTR_STATUS_STENCIL_OOB, pid);
-      continue;
-    }
-    double w[3][4], dw[3][4];
-#pragma unroll
-    for (int a = 0; a < D; ++a) axis_weights<DEG>(xp[a], &crd[a][lb[a]], ioh, w[a], dw[a]);
-    constexpr int KN = D == 3 ? 4 : 1;
-#pragma unroll
-    for (int ii = 0; ii < 4; ++ii)
-#pragma unroll
-      for (int jj = 0; jj < 4; ++jj)
-#pragma unroll
-        for (int kk = 0; kk < KN; ++kk) {
-          const double wxy = w[0][ii] * w[1][jj];
-          const double weight = D == 3 ? wxy * w[2][kk] : wxy;
-          if (!(weight > 1e-25)) continue;
-          const int node = D == 3 ? ((lb[0] + ii) * PN + (lb[1] + jj)) * PN + (lb[2] + kk)
-                                  : (lb[0] + ii) * PN + (lb[1] + jj);
-          double pd[3] = {crd[0][lb[0] + ii] - xp[0], crd[1][lb[1] + jj] - xp[1],
-                          D == 3 ? crd[2][lb[2] + kk] - xp[2] : 0.0};
-#pragma unroll
-          for (int a = 0; a < D; ++a) {
-            double m = vn[a] * weight;
-            if (fr < 0) {
-              double bv = Bp[a][0] * pd[0];
-#pragma unroll
-              for (int c = 1; c < D; ++c) bv += Bp[a][c] * pd[c];
-              m += bv * P.apicDinverse * weight;
-            }
-            atomicAdd(&patch[a][node], m);
-          }
-        }
-  }
-  __syncthreads();
-  const uint32_t cap = A.cap_nodes;
-  for (int n = threadIdx.x; n < NODES; n += blockDim.x) {
-    int li, lj, lk;
-    if constexpr (D == 3) {
-      lk = n % PN;
-      lj = (n / PN) % PN;
-      li = n / (PN * PN);
-    } else {
-      lk = 0;
-      lj = n % PN;
-      li = n / PN;
-    }
-    const int gi = n0[0] + li, gj = n0[1] + lj, gk = n0[2] + lk;
-    if (gi < 0 || gj < 0 || gk < 0 || gi >= (int)H->N[0] || gj >= (int)H->N[1] || gk >= (int)H->N[2]) continue;
-    const uint32_t l = node_index(H, gi, gj, gk);
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      const double val = patch[a][n];
-      if (val != 0.0) atomicAdd(&A.v2[(size_t)a * cap + l], val);
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Tile-structured gathers.  A tile block first copies the node values its
-// particles' stencils can reach (the PN^D patch of the tile) from the node
-// arrays into shared memory, then every particle gathers from there.
-// ---------------------------------------------------------------------------
-template <int D>
-__device__ __forceinline__ void load_tile_setup(const StepArgs& A, const StepHeader* H, uint32_t t, int (&n0)[3],
+__device__ __forceinline__ void load_tile_setup(const StepCommon& A, const StepHeader* H, uint32_t t, int (&n0)[3],
                                                 double (*crd)[Tiling<D>::PN]) {
   constexpr int PN = Tiling<D>::PN, TB = Tiling<D>::TB;
   int tc[3];
@@ -1242,111 +535,6 @@ __device__ __forceinline__ void load_tile_setup(const StepArgs& A, const StepHea
     const int g = n0[a] + o;
     const double* ax = a == 0 ? A.gx : (a == 1 ? A.gy : A.gz);
     crd[a][o] = (g >= 0 && g < (int)H->N[a]) ? ax[g] : 0.0;
-  }
-}
-
-// copies NF fields of D components each, src[f] = [D][cap] node arrays
-template <int D, int NF>
-__device__ __forceinline__ void load_node_patch(const StepArgs& A, const StepHeader* H, const int (&n0)[3],
-                                                const double* const (&src)[NF], double* dst /*[NF*D][NODES]*/) {
-  constexpr int PN = Tiling<D>::PN, NODES = Tiling<D>::NODES;
-  const uint32_t cap = A.cap_nodes;
-  for (int n = threadIdx.x; n < NODES; n += blockDim.x) {
-    int li, lj, lk;
-    if constexpr (D == 3) {
-      lk = n % PN;
-      lj = (n / PN) % PN;
-      li = n / (PN * PN);
-    } else {
-      lk = 0;
-      lj = n % PN;
-      li = n / PN;
-    }
-    const int gi = n0[0] + li, gj = n0[1] + lj, gk = n0[2] + lk;
-    const bool in = gi >= 0 && gj >= 0 && gk >= 0 && gi < (int)H->N[0] && gj < (int)H->N[1] && gk < (int)H->N[2];
-    const uint32_t l = in ? node_index(H, gi, gj, gk) : 0u;
-#pragma unroll
-    for (int f = 0; f < NF; ++f)
-#pragma unroll
-      for (int a = 0; a < D; ++a) dst[(f * D + a) * NODES + n] = in ? src[f][(size_t)a * cap + l] : 0.0;
-  }
-}
-
-// G2P gather (g2p.cpp:24-77) and velocity gradient (deformation_update.cpp:17-40)
-// from a shared node patch; lb = stencil base relative to the patch origin.
-// Sums are factorised over the tensor-product stencil.
-template <int D, int DEG, bool GRADV>
-__device__ __forceinline__ void gather_patch(const double* pv, const double* pf, const double (*crd)[Tiling<D>::PN],
-                                             const int (&lb)[3], const double (&xp)[3], double ioh, double (&pic)[3],
-                                             double (&Bp)[D][D], double (&flp)[3], double (&gv)[D][D], bool want_b,
-                                             bool want_flip) {
-  constexpr int PN = Tiling<D>::PN, NODES = Tiling<D>::NODES;
-  double w[3][4], dw[3][4], pd[3][4];
-#pragma unroll
-  for (int a = 0; a < D; ++a)
-#pragma unroll
-    for (int o = 0; o < 4; ++o) {
-      const double c = crd[a][lb[a] + o];
-      const double u = (xp[a] - c) * ioh;
-      w[a][o] = bspline_N<DEG>(u);
-      dw[a][o] = GRADV ? bspline_dN<DEG>(u) : 0.0;
-      pd[a][o] = c - xp[a];
-    }
-#pragma unroll
-  for (int a = 0; a < 3; ++a) pic[a] = flp[a] = 0.0;
-#pragma unroll
-  for (int r = 0; r < D; ++r)
-#pragma unroll
-    for (int c = 0; c < D; ++c) Bp[r][c] = gv[r][c] = 0.0;
-  constexpr int KN = D == 3 ? 4 : 1;
-#pragma unroll
-  for (int ii = 0; ii < 4; ++ii)
-#pragma unroll
-    for (int jj = 0; jj < 4; ++jj) {
-      const double wxy = w[0][ii] * w[1][jj];
-      const double gx_ = dw[0][ii] * w[1][jj], gy_ = w[0][ii] * dw[1][jj];
-#pragma unroll
-      for (int kk = 0; kk < KN; ++kk) {
-        const int node = D == 3 ? ((lb[0] + ii) * PN + (lb[1] + jj)) * PN + (lb[2] + kk) : (lb[0] + ii) * PN + (lb[1] + jj);
-        const double weight = D == 3 ? wxy * w[2][kk] : wxy;
-        double vi[D];
-#pragma unroll
-        for (int a = 0; a < D; ++a) vi[a] = pv[a * NODES + node];
-#pragma unroll
-        for (int a = 0; a < D; ++a) pic[a] += vi[a] * weight;
-        if (want_b) {
-          double wpd[3] = {weight * pd[0][ii], weight * pd[1][jj], D == 3 ? weight * pd[2][kk] : 0.0};
-#pragma unroll
-          for (int r = 0; r < D; ++r)
-#pragma unroll
-            for (int c = 0; c < D; ++c) Bp[r][c] += vi[r] * wpd[c];
-        }
-        if (want_flip) {
-#pragma unroll
-          for (int a = 0; a < D; ++a) flp[a] += pf[a * NODES + node] * weight;
-        }
-        if (GRADV) {
-          double g[3];
-          if constexpr (D == 3) {
-            g[0] = gx_ * w[2][kk];
-            g[1] = gy_ * w[2][kk];
-            g[2] = wxy * dw[2][kk];
-          } else {
-            g[0] = gx_;
-            g[1] = gy_;
-          }
-#pragma unroll
-          for (int r = 0; r < D; ++r)
-#pragma unroll
-            for (int c = 0; c < D; ++c) gv[r][c] += vi[r] * g[c];
-        }
-      }
-    }
-  if (GRADV) {
-#pragma unroll
-    for (int r = 0; r < D; ++r)
-#pragma unroll
-      for (int c = 0; c < D; ++c) gv[r][c] *= ioh;
   }
 }
 
@@ -1367,170 +555,121 @@ __device__ __forceinline__ bool local_base(const StepHeader* H, const double (&x
   return ok;
 }
 
-// USL: G2P + deformation update + return mapping + position update, one
-// block per tile, node patch in shared memory.
-template <int D, int DEG>
-__global__ void __launch_bounds__(kChunk) k_g2p_t(StepArgs A, const uint32_t* __restrict__ perm) {
-  using TL = Tiling<D>;
-  constexpr int PN = TL::PN, NODES = TL::NODES;
-  StepHeader* H = A.H;
-  if (step_inactive(H)) return;
-  const uint32_t t = blockIdx.x;
-  if (t >= H->ntiles) return;
-  const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
-  if (pb >= pe) return;
-  const DevParams& P = *A.P;
-  __shared__ double pv[2 * D * NODES];
-  __shared__ double crd[3][PN];
-  int n0[3];
-  load_tile_setup<D>(A, H, t, n0, crd);
-  const double* const src[2] = {A.nv, A.nflip};
-  load_node_patch<D, 2>(A, H, n0, src, pv);
-  __syncthreads();
-  const uint32_t Np = A.Np;
-  const double dt = H->dt, fr = P.flip_ratio, ioh = P.one_over_dx;
-  uint32_t flags = 0;
-  bool any_plastic = false;
-  for (uint32_t s = pb + threadIdx.x; s < pe; s += blockDim.x) {
-    const uint32_t j = perm[s];
-    PLoad<D> p;
-    load_particle<D>(A.in, Np, j, p);
-    double pic[3], flp[3], Bp[D][D], gv[D][D];
-    int lb[3];
-    if (local_base<D>(H, p.x, ioh, n0, false, lb)) {
-      gather_patch<D, DEG, true>(pv, pv + D * NODES, crd, lb, p.x, ioh, pic, Bp, flp, gv, fr < 0, fr >= -1);
-    } else {
-      raise_status(H, MTR_STATUS_STENCIL_OOB, p.id);
-#pragma unroll
-      for (int a = 0; a < 3; ++a) pic[a] = flp[a] = 0.0;
-#pragma unroll
-      for (int r = 0; r < D; ++r)
-#pragma unroll
-        for (int c = 0; c < D; ++c) Bp[r][c] = gv[r][c] = 0.0;
-    }
-    uint32_t f = 0;
-    bool plastic = false;
-    defgrad_and_store<D>(A, s, dt, p, gv, f, plastic);
-    flags |= f;
-    if (f) raise_status(H, f, p.id);
-    any_plastic |= plastic;
-    if (plastic) atomicAdd(&H->plastic_count, 1ull);
-    double xn[3], vn[3];
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      xn[a] = p.x[a] + dt * pic[a];
-      vn[a] = blend_v(fr, p.v[a], flp[a], pic[a]);
-    }
-    if (P.change_particle_positions && xn[0] > 0.8) {  // position_update.cpp:35-41
-      xn[0] = -0.1;
-      xn[1] += 0.27;
-    }
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      A.out.x[(size_t)a * Np + s] = xn[a];
-      A.out.v[(size_t)a * Np + s] = vn[a];
-    }
-#pragma unroll
-    for (int r = 0; r < D; ++r)
-#pragma unroll
-      for (int c = 0; c < D; ++c) A.out.B[(size_t)(r * D + c) * Np + s] = (fr < 0) ? Bp[r][c] : 0.0;
-    A.out.id[s] = p.id;
-    if (P.store_pic_flip) {
-#pragma unroll
-      for (int a = 0; a < D; ++a) {
-        A.pic[(size_t)a * Np + s] = pic[a];
-        A.flip[(size_t)a * Np + s] = (fr >= -1) ? flp[a] : 0.0;
-      }
-    }
-  }
-}
-
-// MUSL: deformation update from the normalised re-projected velocity v2 and
-// the old positions (deformation_update.cpp:6), then the return mapping.
-template <int D, int DEG>
-__global__ void __launch_bounds__(kChunk) k_defgrad_t(StepArgs A, const uint32_t* __restrict__ perm) {
-  using TL = Tiling<D>;
-  constexpr int PN = TL::PN, NODES = TL::NODES;
-  StepHeader* H = A.H;
-  if (step_inactive(H)) return;
-  const uint32_t t = blockIdx.x;
-  if (t >= H->ntiles) return;
-  const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
-  if (pb >= pe) return;
-  __shared__ double pv[D * NODES];
-  __shared__ double crd[3][PN];
-  int n0[3];
-  load_tile_setup<D>(A, H, t, n0, crd);
-  const double* const src[1] = {A.v2};
-  load_node_patch<D, 1>(A, H, n0, src, pv);
-  __syncthreads();
-  const uint32_t Np = A.Np;
-  const double dt = H->dt, ioh = A.P->one_over_dx;
-  for (uint32_t s = pb + threadIdx.x; s < pe; s += blockDim.x) {
-    const uint32_t j = perm[s];
-    PLoad<D> p;
-    load_particle<D>(A.in, Np, j, p);
-    double pic[3], flp[3], Bp[D][D], gv[D][D];
-    int lb[3];
-    if (local_base<D>(H, p.x, ioh, n0, false, lb)) {
-      gather_patch<D, DEG, true>(pv, nullptr, crd, lb, p.x, ioh, pic, Bp, flp, gv, false, false);
-    } else {
-      raise_status(H, MTR_STATUS_STENCIL_OOB, p.id);
-#pragma unroll
-      for (int r = 0; r < D; ++r)
-#pragma unroll
-        for (int c = 0; c < D; ++c) gv[r][c] = 0.0;
-    }
-    uint32_t f = 0;
-    bool plastic = false;
-    defgrad_and_store<D>(A, s, dt, p, gv, f, plastic);
-    if (f) raise_status(H, f, p.id);
-    if (plastic) atomicAdd(&H->plastic_count, 1ull);
-  }
-}
-
-// MUSL (musl.cpp:6-96), one block per tile.  Phase 1 (thread per particle):
-// gather pic/B/flip from the shared node patch, blend v, write x + dt pic, v,
-// B; stage v_new, B_new and the re-scatter weights.  Phase 2 (lane groups
-// owning stencil columns): accumulate v_p + B D^-1 (x_i - x_p) per cell in
-// registers, add once per cell to the shared re-projection patch.
+// global node of patch entry n, or false outside the grid
 template <int D>
-struct MStage {
-  double x[D], v[D], B[D * D], w[D * 4];
-  int lb;
+__device__ __forceinline__ bool patch_node(const StepHeader* H, const int (&n0)[3], int n, uint32_t& l) {
+  constexpr int PN = Tiling<D>::PN;
+  int li, lj, lk;
+  if constexpr (D == 3) {
+    lk = n % PN;
+    lj = (n / PN) % PN;
+    li = n / (PN * PN);
+  } else {
+    lk = 0;
+    lj = n % PN;
+    li = n / PN;
+  }
+  const int gi = n0[0] + li, gj = n0[1] + lj, gk = n0[2] + lk;
+  if (gi < 0 || gj < 0 || gk < 0 || gi >= (int)H->N[0] || gj >= (int)H->N[1] || gk >= (int)H->N[2]) return false;
+  l = node_index(H, gi, gj, gk);
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// 5. P2G + stress force, warp-cooperative, one block per tile.
+//
+// A tile block walks its sorted particles in chunks of kChunk.  Phase 1, one
+// thread per particle, loads the particle and stages its stencil weights and
+// gradients in shared memory.  Phase 2: lane groups (3D: 16 lanes, 2D: 4 lanes)
+// take consecutive staged particles; a lane owns one stencil column of the
+// particle's cell (3D: (iy, iz) and its 4 ix nodes, 2D: iy and its 4 ix
+// nodes), accumulates every channel in registers while consecutive particles
+// share a cell, and adds them to the shared patch once per cell.  Sorted
+// particles share cells in runs of about ppc, so this issues ~ppc times fewer
+// shared atomics than one atomic per particle and node, with no two lanes of
+// a group on one address.  The patch is flushed with one global atomic per
+// node and channel.
+// ---------------------------------------------------------------------------
+constexpr int kChunk = 128;
+
+// Minimum resident blocks per SM requested for the tile kernels that run the
+// return mapping (k_g2p_t, k_defgrad_t); it bounds their registers per thread.
+#ifndef MTR_RM_MIN_BLOCKS
+#define MTR_RM_MIN_BLOCKS 1
+#endif
+
+// FP64 stage: the position is kept and node offsets are formed in phase 2.
+template <int D, typename R = double>
+struct PStage {
+  double x[D], v[D], B[D * D], tau[Sym<D>::n], w[D * 4], dw[D * 4];
+  double mui;
+  int lb;  // packed local stencil base (4 bits per axis); -1 marks an empty slot
   int pad;
 };
 
+// FP32 stage: node offsets x_i - x_p are formed in FP64 in phase 1 and
+// stored rounded, so phase 2 runs in FP32 only.
 template <int D>
-constexpr size_t musl_smem_bytes() {
-  return sizeof(double) * ((3 * D) * Tiling<D>::NODES + 3 * Tiling<D>::PN) + sizeof(MStage<D>) * kChunk;
+struct PStage<D, float> {
+  float pd[D * 4], v[D], B[D * D], tau[Sym<D>::n], w[D * 4], dw[D * 4];
+  float mui;
+  int lb;
+};
+
+template <int D, typename R>
+__device__ __forceinline__ R stage_pd(const PStage<D, R>& S, const double (*crd)[Tiling<D>::PN], int a, int lba,
+                                      int o) {
+  if constexpr (kFP64<R>)
+    return crd[a][lba + o] - S.x[a];
+  else
+    return S.pd[a * 4 + o];
 }
 
-template <int D, int DEG>
-__global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgs A, const uint32_t* __restrict__ perm) {
+template <int D, typename R>
+constexpr size_t p2g_crd_bytes() {
+  return align16(sizeof(double) * 3 * Tiling<D>::PN);
+}
+template <int D, typename R>
+constexpr size_t p2g_patch_bytes() {
+  return align16(sizeof(R) * Tiling<D>::NCH * Tiling<D>::NODES);
+}
+template <int D, typename R>
+constexpr size_t p2g_smem_bytes() {
+  return p2g_crd_bytes<D, R>() + p2g_patch_bytes<D, R>() + sizeof(PStage<D, R>) * kChunk;
+}
+
+template <int D, int DEG, typename R>
+__global__ void __launch_bounds__(kChunk) k_p2g_w(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
   using TL = Tiling<D>;
-  constexpr int PN = TL::PN, NODES = TL::NODES;
-  StepHeader* H = A.H;
+  constexpr int PN = TL::PN, NODES = TL::NODES, NCH = TL::NCH, TB = TL::TB;
+  constexpr int NS = Sym<D>::n;
+  const StepHeader* H = A.H;
   if (step_inactive(H)) return;
   const uint32_t t = blockIdx.x;
   if (t >= H->ntiles) return;
   const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
   if (pb >= pe) return;
   const DevParams& P = *A.P;
-  extern __shared__ double smem[];
-  double* pv = smem;                                              // [2D][NODES] node v, flip
-  double(*vsum)[NODES] = reinterpret_cast<double(*)[NODES]>(smem + 2 * D * NODES);  // [D][NODES]
-  double(*crd)[PN] = reinterpret_cast<double(*)[PN]>(smem + 3 * D * NODES);
-  MStage<D>* st = reinterpret_cast<MStage<D>*>(smem + 3 * D * NODES + 3 * PN);
-  int n0[3];
-  load_tile_setup<D>(A, H, t, n0, crd);
-  const double* const src[2] = {A.nv, A.nflip};
-  load_node_patch<D, 2>(A, H, n0, src, pv);
-  for (int i = threadIdx.x; i < D * NODES; i += blockDim.x) (&vsum[0][0])[i] = 0.0;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double(*crd)[PN] = reinterpret_cast<double(*)[PN]>(smem_raw);
+  R(*patch)[NODES] = reinterpret_cast<R(*)[NODES]>(smem_raw + p2g_crd_bytes<D, R>());
+  PStage<D, R>* st = reinterpret_cast<PStage<D, R>*>(smem_raw + p2g_crd_bytes<D, R>() + p2g_patch_bytes<D, R>());
+  int tc[3];
+  tile_coords<D>(H, t, tc);
+  const int n0[3] = {tc[0] * TB - 1, tc[1] * TB - 1, D == 3 ? tc[2] * TB - 1 : 0};
+  for (int i = threadIdx.x; i < NCH * NODES; i += blockDim.x) (&patch[0][0])[i] = R(0.0);
+  for (int i = threadIdx.x; i < D * PN; i += blockDim.x) {
+    const int a = i / PN, o = i % PN;
+    const int g = n0[a] + o;
+    const double* ax = a == 0 ? A.gx : (a == 1 ? A.gy : A.gz);
+    crd[a][o] = (g >= 0 && g < (int)H->N[a]) ? ax[g] : 0.0;
+  }
   __syncthreads();
   const uint32_t Np = A.Np;
-  const double dt = H->dt, fr = P.flip_ratio, ioh = P.one_over_dx, apicD = P.apicDinverse;
-  const bool apic = fr < 0;
+  const double ioh = P.one_over_dx;
+  const R iohR = (R)ioh, apicD = (R)P.apicDinverse;
+  const bool apic = P.flip_ratio < 0;
+  const bool mibf = P.use_mibf;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int LPP = D == 3 ? 16 : 4;
   const int q = lane % LPP;
@@ -1542,9 +681,561 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgs A, const uint32_
   // cell at once, which measured slower despite fewer bank conflicts)
   const int kbeg = warp * 32 + (lane / LPP) * LPP, kend = kbeg + LPP;
   for (uint32_t c0 = pb; c0 < pe; c0 += kChunk) {
+    {  // phase 1: stage one particle per thread
+      const uint32_t s = c0 + threadIdx.x;
+      PStage<D, R>& S = st[threadIdx.x];
+      int packed = -1;
+      if (s < pe) {
+        const uint32_t j = perm[s];
+        double xp[3] = {0.0, 0.0, 0.0};
+        int lb[3] = {0, 0, 0};
+        bool oob = false;
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+          xp[a] = A.in.x[(size_t)a * Np + j];
+          if constexpr (kFP64<R>) S.x[a] = xp[a];
+          S.v[a] = A.in.v[(size_t)a * Np + j];
+          int b = (int)floor((xp[a] - H->org[a]) * ioh) - 1;
+          b = b < 0 ? 0 : b;  // p2g.cpp:21-24 clamps at zero
+          lb[a] = b - n0[a];
+          if (lb[a] < 0 || lb[a] > PN - 4 || b + 3 >= (int)H->N[a]) oob = true;
+        }
+#pragma unroll
+        for (int q = 0; q < D * D; ++q) S.B[q] = apic ? A.in.B[(size_t)q * Np + j] : R(0.0);
+#pragma unroll
+        for (int q = 0; q < NS; ++q) S.tau[q] = A.in.tau[(size_t)q * Np + j];
+        // MIBF friction is accumulated as the deviation from its initial value
+        // mui0, so a uniform field reproduces mui0 exactly at every node
+        S.mui = mibf ? (R)((double)A.in.sc[(size_t)MTR_SCALAR_MUI * Np + j] - P.mui0) : R(0.0);
+        if (oob) {
+          raise_status(A.H, MTR_STATUS_STENCIL_OOB, A.in.id[j]);
+        } else {
+#pragma unroll
+          for (int a = 0; a < D; ++a) {
+#pragma unroll
+            for (int o = 0; o < 4; ++o) {
+              const double c = crd[a][lb[a] + o];
+              const R u = (R)((xp[a] - c) * ioh);
+              S.w[a * 4 + o] = bspline_N<DEG>(u);
+              S.dw[a * 4 + o] = bspline_dN<DEG>(u);
+              if constexpr (!kFP64<R>) S.pd[a * 4 + o] = (R)(c - xp[a]);
+            }
+          }
+          packed = lb[0] | (lb[1] << 4) | (lb[2] << 8);
+        }
+      }
+      S.lb = packed;
+    }
+    __syncthreads();
+    {  // phase 2: a lane owns one (iy, iz) stencil column and its 4 ix nodes
+      R acc[4][NCH];
+#pragma unroll
+      for (int h = 0; h < 4; ++h)
+#pragma unroll
+        for (int ch = 0; ch < NCH; ++ch) acc[h][ch] = R(0.0);
+      int cur = -1;
+      auto flush = [&]() {
+        const int lbx = cur & 15, lby = (cur >> 4) & 15, lbz = cur >> 8;
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          const int node = D == 3 ? ((lbx + h) * PN + (lby + iy)) * PN + (lbz + iz) : (lbx + h) * PN + (lby + iy);
+#pragma unroll
+          for (int ch = 0; ch < NCH; ++ch) {
+            if (acc[h][ch] != R(0.0)) atomicAdd(&patch[ch][node], acc[h][ch]);
+            acc[h][ch] = R(0.0);
+          }
+        }
+      };
+      for (int k = kbeg; k < kend; ++k) {
+        const PStage<D, R>& S = st[k];
+        const int lbp = S.lb;
+        if (lbp < 0) continue;
+        if (lbp != cur) {
+          if (cur >= 0) flush();
+          cur = lbp;
+        }
+        const int lbx = lbp & 15, lby = (lbp >> 4) & 15, lbz = lbp >> 8;
+        // tensor-product factors of this lane's column
+        const R wy = S.w[4 + iy], dwy = S.dw[4 + iy];
+        R wyz, G0, G1, G2 = R(0.0);
+        if constexpr (D == 3) {
+          const R wz = S.w[8 + iz], dwz = S.dw[8 + iz];
+          wyz = wy * wz;
+          G0 = wyz * iohR;
+          G1 = dwy * wz * iohR;
+          G2 = wy * dwz * iohR;
+        } else {
+          wyz = wy;
+          G0 = wy * iohR;
+          G1 = dwy * iohR;
+        }
+        // force f_a = tau_a . grad w = dwx * Pf_a + wx * Qf_a
+        R Pf[D], Qf[D];
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+          Pf[a] = sym_at<D>(S.tau, a, 0) * G0;
+          R q = sym_at<D>(S.tau, a, 1) * G1;
+          if constexpr (D == 3) q += sym_at<D>(S.tau, a, 2) * G2;
+          Qf[a] = q;
+        }
+        // momentum per weight: v_a + apicD B_a . (x_i - x_p) = Tm_a + Sm_a * pdx
+        const R pdy = stage_pd<D, R>(S, crd, 1, lby, iy);
+        const R pdz = D == 3 ? stage_pd<D, R>(S, crd, D - 1, lbz, iz) : R(0.0);
+        R Tm[D], Sm[D];
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+          if (apic) {
+            R byz = S.B[a * D + 1] * pdy;
+            if constexpr (D == 3) byz += S.B[a * D + 2] * pdz;
+            Tm[a] = S.v[a] + apicD * byz;
+            Sm[a] = apicD * S.B[a * D];
+          } else {
+            Tm[a] = S.v[a];
+            Sm[a] = R(0.0);
+          }
+        }
+        const R mui = S.mui;
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          const R wx = S.w[h], dwx = S.dw[h];
+          const R weight = wx * wyz;
+          if (weight > R(1e-25)) {
+            const R pdx = stage_pd<D, R>(S, crd, 0, lbx, h);
+            acc[h][0] += weight;
+#pragma unroll
+            for (int a = 0; a < D; ++a) acc[h][1 + a] += weight * (Tm[a] + Sm[a] * pdx);
+            if (mibf) acc[h][1 + 2 * D] += mui * weight;
+          }
+#pragma unroll
+          for (int a = 0; a < D; ++a) acc[h][1 + D + a] += dwx * Pf[a] + wx * Qf[a];
+        }
+      }
+      if (cur >= 0) flush();
+    }
+    __syncthreads();
+  }
+  const uint32_t cap = A.cap_nodes;
+  for (int n = threadIdx.x; n < NODES; n += blockDim.x) {
+    uint32_t l;
+    if (!patch_node<D>(H, n0, n, l)) continue;
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) {
+      const R val = patch[ch][n];
+      if (val != R(0.0)) atomicAdd(&A.acc[(size_t)ch * cap + l], val);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 6. grid update, one thread per node (arithmetic in FP64 on both paths)
+// ---------------------------------------------------------------------------
+template <int D, typename R>
+__global__ void __launch_bounds__(256) k_grid(StepArgsT<R> A) {
+  StepHeader* H = A.H;
+  if (step_inactive(H)) return;
+  const DevParams& P = *A.P;
+  const uint32_t G = H->G, cap = A.cap_nodes;
+  const double dt = H->dt;
+  const double dtpv = dt * P.particle_volume;
+  double dtg[3];
+#pragma unroll
+  for (int a = 0; a < D; ++a) dtg[a] = dt * H->gravity[a];
+  __shared__ mtr_plate plates[MTR_MAXP];
+  for (int i = threadIdx.x; i < P.nplates; i += blockDim.x) plates[i] = H->plates[i];
+  __syncthreads();
+  constexpr int NCH = Tiling<D>::NCH;
+  double sum_m = 0.0, sum_p[3] = {0.0, 0.0, 0.0};  // mass and momentum balance (simulation.cpp:292-333)
+  for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < G; l += gridDim.x * blockDim.x) {
+    const double mraw = A.acc[l];
+    double v[3] = {0, 0, 0}, vold[3] = {0, 0, 0};
+    double fric = 0.0;
+    sum_m += mraw;
+    if (mraw > 0) {
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        const double pa = A.acc[(size_t)(1 + a) * cap + l];
+        sum_p[a] += pa;
+        v[a] = pa / mraw;
+      }
+    }
+    if (P.use_mibf) fric = P.mui0 + (double)A.acc[(size_t)(1 + 2 * D) * cap + l] / mraw;
+    const double mi = mraw * P.particle_mass;
+    double fl[3] = {0, 0, 0};
+    if (mi > 0) {
+      uint32_t k = D == 3 ? l % H->N[2] : 0;
+      uint32_t r = D == 3 ? l / H->N[2] : l;
+      uint32_t jj = r % H->N[1], i = r / H->N[1];
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        double inc = -dtpv * (double)A.acc[(size_t)(1 + D + a) * cap + l] / mi + dtg[a];
+        vold[a] = v[a];
+        v[a] = vold[a] + inc;
+      }
+      double Xi[3] = {A.gx[i], A.gy[jj], D == 3 ? A.gz[k] : 0.0};
+      if (!boundary_collision<D>(P, plates, fric, Xi, dt, v)) raise_status(H, MTR_STATUS_BAD_BC, 0xffffffffu);
+#pragma unroll
+      for (int a = 0; a < D; ++a) fl[a] = v[a] - vold[a];
+    }
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      A.nv[(size_t)a * cap + l] = (R)v[a];
+      A.nflip[(size_t)a * cap + l] = (R)fl[a];
+    }
+    A.nmass[l] = (R)mi;
+    if (P.use_mibf) A.nfric[l] = (R)fric;
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) A.acc[(size_t)ch * cap + l] = R(0.0);  // ready for the next step
+  }
+  block_add(sum_m * P.particle_mass, &H->grid_mass);
+#pragma unroll
+  for (int a = 0; a < D; ++a) block_add(sum_p[a] * P.particle_mass, &H->grid_mom[a]);
+}
+
+// ---------------------------------------------------------------------------
+// particle I/O helpers (the deformation update and return mapping are FP64)
+// ---------------------------------------------------------------------------
+template <int D>
+struct PLoad {
+  double x[3], v[3], F[D][D];
+  PScalars s;
+  uint32_t id;
+};
+
+template <int D, typename R>
+__device__ __forceinline__ void load_particle(const PBufT<R>& b, uint32_t Np, uint32_t j, PLoad<D>& p) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) p.x[a] = p.v[a] = 0.0;
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    p.x[a] = b.x[(size_t)a * Np + j];
+    p.v[a] = b.v[(size_t)a * Np + j];
+  }
+#pragma unroll
+  for (int r = 0; r < D; ++r)
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+      if constexpr (kFP64<R>)
+        p.F[r][c] = b.F[(size_t)(r * D + c) * Np + j];
+      else
+        p.F[r][c] = (double)b.F[(size_t)(r * D + c) * Np + j] + (r == c ? 1.0 : 0.0);
+    }
+  p.s.eps_pl_dev = b.sc[(size_t)MTR_SCALAR_EPS_PL_DEV * Np + j];
+  p.s.eps_pl_vol = b.sc[(size_t)MTR_SCALAR_EPS_PL_VOL * Np + j];
+  p.s.eps_pl_vol_pradhana = b.sc[(size_t)MTR_SCALAR_EPS_PL_VOL_PRADHANA * Np + j];
+  p.s.delta_gamma = 0.0;  // deformation_update.cpp:13 zeroes it every step
+  p.s.viscosity = b.sc[(size_t)MTR_SCALAR_VISCOSITY * Np + j];
+  p.s.muI = b.sc[(size_t)MTR_SCALAR_MUI * Np + j];
+  p.id = b.id[j];
+}
+
+template <int D, typename R>
+__device__ __forceinline__ void store_defgrad(const PBufT<R>& b, uint32_t Np, uint32_t s, const double (&F)[D][D],
+                                              const PScalars& sc, const double* tau) {
+#pragma unroll
+  for (int r = 0; r < D; ++r)
+#pragma unroll
+    for (int c = 0; c < D; ++c) {
+      if constexpr (kFP64<R>)
+        b.F[(size_t)(r * D + c) * Np + s] = F[r][c];
+      else
+        b.F[(size_t)(r * D + c) * Np + s] = (R)(F[r][c] - (r == c ? 1.0 : 0.0));
+    }
+  b.sc[(size_t)MTR_SCALAR_EPS_PL_DEV * Np + s] = (R)sc.eps_pl_dev;
+  b.sc[(size_t)MTR_SCALAR_EPS_PL_VOL * Np + s] = (R)sc.eps_pl_vol;
+  b.sc[(size_t)MTR_SCALAR_EPS_PL_VOL_PRADHANA * Np + s] = (R)sc.eps_pl_vol_pradhana;
+  b.sc[(size_t)MTR_SCALAR_DELTA_GAMMA * Np + s] = (R)sc.delta_gamma;
+  b.sc[(size_t)MTR_SCALAR_VISCOSITY * Np + s] = (R)sc.viscosity;
+  b.sc[(size_t)MTR_SCALAR_MUI * Np + s] = (R)sc.muI;
+#pragma unroll
+  for (int q = 0; q < Sym<D>::n; ++q) b.tau[(size_t)q * Np + s] = (R)tau[q];
+}
+
+// velocity blend of position_update.cpp:14-24 / musl.cpp:15-22
+__device__ __forceinline__ double blend_v(double fr, double v, double fl, double pic) {
+  if (fr < -1) return pic;
+  if (fr < 0) return (-fr) * (v + fl) + (1 - (-fr)) * pic;
+  return fr * (v + fl) + (1 - fr) * pic;
+}
+
+// F_trial = F + dt * gradv * F (deformation_update.cpp:42-44), then the
+// return mapping; writes F, scalars and tau into the out buffer at slot s.
+template <int D, typename R>
+__device__ __forceinline__ void defgrad_and_store(const StepArgsT<R>& A, uint32_t s, double dt, PLoad<D>& p,
+                                                  const R (&gv)[D][D], uint32_t& flags, bool& plastic) {
+  double T1[D][D], T2[D][D];
+#pragma unroll
+  for (int r = 0; r < D; ++r)
+#pragma unroll
+    for (int c = 0; c < D; ++c) T1[r][c] = dt * (double)gv[r][c];
+  mat_mul<D>(T1, p.F, T2);
+#pragma unroll
+  for (int r = 0; r < D; ++r)
+#pragma unroll
+    for (int c = 0; c < D; ++c) p.F[r][c] = p.F[r][c] + T2[r][c];
+  double tau[Sym<D>::n];
+  plastic = return_map<D>(*A.P, dt, p.F, p.s, tau, flags);
+  store_defgrad<D, R>(A.out, A.Np, s, p.F, p.s, tau);
+}
+
+// ---------------------------------------------------------------------------
+// Tile-structured gathers.  A tile block first copies the node values its
+// particles' stencils can reach (the PN^D patch of the tile) from the node
+// arrays into shared memory, then every particle gathers from there.
+// ---------------------------------------------------------------------------
+
+// copies NF fields of D components each, src[f] = [D][cap] node arrays
+template <int D, int NF, typename R>
+__device__ __forceinline__ void load_node_patch(const StepCommon& A, const StepHeader* H, const int (&n0)[3],
+                                                const R* const (&src)[NF], R* dst /*[NF*D][NODES]*/) {
+  constexpr int NODES = Tiling<D>::NODES;
+  const uint32_t cap = A.cap_nodes;
+  for (int n = threadIdx.x; n < NODES; n += blockDim.x) {
+    uint32_t l = 0;
+    const bool in = patch_node<D>(H, n0, n, l);
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+      for (int a = 0; a < D; ++a) dst[(f * D + a) * NODES + n] = in ? src[f][(size_t)a * cap + l] : R(0.0);
+  }
+}
+
+// G2P gather (g2p.cpp:24-77) and velocity gradient (deformation_update.cpp:17-40)
+// from a shared node patch; lb = stencil base relative to the patch origin.
+// Sums are factorised over the tensor-product stencil.  The offsets and the
+// spline argument are formed in FP64 from the FP64 position, then rounded to R.
+template <int D, int DEG, bool GRADV, typename R>
+__device__ __forceinline__ void gather_patch(const R* pv, const R* pf, const double (*crd)[Tiling<D>::PN],
+                                             const int (&lb)[3], const double (&xp)[3], double ioh, R (&pic)[3],
+                                             R (&Bp)[D][D], R (&flp)[3], R (&gv)[D][D], bool want_b, bool want_flip) {
+  constexpr int PN = Tiling<D>::PN, NODES = Tiling<D>::NODES;
+  R w[3][4], dw[3][4], pd[3][4];
+#pragma unroll
+  for (int a = 0; a < D; ++a)
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+      const double c = crd[a][lb[a] + o];
+      const R u = (R)((xp[a] - c) * ioh);
+      w[a][o] = bspline_N<DEG>(u);
+      dw[a][o] = GRADV ? bspline_dN<DEG>(u) : R(0.0);
+      pd[a][o] = (R)(c - xp[a]);
+    }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) pic[a] = flp[a] = R(0.0);
+#pragma unroll
+  for (int r = 0; r < D; ++r)
+#pragma unroll
+    for (int c = 0; c < D; ++c) Bp[r][c] = gv[r][c] = R(0.0);
+  constexpr int KN = D == 3 ? 4 : 1;
+#pragma unroll
+  for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const R wxy = w[0][ii] * w[1][jj];
+      const R gx_ = dw[0][ii] * w[1][jj], gy_ = w[0][ii] * dw[1][jj];
+#pragma unroll
+      for (int kk = 0; kk < KN; ++kk) {
+        const int node = D == 3 ? ((lb[0] + ii) * PN + (lb[1] + jj)) * PN + (lb[2] + kk) : (lb[0] + ii) * PN + (lb[1] + jj);
+        const R weight = D == 3 ? wxy * w[2][kk] : wxy;
+        R vi[D];
+#pragma unroll
+        for (int a = 0; a < D; ++a) vi[a] = pv[a * NODES + node];
+#pragma unroll
+        for (int a = 0; a < D; ++a) pic[a] += vi[a] * weight;
+        if (want_b) {
+          R wpd[3] = {weight * pd[0][ii], weight * pd[1][jj], D == 3 ? weight * pd[2][kk] : R(0.0)};
+#pragma unroll
+          for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) Bp[r][c] += vi[r] * wpd[c];
+        }
+        if (want_flip) {
+#pragma unroll
+          for (int a = 0; a < D; ++a) flp[a] += pf[a * NODES + node] * weight;
+        }
+        if (GRADV) {
+          R g[3];
+          if constexpr (D == 3) {
+            g[0] = gx_ * w[2][kk];
+            g[1] = gy_ * w[2][kk];
+            g[2] = wxy * dw[2][kk];
+          } else {
+            g[0] = gx_;
+            g[1] = gy_;
+          }
+#pragma unroll
+          for (int r = 0; r < D; ++r)
+#pragma unroll
+            for (int c = 0; c < D; ++c) gv[r][c] += vi[r] * g[c];
+        }
+      }
+    }
+  if (GRADV) {
+    const R iohR = (R)ioh;
+#pragma unroll
+    for (int r = 0; r < D; ++r)
+#pragma unroll
+      for (int c = 0; c < D; ++c) gv[r][c] *= iohR;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 7a. USL: G2P + deformation update + return mapping + position update, one
+// block per tile, node patch in shared memory.
+// ---------------------------------------------------------------------------
+template <int D, int DEG, typename R>
+__global__ void __launch_bounds__(kChunk, MTR_RM_MIN_BLOCKS) k_g2p_t(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
+  using TL = Tiling<D>;
+  constexpr int PN = TL::PN, NODES = TL::NODES;
+  StepHeader* H = A.H;
+  if (step_inactive(H)) return;
+  const uint32_t t = blockIdx.x;
+  if (t >= H->ntiles) return;
+  const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
+  if (pb >= pe) return;
+  const DevParams& P = *A.P;
+  __shared__ R pv[2 * D * NODES];
+  __shared__ double crd[3][PN];
+  int n0[3];
+  load_tile_setup<D>(A, H, t, n0, crd);
+  const R* const src[2] = {A.nv, A.nflip};
+  load_node_patch<D, 2, R>(A, H, n0, src, pv);
+  __syncthreads();
+  const uint32_t Np = A.Np;
+  const double dt = H->dt, fr = P.flip_ratio, ioh = P.one_over_dx;
+  unsigned nplastic = 0;
+  for (uint32_t s = pb + threadIdx.x; s < pe; s += blockDim.x) {
+    const uint32_t j = perm[s];
+    PLoad<D> p;
+    load_particle<D, R>(A.in, Np, j, p);
+    R pic[3], flp[3], Bp[D][D], gv[D][D];
+    int lb[3];
+    if (local_base<D>(H, p.x, ioh, n0, false, lb)) {
+      gather_patch<D, DEG, true, R>(pv, pv + D * NODES, crd, lb, p.x, ioh, pic, Bp, flp, gv, fr < 0, fr >= -1);
+    } else {
+      raise_status(H, MTR_STATUS_STENCIL_OOB, p.id);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) pic[a] = flp[a] = R(0.0);
+#pragma unroll
+      for (int r = 0; r < D; ++r)
+#pragma unroll
+        for (int c = 0; c < D; ++c) Bp[r][c] = gv[r][c] = R(0.0);
+    }
+    uint32_t f = 0;
+    bool plastic = false;
+    defgrad_and_store<D, R>(A, s, dt, p, gv, f, plastic);
+    if (f) raise_status(H, f, p.id);
+    nplastic += plastic ? 1u : 0u;
+    double xn[3], vn[3];
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      xn[a] = p.x[a] + dt * (double)pic[a];
+      vn[a] = blend_v(fr, p.v[a], (double)flp[a], (double)pic[a]);
+    }
+    if (P.change_particle_positions && xn[0] > 0.8) {  // position_update.cpp:35-41
+      xn[0] = -0.1;
+      xn[1] += 0.27;
+    }
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      A.out.x[(size_t)a * Np + s] = xn[a];
+      A.out.v[(size_t)a * Np + s] = (R)vn[a];
+    }
+#pragma unroll
+    for (int r = 0; r < D; ++r)
+#pragma unroll
+      for (int c = 0; c < D; ++c) A.out.B[(size_t)(r * D + c) * Np + s] = (fr < 0) ? Bp[r][c] : R(0.0);
+    A.out.id[s] = p.id;
+    if (P.store_pic_flip) {
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        A.pic[(size_t)a * Np + s] = pic[a];
+        A.flip[(size_t)a * Np + s] = (fr >= -1) ? flp[a] : R(0.0);
+      }
+    }
+  }
+  block_count(nplastic, &H->plastic_count);
+}
+
+// ---------------------------------------------------------------------------
+// 7b. MUSL (musl.cpp:6-96), one block per tile.  Phase 1 (thread per
+// particle): gather pic/B/flip from the shared node patch, blend v, write
+// x + dt pic, v, B; stage v_new, B_new and the re-scatter weights.  Phase 2
+// (lane groups owning stencil columns, as in P2G): accumulate
+// v_p + B D^-1 (x_i - x_p) per cell in registers, add once per cell to the
+// shared re-projection patch, flush with one global atomic per node.
+// ---------------------------------------------------------------------------
+template <int D, typename R = double>
+struct MStage {
+  double x[D], v[D], B[D * D], w[D * 4];
+  int lb;
+  int pad;
+};
+
+template <int D>
+struct MStage<D, float> {
+  float pd[D * 4], v[D], B[D * D], w[D * 4];
+  int lb;
+};
+
+template <int D, typename R>
+__device__ __forceinline__ R stage_pd(const MStage<D, R>& S, const double (*crd)[Tiling<D>::PN], int a, int lba,
+                                      int o) {
+  if constexpr (kFP64<R>)
+    return crd[a][lba + o] - S.x[a];
+  else
+    return S.pd[a * 4 + o];
+}
+
+template <int D, typename R>
+constexpr size_t musl_crd_bytes() {
+  return align16(sizeof(double) * 3 * Tiling<D>::PN);
+}
+template <int D, typename R>
+constexpr size_t musl_patch_bytes() {
+  return align16(sizeof(R) * 3 * D * Tiling<D>::NODES);
+}
+template <int D, typename R>
+constexpr size_t musl_smem_bytes() {
+  return musl_crd_bytes<D, R>() + musl_patch_bytes<D, R>() + sizeof(MStage<D, R>) * kChunk;
+}
+
+template <int D, int DEG, typename R>
+__global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
+  using TL = Tiling<D>;
+  constexpr int PN = TL::PN, NODES = TL::NODES;
+  StepHeader* H = A.H;
+  if (step_inactive(H)) return;
+  const uint32_t t = blockIdx.x;
+  if (t >= H->ntiles) return;
+  const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
+  if (pb >= pe) return;
+  const DevParams& P = *A.P;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double(*crd)[PN] = reinterpret_cast<double(*)[PN]>(smem_raw);
+  R* pv = reinterpret_cast<R*>(smem_raw + musl_crd_bytes<D, R>());  // [2D][NODES] node v, flip
+  R(*vsum)[NODES] = reinterpret_cast<R(*)[NODES]>(pv + 2 * D * NODES);  // [D][NODES]
+  MStage<D, R>* st = reinterpret_cast<MStage<D, R>*>(smem_raw + musl_crd_bytes<D, R>() + musl_patch_bytes<D, R>());
+  int n0[3];
+  load_tile_setup<D>(A, H, t, n0, crd);
+  const R* const src[2] = {A.nv, A.nflip};
+  load_node_patch<D, 2, R>(A, H, n0, src, pv);
+  for (int i = threadIdx.x; i < D * NODES; i += blockDim.x) (&vsum[0][0])[i] = R(0.0);
+  __syncthreads();
+  const uint32_t Np = A.Np;
+  const double dt = H->dt, fr = P.flip_ratio, ioh = P.one_over_dx;
+  const R apicD = (R)P.apicDinverse;
+  const bool apic = fr < 0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int LPP = D == 3 ? 16 : 4;
+  const int q = lane % LPP;
+  const int iy = D == 3 ? (q >> 2) : q;
+  const int iz = D == 3 ? (q & 3) : 0;
+  // consecutive particles per lane group, as in k_p2g_w
+  const int kbeg = warp * 32 + (lane / LPP) * LPP, kend = kbeg + LPP;
+  for (uint32_t c0 = pb; c0 < pe; c0 += kChunk) {
     {  // phase 1
       const uint32_t s = c0 + threadIdx.x;
-      MStage<D>& S = st[threadIdx.x];
+      MStage<D, R>& S = st[threadIdx.x];
       int packed = -1;
       if (s < pe) {
         const uint32_t j = perm[s];
@@ -1555,33 +1246,33 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgs A, const uint32_
           vp[a] = A.in.v[(size_t)a * Np + j];
         }
         const uint32_t pid = A.in.id[j];
-        double pic[3], flp[3], Bp[D][D], gv[D][D];
+        R pic[3], flp[3], Bp[D][D], gv[D][D];
         int lb[3];
         const bool ok = local_base<D>(H, xp, ioh, n0, false, lb);
         if (ok) {
-          gather_patch<D, DEG, false>(pv, pv + D * NODES, crd, lb, xp, ioh, pic, Bp, flp, gv, apic, fr >= -1);
+          gather_patch<D, DEG, false, R>(pv, pv + D * NODES, crd, lb, xp, ioh, pic, Bp, flp, gv, apic, fr >= -1);
         } else {
           raise_status(H, MTR_STATUS_STENCIL_OOB, pid);
 #pragma unroll
-          for (int a = 0; a < 3; ++a) pic[a] = flp[a] = 0.0;
+          for (int a = 0; a < 3; ++a) pic[a] = flp[a] = R(0.0);
 #pragma unroll
           for (int r = 0; r < D; ++r)
 #pragma unroll
-            for (int c = 0; c < D; ++c) Bp[r][c] = 0.0;
+            for (int c = 0; c < D; ++c) Bp[r][c] = R(0.0);
         }
 #pragma unroll
         for (int a = 0; a < D; ++a) {
-          const double vn = blend_v(fr, vp[a], flp[a], pic[a]);
-          S.x[a] = xp[a];
-          S.v[a] = vn;
-          A.out.x[(size_t)a * Np + s] = xp[a] + dt * pic[a];  // positionUpdate: x + dt pic
-          A.out.v[(size_t)a * Np + s] = vn;
+          const double vn = blend_v(fr, vp[a], (double)flp[a], (double)pic[a]);
+          if constexpr (kFP64<R>) S.x[a] = xp[a];
+          S.v[a] = (R)vn;
+          A.out.x[(size_t)a * Np + s] = xp[a] + dt * (double)pic[a];  // positionUpdate: x + dt pic
+          A.out.v[(size_t)a * Np + s] = (R)vn;
         }
 #pragma unroll
         for (int r = 0; r < D; ++r)
 #pragma unroll
           for (int c = 0; c < D; ++c) {
-            const double b = apic ? Bp[r][c] : 0.0;
+            const R b = apic ? Bp[r][c] : R(0.0);
             A.out.B[(size_t)(r * D + c) * Np + s] = b;
             S.B[r * D + c] = b;
           }
@@ -1590,7 +1281,7 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgs A, const uint32_
 #pragma unroll
           for (int a = 0; a < D; ++a) {
             A.pic[(size_t)a * Np + s] = pic[a];
-            A.flip[(size_t)a * Np + s] = (fr >= -1) ? flp[a] : 0.0;
+            A.flip[(size_t)a * Np + s] = (fr >= -1) ? flp[a] : R(0.0);
           }
         }
         // re-scatter stencil, base clamped at zero like P2G (musl.cpp:35-40)
@@ -1599,7 +1290,11 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgs A, const uint32_
 #pragma unroll
           for (int a = 0; a < D; ++a)
 #pragma unroll
-            for (int o = 0; o < 4; ++o) S.w[a * 4 + o] = bspline_N<DEG>((xp[a] - crd[a][lbs[a] + o]) * ioh);
+            for (int o = 0; o < 4; ++o) {
+              const double c = crd[a][lbs[a] + o];
+              S.w[a * 4 + o] = bspline_N<DEG>((R)((xp[a] - c) * ioh));
+              if constexpr (!kFP64<R>) S.pd[a * 4 + o] = (R)(c - xp[a]);
+            }
           packed = lbs[0] | (lbs[1] << 4) | (lbs[2] << 8);
         } else if (ok) {
           raise_status(H, MTR_STATUS_STENCIL_OOB, pid);
@@ -1609,11 +1304,11 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgs A, const uint32_
     }
     __syncthreads();
     {  // phase 2
-      double acc[4][D];
+      R acc[4][D];
 #pragma unroll
       for (int h = 0; h < 4; ++h)
 #pragma unroll
-        for (int a = 0; a < D; ++a) acc[h][a] = 0.0;
+        for (int a = 0; a < D; ++a) acc[h][a] = R(0.0);
       int cur = -1;
       auto flush = [&]() {
         const int lbx = cur & 15, lby = (cur >> 4) & 15, lbz = cur >> 8;
@@ -1622,13 +1317,13 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgs A, const uint32_
           const int node = D == 3 ? ((lbx + h) * PN + (lby + iy)) * PN + (lbz + iz) : (lbx + h) * PN + (lby + iy);
 #pragma unroll
           for (int a = 0; a < D; ++a) {
-            if (acc[h][a] != 0.0) atomicAdd(&vsum[a][node], acc[h][a]);
-            acc[h][a] = 0.0;
+            if (acc[h][a] != R(0.0)) atomicAdd(&vsum[a][node], acc[h][a]);
+            acc[h][a] = R(0.0);
           }
         }
       };
       for (int k = kbeg; k < kend; ++k) {
-        const MStage<D>& S = st[k];
+        const MStage<D, R>& S = st[k];
         const int lbp = S.lb;
         if (lbp < 0) continue;
         if (lbp != cur) {
@@ -1636,28 +1331,27 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgs A, const uint32_
           cur = lbp;
         }
         const int lbx = lbp & 15, lby = (lbp >> 4) & 15, lbz = lbp >> 8;
-        const double wyz = D == 3 ? S.w[4 + iy] * S.w[8 + iz] : S.w[4 + iy];
-        const double pdy = crd[1][lby + iy] - S.x[1];
-        const double pdz = D == 3 ? crd[2][lbz + iz] - S.x[D - 1] : 0.0;
-        double Tm[D], Sm[D];
+        const R wyz = D == 3 ? S.w[4 + iy] * S.w[8 + iz] : S.w[4 + iy];
+        const R pdy = stage_pd<D, R>(S, crd, 1, lby, iy);
+        const R pdz = D == 3 ? stage_pd<D, R>(S, crd, D - 1, lbz, iz) : R(0.0);
+        R Tm[D], Sm[D];
 #pragma unroll
         for (int a = 0; a < D; ++a) {
           if (apic) {
-            double byz = S.B[a * D + 1] * pdy;
+            R byz = S.B[a * D + 1] * pdy;
             if constexpr (D == 3) byz += S.B[a * D + 2] * pdz;
             Tm[a] = S.v[a] + apicD * byz;
             Sm[a] = apicD * S.B[a * D];
           } else {
             Tm[a] = S.v[a];
-            Sm[a] = 0.0;
+            Sm[a] = R(0.0);
           }
         }
-        const double xp0 = S.x[0];
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
-          const double weight = S.w[h] * wyz;
-          if (!(weight > 1e-25)) continue;
-          const double pdx = crd[0][lbx + h] - xp0;
+          const R weight = S.w[h] * wyz;
+          if (!(weight > R(1e-25))) continue;
+          const R pdx = stage_pd<D, R>(S, crd, 0, lbx, h);
 #pragma unroll
           for (int a = 0; a < D; ++a) acc[h][a] += weight * (Tm[a] + Sm[a] * pdx);
         }
@@ -1668,30 +1362,19 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgs A, const uint32_
   }
   const uint32_t cap = A.cap_nodes;
   for (int n = threadIdx.x; n < NODES; n += blockDim.x) {
-    int li, lj, lk;
-    if constexpr (D == 3) {
-      lk = n % PN;
-      lj = (n / PN) % PN;
-      li = n / (PN * PN);
-    } else {
-      lk = 0;
-      lj = n % PN;
-      li = n / PN;
-    }
-    const int gi = n0[0] + li, gj = n0[1] + lj, gk = n0[2] + lk;
-    if (gi < 0 || gj < 0 || gk < 0 || gi >= (int)H->N[0] || gj >= (int)H->N[1] || gk >= (int)H->N[2]) continue;
-    const uint32_t l = node_index(H, gi, gj, gk);
+    uint32_t l;
+    if (!patch_node<D>(H, n0, n, l)) continue;
 #pragma unroll
     for (int a = 0; a < D; ++a) {
-      const double val = vsum[a][n];
-      if (val != 0.0) atomicAdd(&A.v2[(size_t)a * cap + l], val);
+      const R val = vsum[a][n];
+      if (val != R(0.0)) atomicAdd(&A.v2[(size_t)a * cap + l], val);
     }
   }
 }
 
 // musl.cpp:80-95: v2 /= (m_i / m_p) (zero where m_i == 0)
-template <int D>
-__global__ void __launch_bounds__(256) k_musl_norm(StepArgs A) {
+template <int D, typename R>
+__global__ void __launch_bounds__(256) k_musl_norm(StepArgsT<R> A) {
   StepHeader* H = A.H;
   if (step_inactive(H)) return;
   const uint32_t G = H->G, cap = A.cap_nodes;
@@ -1700,44 +1383,63 @@ __global__ void __launch_bounds__(256) k_musl_norm(StepArgs A) {
     const double mi = A.nmass[l];
 #pragma unroll
     for (int a = 0; a < D; ++a) {
-      double* p = &A.v2[(size_t)a * cap + l];
-      *p = (mi > 0) ? *p / (mi / mp) : 0.0;
+      R* p = &A.v2[(size_t)a * cap + l];
+      *p = (mi > 0) ? (R)((double)*p / (mi / mp)) : R(0.0);
     }
   }
 }
 
-// MUSL: deformation update from the re-projected velocities and the OLD
-// positions (deformation_update.cpp:6), then the return mapping.
-template <int D, int DEG>
-__global__ void __launch_bounds__(128) k_defgrad(StepArgs A, const uint32_t* __restrict__ perm) {
+// MUSL: deformation update from the normalised re-projected velocity v2 and
+// the old positions (deformation_update.cpp:6), then the return mapping.
+template <int D, int DEG, typename R>
+__global__ void __launch_bounds__(kChunk, MTR_RM_MIN_BLOCKS) k_defgrad_t(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
+  using TL = Tiling<D>;
+  constexpr int PN = TL::PN, NODES = TL::NODES;
   StepHeader* H = A.H;
   if (step_inactive(H)) return;
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= A.Np) return;
-  const uint32_t Np = A.Np, j = perm[s];
-  const double dt = H->dt;
-  PLoad<D> p;
-  load_particle<D>(A.in, Np, j, p);
-  double pic[3], flp[3], Bp[D][D], gv[D][D];
-  if (!gather<D, DEG, true>(A, H, A.v2, p.x, pic, Bp, flp, gv, false, false)) {
-    raise_status(H, MTR_STATUS_STENCIL_OOB, p.id);
+  const uint32_t t = blockIdx.x;
+  if (t >= H->ntiles) return;
+  const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
+  if (pb >= pe) return;
+  __shared__ R pv[D * NODES];
+  __shared__ double crd[3][PN];
+  int n0[3];
+  load_tile_setup<D>(A, H, t, n0, crd);
+  const R* const src[1] = {A.v2};
+  load_node_patch<D, 1, R>(A, H, n0, src, pv);
+  __syncthreads();
+  const uint32_t Np = A.Np;
+  const double dt = H->dt, ioh = A.P->one_over_dx;
+  unsigned nplastic = 0;
+  for (uint32_t s = pb + threadIdx.x; s < pe; s += blockDim.x) {
+    const uint32_t j = perm[s];
+    PLoad<D> p;
+    load_particle<D, R>(A.in, Np, j, p);
+    R pic[3], flp[3], Bp[D][D], gv[D][D];
+    int lb[3];
+    if (local_base<D>(H, p.x, ioh, n0, false, lb)) {
+      gather_patch<D, DEG, true, R>(pv, nullptr, crd, lb, p.x, ioh, pic, Bp, flp, gv, false, false);
+    } else {
+      raise_status(H, MTR_STATUS_STENCIL_OOB, p.id);
 #pragma unroll
-    for (int r = 0; r < D; ++r)
+      for (int r = 0; r < D; ++r)
 #pragma unroll
-      for (int c = 0; c < D; ++c) gv[r][c] = 0.0;
+        for (int c = 0; c < D; ++c) gv[r][c] = R(0.0);
+    }
+    uint32_t f = 0;
+    bool plastic = false;
+    defgrad_and_store<D, R>(A, s, dt, p, gv, f, plastic);
+    if (f) raise_status(H, f, p.id);
+    nplastic += plastic ? 1u : 0u;
   }
-  uint32_t flags = 0;
-  bool plastic = false;
-  defgrad_and_store<D>(A, s, dt, p, gv, flags, plastic);
-  if (flags) raise_status(H, flags, p.id);
-  count_plastic(H, plastic);
+  block_count(nplastic, &H->plastic_count);
 }
 
 // ---------------------------------------------------------------------------
 // 8. end of step: moveObjects and the clock of simulate()
 // ---------------------------------------------------------------------------
 template <int D>
-__global__ void k_tail(StepArgs A, int out_parity) {
+__global__ void k_tail(StepCommon A, int out_parity) {
   StepHeader* H = A.H;
   if (step_inactive(H)) return;
   const DevParams& P = *A.P;
@@ -1774,44 +1476,45 @@ __global__ void k_tail(StepArgs A, int out_parity) {
 // ---------------------------------------------------------------------------
 // set-up and download
 // ---------------------------------------------------------------------------
-template <int D>
-__global__ void k_init_state(StepArgs A, PBuf b) {  // tau of the uploaded F, id = index
+template <int D, typename R>
+__global__ void k_init_state(StepCommon A, PBufT<R> b) {  // tau of the uploaded F, id = index
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.Np) return;
-  double F[D][D];
-#pragma unroll
-  for (int r = 0; r < D; ++r)
-#pragma unroll
-    for (int c = 0; c < D; ++c) F[r][c] = b.F[(size_t)(r * D + c) * A.Np + i];
+  PLoad<D> p;
+  load_particle<D, R>(b, A.Np, i, p);
   double tau[Sym<D>::n];
-  initial_tau<D>(*A.P, F, tau);
+  initial_tau<D>(*A.P, p.F, tau);
 #pragma unroll
-  for (int q = 0; q < Sym<D>::n; ++q) b.tau[(size_t)q * A.Np + i] = tau[q];
+  for (int q = 0; q < Sym<D>::n; ++q) b.tau[(size_t)q * A.Np + i] = (R)tau[q];
   b.id[i] = i;
 }
 
-// AoS (host layout, column-major matrices) <-> SoA, in original particle order
-template <int D>
-__global__ void k_aos_to_soa(uint32_t Np, const double* __restrict__ src, double* dst, int kind) {
-  // kind 0: vector (D), 1: matrix (D*D, column-major src -> (r*D+c) dst), 2: scalars (6)
+// AoS (host layout, column-major matrices) <-> SoA, in original particle order.
+// kind 0: vector (D), 1: matrix (D*D, column-major AoS <-> (r*D+c) SoA),
+// 2: scalars (6), 3: matrix stored as M - I (the FP32 deformation gradient).
+template <int D, typename R>
+__global__ void k_aos_to_soa(uint32_t Np, const double* __restrict__ src, R* dst, int kind) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= Np) return;
   if (kind == 0) {
 #pragma unroll
-    for (int a = 0; a < D; ++a) dst[(size_t)a * Np + i] = src[(size_t)i * D + a];
-  } else if (kind == 1) {
+    for (int a = 0; a < D; ++a) dst[(size_t)a * Np + i] = (R)src[(size_t)i * D + a];
+  } else if (kind == 1 || kind == 3) {
 #pragma unroll
     for (int r = 0; r < D; ++r)
 #pragma unroll
-      for (int c = 0; c < D; ++c) dst[(size_t)(r * D + c) * Np + i] = src[(size_t)i * D * D + c * D + r];
+      for (int c = 0; c < D; ++c) {
+        const double m = src[(size_t)i * D * D + c * D + r];
+        dst[(size_t)(r * D + c) * Np + i] = (R)(kind == 3 ? m - (r == c ? 1.0 : 0.0) : m);
+      }
   } else {
 #pragma unroll
-    for (int q = 0; q < MTR_NUM_SCALARS; ++q) dst[(size_t)q * Np + i] = src[(size_t)i * MTR_NUM_SCALARS + q];
+    for (int q = 0; q < MTR_NUM_SCALARS; ++q) dst[(size_t)q * Np + i] = (R)src[(size_t)i * MTR_NUM_SCALARS + q];
   }
 }
 
-template <int D>
-__global__ void k_soa_to_aos(uint32_t Np, const double* __restrict__ src, const uint32_t* __restrict__ id, double* dst,
+template <int D, typename R>
+__global__ void k_soa_to_aos(uint32_t Np, const R* __restrict__ src, const uint32_t* __restrict__ id, double* dst,
                              int kind) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= Np) return;
@@ -1819,15 +1522,25 @@ __global__ void k_soa_to_aos(uint32_t Np, const double* __restrict__ src, const 
   if (kind == 0) {
 #pragma unroll
     for (int a = 0; a < D; ++a) dst[(size_t)i * D + a] = src[(size_t)a * Np + s];
-  } else if (kind == 1) {
+  } else if (kind == 1 || kind == 3) {
 #pragma unroll
     for (int r = 0; r < D; ++r)
 #pragma unroll
-      for (int c = 0; c < D; ++c) dst[(size_t)i * D * D + c * D + r] = src[(size_t)(r * D + c) * Np + s];
+      for (int c = 0; c < D; ++c) {
+        const double m = src[(size_t)(r * D + c) * Np + s];
+        dst[(size_t)i * D * D + c * D + r] = kind == 3 ? m + (r == c ? 1.0 : 0.0) : m;
+      }
   } else {
 #pragma unroll
     for (int q = 0; q < MTR_NUM_SCALARS; ++q) dst[(size_t)i * MTR_NUM_SCALARS + q] = src[(size_t)q * Np + s];
   }
+}
+
+// node array of type R -> FP64 (grid read-back of the FP32 path)
+template <typename R>
+__global__ void k_to_f64(uint64_t n, const R* __restrict__ src, double* dst) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    dst[i] = src[i];
 }
 
 }  // namespace mtr

@@ -237,6 +237,8 @@ __global__ void k_noalloc_setup(StepHeader* H, DevParams* P, const double* gx, c
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   H->done = 0;
   H->abort = 0;
+  H->frame = 0;
+  H->stop_frame = 0xffffffffu;
   H->status = 0;
   H->first_bad = 0xffffffffu;
   H->org[0] = gx[0];
@@ -335,6 +337,7 @@ int run_noalloc(unsigned char* base, const mtr_params& p, const double* x, const
   A.tile_begin = reinterpret_cast<uint32_t*>(base + kOffTileB);
   A.tile_end = reinterpret_cast<uint32_t*>(base + kOffTileE);
   A.in.x = const_cast<double*>(x);
+  A.xin = x;
   A.in.v = const_cast<double*>(v);
   A.in.B = const_cast<double*>(B);
   k_noalloc_setup<<<1, 32, 0, st>>>(H, P, gx, gy, gz, nx, ny, nz, tx, ty, tz, 1.0 / p.dx, apicD, p.flip_ratio,

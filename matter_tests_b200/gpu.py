@@ -21,7 +21,8 @@ EXPORTS = (
     "mtr_ctx_create", "mtr_upload", "mtr_set_objects", "mtr_step", "mtr_run", "mtr_run_frame", "mtr_download",
     "mtr_download_pic_flip", "mtr_get_grid", "mtr_get_sort", "mtr_get_plates", "mtr_get_clock",
     "mtr_status", "mtr_clear_status", "mtr_sync", "mtr_stream", "mtr_launch_count", "mtr_keep_pic_flip",
-    "mtr_use_graphs", "mtr_profile", "mtr_active_nodes", "mtr_ctx_destroy", "mtr_last_error", "mtr_p2g_noalloc",
+    "mtr_use_graphs", "mtr_profile", "mtr_active_nodes", "mtr_balance", "mtr_ctx_destroy", "mtr_last_error",
+    "mtr_p2g_noalloc",
 )
 
 _lib = None
@@ -64,6 +65,7 @@ def load_library(path=LIB_PATH):
     lib.mtr_use_graphs.argtypes = [C.c_void_p, C.c_int]
     lib.mtr_profile.argtypes = [C.c_void_p, C.c_int, _P, C.POINTER(C.c_char_p), C.c_int, C.POINTER(C.c_int)]
     lib.mtr_active_nodes.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    lib.mtr_balance.argtypes = [C.c_void_p, _P, _P, _P, _P]
     lib.mtr_p2g_noalloc.argtypes = [C.POINTER(MtrParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                     C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32), C.c_void_p,
                                     C.c_void_p, C.c_void_p]
@@ -160,6 +162,13 @@ class GpuSim:
         a, t = C.c_uint64(), C.c_uint64()
         _check(self.lib, "mtr_active_nodes", self.lib.mtr_active_nodes(self.h, C.byref(a), C.byref(t)))
         return a.value, t.value
+
+    def balance(self):
+        """FP64 mass and momentum balance of the last step (mtr_balance)."""
+        gm, pm = C.c_double(), C.c_double()
+        gp, pp = np.zeros(self.dim), np.zeros(self.dim)
+        _check(self.lib, "mtr_balance", self.lib.mtr_balance(self.h, C.byref(gm), _ptr(gp), C.byref(pm), _ptr(pp)))
+        return {"grid_mass": gm.value, "grid_momentum": gp, "particle_mass": pm.value, "particle_momentum": pp}
 
     # -- read-back ------------------------------------------------------
     def particles(self, pic_flip=False):

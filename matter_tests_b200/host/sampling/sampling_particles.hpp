@@ -8,7 +8,7 @@
 // this is this project's own implementation of Bridson's algorithm ("Fast
 // Poisson disk sampling in arbitrary dimensions", SIGGRAPH 2007 sketch):
 // background grid of cell r/sqrt(d), active list, `attempts` candidates per
-// active point in the annulus [r, 2r).  Samples differ from the reference's
+// active point drawn uniformly from the annulus r <= |d| < 2r around it.  Samples differ from the reference's
 // point for point, with the same density and minimum spacing.
 #ifndef SAMPLING_PARTICLES_HPP
 #define SAMPLING_PARTICLES_HPP
@@ -82,20 +82,20 @@ std::vector<std::array<T, D>> poisson_disk(T r, const std::array<T, D>& lo, cons
     const std::array<T, D> base = pts[active[ai]];
     bool found = false;
     for (uint32_t t = 0; t < attempts && !found; ++t) {
+      // uniform in the annulus r <= |d| < 2r: rejection from the cube [-2r, 2r]^D
       std::array<T, D> dir;
       T nn = 0;
-      do {  // uniform direction by rejection from the cube
+      do {
         nn = 0;
         for (int a = 0; a < D; ++a) {
-          dir[a] = 2 * uni(rng) - 1;
+          dir[a] = (4 * uni(rng) - 2) * r;
           nn += dir[a] * dir[a];
         }
-      } while (nn > 1 || nn < 1e-12);
-      const T rad = r * (1 + uni(rng));
+      } while (nn < r * r || nn >= 4 * r * r);
       std::array<T, D> cand;
       bool in = true;
       for (int a = 0; a < D; ++a) {
-        cand[a] = base[a] + rad * dir[a] / std::sqrt(nn);
+        cand[a] = base[a] + dir[a];
         if (cand[a] < lo[a] || cand[a] > hi[a]) in = false;
       }
       if (in && far_enough(cand)) {

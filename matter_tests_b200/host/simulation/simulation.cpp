@@ -435,21 +435,34 @@ void Simulation::moveObjects() { phase_unavailable("moveObjects"); }
 void Simulation::boundaryCollision(int, TV, TV&) { phase_unavailable("boundaryCollision"); }
 void Simulation::overwriteGridVelocity(TV, TV&) { phase_unavailable("overwriteGridVelocity"); }
 void Simulation::addExternalParticleGravity() {}
-void Simulation::checkMomentumConservation() { phase_unavailable("checkMomentumConservation"); }
 
-void Simulation::checkMassConservation() {  // simulation.cpp:319-333, on the last step's grid
+// simulation.cpp:292-333, from the FP64 balance the device keeps for the last step
+void Simulation::checkMassConservation() {
   if (!ctx_) return;
-  uint32_t dims[3];
-  if (mtr_get_grid(ctx_, dims, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr) != MTR_OK) return;
-  std::vector<double> m((size_t)dims[0] * dims[1] * dims[2]);
-  mtr_get_grid(ctx_, dims, nullptr, nullptr, nullptr, m.data(), nullptr, nullptr);
-  T grid_mass_total = 0;
-  for (double v : m) grid_mass_total += v;
-  const T particle_mass_total = particle_mass * Np;
-  debug("               Total grid mass = ", grid_mass_total);
-  debug("               Total part mass = ", particle_mass_total);
-  if (std::abs(grid_mass_total - particle_mass_total) > 1e-10 * particle_mass_total) {
+  double gm = 0, pm = 0;
+  if (mtr_balance(ctx_, &gm, nullptr, &pm, nullptr) != MTR_OK) return;
+  debug("               Total grid mass = ", gm);
+  debug("               Total part mass = ", pm);
+  if (std::abs(gm - pm) > 1e-10 * pm) {
     debug("MASS NOT CONSERVED!!!");
+    exit = 1;
+  }
+}
+
+void Simulation::checkMomentumConservation() {
+  if (!ctx_) return;
+  double gp[3] = {0, 0, 0}, pp[3] = {0, 0, 0};
+  if (mtr_balance(ctx_, nullptr, gp, nullptr, pp) != MTR_OK) return;
+  T gn = 0, pn = 0, dn = 0;
+  for (int a = 0; a < DIMENSION; ++a) {
+    gn += gp[a] * gp[a];
+    pn += pp[a] * pp[a];
+    dn += (gp[a] - pp[a]) * (gp[a] - pp[a]);
+  }
+  debug("               Total part momentum = ", std::sqrt(pn));
+  debug("               Total grid momentum = ", std::sqrt(gn));
+  if (std::sqrt(dn) > 1e-10 * std::sqrt(pn)) {
+    debug("MOMENTUM NOT CONSERVED!!!");
     exit = 1;
   }
 }

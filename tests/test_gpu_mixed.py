@@ -1,0 +1,161 @@
+"""The mixed-precision step (MTR_PREC_MIXED) and the FP64 balances.
+
+Mixed precision keeps the particle and grid state, the spline weights and the
+transfers in FP32 and the positions, the deformation update, the SVD, the
+return mapping and the balances in FP64, with F stored as F - I.  After one
+step every field is compared with the FP64 oracle; the tolerance of a field is
+a multiple of FP32 rounding (6e-8) of that field's scale, plus, for fields the
+reference computes through cancellation-prone closed forms, the oracle's own
+spread when its inputs move by FP32 rounding (its 4-ulp FP64 spread scaled by
+the ratio of the two roundings, 2^29 / 4).  Over many steps the mixed state is
+compared with the FP64 GPU state: positions in units of dx.
+"""
+import copy
+
+import numpy as np
+import pytest
+
+from matter_tests_b200.abi import BC, PREC_FP64, PREC_MIXED, SCALARS
+from matter_tests_b200 import scenes
+
+import cases
+from gpu_util import needs_gpu, oracle_sensitivity, run_gpu, run_oracle
+
+pytestmark = [pytest.mark.gpu, needs_gpu]
+
+FP32_TO_4ULP_FP64 = 2.0 ** 29 / 4.0
+
+# field -> relative tolerance against the field's scale after one step
+REL_MIXED = {"x": 1e-9, "v": 2e-6, "F": 1e-7, "B": 1e-4, "grid mass": 1e-6, "grid v": 2e-6}
+
+
+def with_precision(sc, prec):
+    out = copy.copy(sc)
+    out.params = copy.copy(sc.params)
+    out.params.precision = prec
+    return out
+
+
+def rel(a, b):
+    scale = np.abs(b).max()
+    return np.abs(a - b).max() / (scale if scale > 0 else 1.0)
+
+
+def check_one_step(sc, report):
+    g = run_gpu(with_precision(sc, PREC_MIXED), 1, keep_pic_flip=False)
+    o = run_oracle(sc, 1)
+    sens = oracle_sensitivity(sc, 1)
+    assert g["c"]["step"] == o["c"]["step"] == 1
+    bad = []
+    for k in ("x", "v", "F", "B"):
+        e = rel(g["p"][k], o["p"][k])
+        report.append((k, e))
+        if not e <= REL_MIXED[k] + FP32_TO_4ULP_FP64 * sens.get(k, 0.0) / max(np.abs(o["p"][k]).max(), 1e-300):
+            bad.append((k, e))
+    for i, k in enumerate(SCALARS):
+        a, b = g["p"]["scalars"][:, i], o["p"]["scalars"][:, i]
+        scale = np.abs(b).max()
+        diff = np.abs(a - b).max()
+        tol = 1e-5 * scale + FP32_TO_4ULP_FP64 * sens[k]
+        report.append((k, diff / scale if scale > 0 else diff))
+        if not diff <= tol:
+            bad.append((k, diff, tol))
+    assert tuple(g["g"]["dims"]) == tuple(o["g"]["dims"])
+    for k, kk in (("grid mass", "mass"), ("grid v", "v")):
+        e = rel(g["g"][kk], o["g"][kk])
+        report.append((k, e))
+        if not e <= REL_MIXED[k] + FP32_TO_4ULP_FP64 * sens.get(k, 0.0) / max(np.abs(o["g"][kk]).max(), 1e-300):
+            bad.append((k, e))
+    assert not bad, f"mixed vs oracle: {bad}; all: {report}"
+
+
+@pytest.mark.parametrize("model", ["noplast", "neohookean", "dp", "dpsoft", "dpvisc", "dpmui", "mccvisc", "vm"])
+def test_mixed_one_step_models(model):
+    if model not in cases.MODEL_CASES:
+        pytest.skip("model case not defined")
+    sc = cases.apply(cases.block(3, 3, n=5), **cases.MODEL_CASES[model])
+    sc = cases.box_plates(sc, BC.SlipStick, 0.3)
+    check_one_step(sc, [])
+
+
+@pytest.mark.parametrize("dim,deg", [(2, 2), (2, 3), (3, 2)])
+@pytest.mark.parametrize("transfer", ["apic_usl", "aflip_musl", "picflip_usl"])
+def test_mixed_one_step_transfers(transfer, dim, deg):
+    sc = cases.apply(cases.block(dim, deg, n=6 if dim == 3 else 10), plastic_model=cases.PM.DP, M=0.6,
+                     **cases.TRANSFER_CASES[transfer])
+    sc = cases.box_plates(sc, BC.SlipFree, 0.4)
+    check_one_step(sc, [])
+
+
+def test_mixed_objects_and_mibf():
+    sc = cases.apply(cases.block(3, 2, n=5), plastic_model=cases.PM.DPVisc, M=0.5, use_mibf=1)
+    sc.objects = cases.object_cases(3)["two_objects"] + cases.object_cases(3)["box"]
+    check_one_step(sc, [])
+
+
+@pytest.mark.parametrize("prec,tol", [(PREC_FP64, 1e-12), (PREC_MIXED, 2e-6)])
+@pytest.mark.parametrize("transfer", ["apic_usl", "aflip_musl", "picflip_usl"])
+def test_mass_and_momentum_balance(prec, tol, transfer):
+    """Grid mass and momentum after P2G equal the particles' (checkMassConservation /
+    checkMomentumConservation, simulation.cpp:292-333): quadratic and cubic
+    B-splines reproduce constants and linears, so APIC's affine term adds no
+    net momentum."""
+    from matter_tests_b200.gpu import GpuSim
+    sc = cases.apply(cases.block(3, 3, n=6), plastic_model=cases.PM.DP, M=0.6, **cases.TRANSFER_CASES[transfer])
+    p = copy.copy(sc.params)
+    p.precision = prec
+    g = GpuSim(p)
+    g.upload(sc.x, sc.v, sc.F, sc.B, sc.scalars)
+    g.set_objects([], [])
+    for _ in range(3):
+        g.step(1)
+        b = g.balance()
+        assert abs(b["grid_mass"] - b["particle_mass"]) <= tol * b["particle_mass"]
+        pscale = b["particle_mass"] * np.abs(g.particles()["v"]).max()
+        assert np.abs(b["grid_momentum"] - b["particle_momentum"]).max() <= tol * pscale, b
+    g.close()
+
+
+def run_steps(sc, prec, n):
+    from matter_tests_b200.gpu import GpuSim
+    p = copy.copy(sc.params)
+    p.precision = prec
+    g = GpuSim(p)
+    g.upload(sc.x, sc.v, sc.F, sc.B, sc.scalars)
+    g.set_objects(sc.plates, sc.objects)
+    g.step(n)
+    out = g.particles()
+    ck = g.clock()
+    status = g.status()
+    g.close()
+    return out, ck, status
+
+
+@pytest.mark.parametrize("builder,scale", [("collapse3d_mui", 0.25), ("collapse2d", 0.5), ("incline3d_mcc", 0.2)])
+def test_mixed_thousand_steps_against_fp64(builder, scale):
+    """1000 steps of each workload: mixed-precision positions stay within
+    1e-4 dx of the FP64 step's, velocities within 1e-3 of the FP64 scale."""
+    sc = scenes.WORKLOADS[builder](scale=scale)
+    ref, ck64, st64 = run_steps(sc, PREC_FP64, 1000)
+    got, ck32, st32 = run_steps(sc, PREC_MIXED, 1000)
+    assert st64[0] == 0 and st32[0] == 0, (st64, st32)
+    assert ck64["step"] == ck32["step"] == 1000
+    dxerr = np.abs(got["x"] - ref["x"]).max() / sc.params.dx
+    verr = rel(got["v"], ref["v"])
+    assert dxerr <= 1e-4, (dxerr, verr)
+    assert verr <= 1e-3, (dxerr, verr)
+
+
+@pytest.mark.parametrize("builder,scale", [("collapse3d_mui", 0.125), ("collapse2d", 0.25)])
+def test_fp64_thousand_steps_against_the_oracle(builder, scale):
+    """1000 FP64 steps against the oracle: positions within 1e-8 dx and
+    velocities within 1e-6 of their scale (the only difference is the order
+    of the GPU's floating-point atomic sums, amplified by the flow)."""
+    sc = scenes.WORKLOADS[builder](scale=scale)
+    got, ck, st = run_steps(sc, PREC_FP64, 1000)
+    o = run_oracle(sc, 1000)
+    assert ck["step"] == o["c"]["step"] == 1000
+    dxerr = np.abs(got["x"] - o["p"]["x"]).max() / sc.params.dx
+    verr = rel(got["v"], o["p"]["v"])
+    assert dxerr <= 1e-8, (dxerr, verr)
+    assert verr <= 1e-6, (dxerr, verr)
