@@ -46,7 +46,7 @@ FALLBACK_HBM_GBS = 6650.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--workload", default="collapse3d_mui")
@@ -162,27 +162,26 @@ def kernel_bytes(name, p, Np, Ga, G, wr=8.0):
     d = p.dim
     dd = d * d
     ns = 6 if d == 3 else 3
-    wx = 8.0
-    nch = 2 + 2 * d
+    w8 = 8.0  # positions and node velocities: FP64 on both paths
     if name == "k_p2g":
-        return Np * (wx * d + wr * (d + dd + ns + (1 if p.use_mibf else 0))) + Ga * wr * (1 + 2 * d)
+        return Np * (w8 * d + wr * (d + dd + ns + (1 if p.use_mibf else 0))) + Ga * wr * (1 + 2 * d)
     if name == "k_g2p":
-        return (Np * (wx * d + wr * (d + dd + 5)) + Ga * wr * 2 * d
-                + Np * (wx * d + wr * (d + 2 * dd + 6 + ns) + 4))
+        return (Np * (w8 * d + wr * (d + dd + 5)) + Ga * (w8 * d + wr * d)
+                + Np * (w8 * d + wr * (d + 2 * dd + 6 + ns) + 4))
     if name == "k_g2p_musl":
-        return Np * (wx * d + wr * d) + Ga * wr * 2 * d + Np * (wx * d + wr * (d + dd) + 4) + Ga * wr * d
+        return Np * (w8 * d + wr * d) + Ga * (w8 * d + wr * d) + Np * (w8 * d + wr * (d + dd) + 4) + Ga * w8 * d
     if name == "k_defgrad":
-        return Np * (wx * d + wr * (dd + 5)) + Ga * wr * d + Np * wr * (dd + 6 + ns)
+        return Np * (w8 * d + wr * (dd + 5)) + Ga * w8 * d + Np * wr * (dd + 6 + ns)
     if name == "k_grid":
-        return G * wr * (nch + 2 * d + 1 + nch)
+        return G * (2 * wr * (2 + 2 * d) + w8 * d + wr * (d + 1))
     if name == "k_musl_norm":
-        return G * wr * (1 + 2 * d)
+        return G * (wr + 2 * w8 * d)
     if name.startswith("k_sort_hist"):
-        return Np * (wx * d + 4) if "keys" in name else Np * 4
+        return Np * (w8 * d + 4) if "keys" in name else Np * 4
     if name == "k_sort_scatter":
         return Np * 16
     if name == "k_bbox":
-        return Np * (wx * d + wr * d)
+        return Np * (w8 * d + wr * d)
     return None
 
 

@@ -81,7 +81,8 @@ struct mtr_ctx {
   uint32_t cap_axis[3] = {0, 0, 0};
   uint32_t cap_nodes = 0, cap_tiles = 0;
   double *gx = nullptr, *gy = nullptr, *gz = nullptr;
-  void *acc = nullptr, *nv = nullptr, *nflip = nullptr, *nmass = nullptr, *nfric = nullptr, *v2 = nullptr;
+  void *acc = nullptr, *nflip = nullptr, *nmass = nullptr, *nfric = nullptr;
+  double *nv = nullptr, *v2 = nullptr;  // node velocities: FP64 on both paths
   uint32_t *tile_begin = nullptr, *tile_end = nullptr;
   // sort
   uint32_t *keys0 = nullptr, *keysA = nullptr, *valsA = nullptr, *keysB = nullptr, *valsB = nullptr;
@@ -127,11 +128,12 @@ int guarded(F&& f) {
 }
 
 void free_grid(mtr_ctx* c) {
-  for (void* p : {(void*)c->gx, (void*)c->gy, (void*)c->gz, (void*)c->acc, (void*)c->nv, (void*)c->nflip,
-                  (void*)c->nmass, (void*)c->nfric, (void*)c->v2, (void*)c->tile_begin, (void*)c->tile_end})
+  for (void* p : {(void*)c->gx, (void*)c->gy, (void*)c->gz, (void*)c->acc, (void*)c->nv,
+                  (void*)c->nflip, (void*)c->nmass, (void*)c->nfric, (void*)c->v2, (void*)c->tile_begin,
+                  (void*)c->tile_end})
     dfree(p);
-  c->gx = c->gy = c->gz = nullptr;
-  c->acc = c->nv = c->nflip = c->nmass = c->nfric = c->v2 = nullptr;
+  c->gx = c->gy = c->gz = c->nv = c->v2 = nullptr;
+  c->acc = c->nflip = c->nmass = c->nfric = nullptr;
   c->tile_begin = c->tile_end = nullptr;
 }
 
@@ -159,24 +161,24 @@ void alloc_grid(mtr_ctx* c, const uint32_t want[3]) {
     throw MtrError{MTR_ERR_OOM, "grid capacity exceeds the 32-bit node/key range"};
   c->cap_nodes = (uint32_t)nodes;
   c->cap_tiles = (uint32_t)tiles;
-  const int nch = 2 + 2 * d;
+  const int nch = 2 + 2 * d;  // mass, momentum, force, friction
   const size_t rs = c->rsize;
   c->gx = dalloc<double>(c->cap_axis[0]);
   c->gy = dalloc<double>(c->cap_axis[1]);
   c->gz = dalloc<double>(c->cap_axis[2]);
   c->acc = dalloc<unsigned char>(rs * nch * nodes);
-  c->nv = dalloc<unsigned char>(rs * d * nodes);
+  c->nv = dalloc<double>((size_t)d * nodes);
   c->nflip = dalloc<unsigned char>(rs * d * nodes);
   c->nmass = dalloc<unsigned char>(rs * nodes);
   c->nfric = dalloc<unsigned char>(rs * nodes);
-  c->v2 = dalloc<unsigned char>(rs * d * nodes);
+  c->v2 = dalloc<double>((size_t)d * nodes);
   c->tile_begin = dalloc<uint32_t>(tiles);
   c->tile_end = dalloc<uint32_t>(tiles);
   CK(cudaMemsetAsync(c->acc, 0, rs * nch * nodes, c->stream));
-  CK(cudaMemsetAsync(c->nv, 0, rs * d * nodes, c->stream));
+  CK(cudaMemsetAsync(c->nv, 0, sizeof(double) * d * nodes, c->stream));
   CK(cudaMemsetAsync(c->nflip, 0, rs * d * nodes, c->stream));
   CK(cudaMemsetAsync(c->nmass, 0, rs * nodes, c->stream));
-  CK(cudaMemsetAsync(c->v2, 0, rs * d * nodes, c->stream));
+  CK(cudaMemsetAsync(c->v2, 0, sizeof(double) * d * nodes, c->stream));
   uint64_t keybits = 1;
   while ((1ull << keybits) < tiles * 64ull) ++keybits;
   c->passes = (int)((keybits + 7) / 8);
@@ -236,11 +238,11 @@ StepArgsT<R> make_args(mtr_ctx* c, int parity) {
   A.cap_nodes = c->cap_nodes;
   A.cap_tiles = c->cap_tiles;
   A.acc = (R*)c->acc;
-  A.nv = (R*)c->nv;
+  A.nv = c->nv;
   A.nflip = (R*)c->nflip;
   A.nmass = (R*)c->nmass;
   A.nfric = (R*)c->nfric;
-  A.v2 = (R*)c->v2;
+  A.v2 = c->v2;
   A.xin = c->buf[parity].x;
   A.keys0 = c->keys0;
   A.keysA = c->keysA;
@@ -310,7 +312,7 @@ int enqueue_step_t(mtr_ctx* c, int parity) {
   ++n;
   mark(c, "k_grid");
   if (c->prm.use_musl) {
-    CK(cudaMemsetAsync(c->v2, 0, sizeof(R) * D * c->cap_nodes, st));
+    CK(cudaMemsetAsync(c->v2, 0, sizeof(double) * D * c->cap_nodes, st));
     mark(c, "memset(v2)");
     k_g2p_musl_w<D, DEG, R><<<c->cap_tiles, kChunk, musl_smem_bytes<D, R>(), st>>>(A, perm);
     mark(c, "k_g2p_musl");
@@ -566,7 +568,7 @@ int mtr_upload(mtr_ctx* c, const double* x, const double* v, const double* F, co
     c->hp.Np = Np;
     const size_t rs = c->rsize;
     for (int s = 0; s < 2; ++s) {
-      double* xb = dalloc<double>((size_t)Np * d);
+      double* xb = dalloc<double>((size_t)Np * d);  // positions: FP64 on both paths
       unsigned char* blk = dalloc<unsigned char>(rs * Np * (d + 2 * dd + MTR_NUM_SCALARS + ns));
       c->pallocs.push_back(xb);
       c->pallocs.push_back(blk);
@@ -864,9 +866,13 @@ int mtr_get_grid(mtr_ctx* c, uint32_t dims[3], double* gx, double* gy, double* g
     for (int w = 0; w < 2; ++w) {
       double* host = w == 0 ? v : flip;
       if (!host) continue;
-      const unsigned char* src = (const unsigned char*)(w == 0 ? (c->prm.use_musl ? c->v2 : c->nv) : c->nflip);
       for (int a = 0; a < d; ++a) {
-        get_nodes(c, tmp.data(), src + c->rsize * a * c->cap_nodes, G);
+        if (w == 0) {  // node velocities are FP64 on both paths
+          const double* src = (c->prm.use_musl ? c->v2 : c->nv) + (size_t)a * c->cap_nodes;
+          CK(cudaMemcpy(tmp.data(), src, sizeof(double) * G, cudaMemcpyDeviceToHost));
+        } else {
+          get_nodes(c, tmp.data(), (const unsigned char*)c->nflip + c->rsize * a * c->cap_nodes, G);
+        }
         for (uint32_t l = 0; l < G; ++l) host[(size_t)l * d + a] = tmp[l];
       }
     }

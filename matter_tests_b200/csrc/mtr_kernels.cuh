@@ -26,12 +26,15 @@
 // Precision.  Every kernel that touches particle or grid state is templated
 // on the storage type R.  R = double is the reference's FP64 arithmetic,
 // operation for operation.  R = float is the mixed-precision form: particle
-// v, F, B, stress and plastic scalars, the grid channels, the spline weights,
-// the P2G/MUSL accumulation and the G2P gathers are FP32; positions, the
-// clock and the grid axes stay FP64, and so do the deformation update, the
-// SVD, the Hencky log/exp, the return mapping with its projections, and the
-// mass and momentum balances.  F is stored as F - I in FP32, so its rounding
-// is relative to the strain (about 1e-3) rather than to 1.
+// v, F, B, stress and plastic scalars, the grid mass, momentum, force,
+// friction and flip channels, the spline weights, the P2G and MUSL sums and
+// the G2P gathers are FP32.  FP64 stays on the positions, the clock, the grid
+// axes and node velocities, the deformation update, the SVD, the Hencky
+// log/exp, the return mapping with its projections, and the mass and
+// momentum balances.  F is stored as F - I in FP32, so its rounding is
+// relative to the strain (about 1e-3) rather than to 1; the gathers work on
+// FP32 deviations from a per-tile reference velocity, so the FP32 sums that
+// form grad v do not cancel a common velocity.
 #pragma once
 #include <type_traits>
 
@@ -76,12 +79,12 @@ struct StepCommon {
 
 template <typename R>
 struct StepArgsT : StepCommon {
-  R* acc;    // [NCH][cap_nodes] P2G accumulators: mass, mom[D], force[D], friction
-  R* nv;     // [D][cap_nodes]  node velocity after the update (MUSL: after re-projection)
-  R* nflip;  // [D][cap_nodes]
-  R* nmass;  // [cap_nodes]
-  R* nfric;  // [cap_nodes]
-  R* v2;     // [D][cap_nodes]  MUSL re-projection accumulator
+  R* acc;         // [NCH][cap_nodes] P2G accumulators: mass, mom[D], force[D], friction
+  double* nv;     // [D][cap_nodes] node velocity after the update (FP64 on both paths)
+  R* nflip;       // [D][cap_nodes]
+  R* nmass;       // [cap_nodes]
+  R* nfric;       // [cap_nodes]
+  double* v2;     // [D][cap_nodes] MUSL re-projection accumulator (FP64 on both paths)
   PBufT<R> in, out;
   R* pic;   // optional [D][Np] in output order
   R* flip;  // optional [D][Np]
@@ -843,7 +846,6 @@ __global__ void __launch_bounds__(256) k_grid(StepArgsT<R> A) {
   __shared__ mtr_plate plates[MTR_MAXP];
   for (int i = threadIdx.x; i < P.nplates; i += blockDim.x) plates[i] = H->plates[i];
   __syncthreads();
-  constexpr int NCH = Tiling<D>::NCH;
   double sum_m = 0.0, sum_p[3] = {0.0, 0.0, 0.0};  // mass and momentum balance (simulation.cpp:292-333)
   for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < G; l += gridDim.x * blockDim.x) {
     const double mraw = A.acc[l];
@@ -878,13 +880,13 @@ __global__ void __launch_bounds__(256) k_grid(StepArgsT<R> A) {
     }
 #pragma unroll
     for (int a = 0; a < D; ++a) {
-      A.nv[(size_t)a * cap + l] = (R)v[a];
+      A.nv[(size_t)a * cap + l] = v[a];
       A.nflip[(size_t)a * cap + l] = (R)fl[a];
     }
     A.nmass[l] = (R)mi;
     if (P.use_mibf) A.nfric[l] = (R)fric;
 #pragma unroll
-    for (int ch = 0; ch < NCH; ++ch) A.acc[(size_t)ch * cap + l] = R(0.0);  // ready for the next step
+    for (int ch = 0; ch < Tiling<D>::NCH; ++ch) A.acc[(size_t)ch * cap + l] = R(0.0);  // ready for the next step
   }
   block_add(sum_m * P.particle_mass, &H->grid_mass);
 #pragma unroll
@@ -999,14 +1001,56 @@ __device__ __forceinline__ void load_node_patch(const StepCommon& A, const StepH
   }
 }
 
+// Reference velocity of a tile: the FP64 node velocity at the patch node
+// nearest the tile centre (zero outside the grid, and always zero on the FP64
+// path, which gathers the node velocities themselves).
+template <int D, typename R>
+__device__ __forceinline__ void tile_vref(const StepCommon& A, const StepHeader* H, const int (&n0)[3],
+                                          const double* src, double (&vref)[3]) {
+  vref[0] = vref[1] = vref[2] = 0.0;
+  if constexpr (!kFP64<R>) {
+    constexpr int c = 1 + Tiling<D>::TB / 2;
+    const int gi = n0[0] + c, gj = n0[1] + c, gk = D == 3 ? n0[2] + c : 0;
+    if (gi < (int)H->N[0] && gj < (int)H->N[1] && gk < (int)H->N[2]) {
+      const uint32_t l = node_index(H, gi, gj, gk);
+#pragma unroll
+      for (int a = 0; a < D; ++a) vref[a] = src[(size_t)a * A.cap_nodes + l];
+    }
+  }
+}
+
+// node velocity patch as deviations from vref, rounded to R
+template <int D, typename R>
+__device__ __forceinline__ void load_velocity_patch(const StepCommon& A, const StepHeader* H, const int (&n0)[3],
+                                                    const double* src, const double (&vref)[3],
+                                                    R* dst /*[D][NODES]*/) {
+  constexpr int NODES = Tiling<D>::NODES;
+  const uint32_t cap = A.cap_nodes;
+  for (int n = threadIdx.x; n < NODES; n += blockDim.x) {
+    uint32_t l = 0;
+    const bool in = patch_node<D>(H, n0, n, l);
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      if constexpr (kFP64<R>)
+        dst[a * NODES + n] = in ? src[(size_t)a * cap + l] : 0.0;
+      else
+        dst[a * NODES + n] = in ? (R)(src[(size_t)a * cap + l] - vref[a]) : R(0.0);
+    }
+  }
+}
+
 // G2P gather (g2p.cpp:24-77) and velocity gradient (deformation_update.cpp:17-40)
 // from a shared node patch; lb = stencil base relative to the patch origin.
 // Sums are factorised over the tensor-product stencil.  The offsets and the
-// spline argument are formed in FP64 from the FP64 position, then rounded to R.
+// spline argument are formed in FP64 from the FP64 position, then rounded to
+// R.  pv holds node velocities minus vref: B-spline weights sum to one and
+// reproduce linears, so pic = vref + sum w dv, while B and grad v need the
+// deviations only.
 template <int D, int DEG, bool GRADV, typename R>
 __device__ __forceinline__ void gather_patch(const R* pv, const R* pf, const double (*crd)[Tiling<D>::PN],
-                                             const int (&lb)[3], const double (&xp)[3], double ioh, R (&pic)[3],
-                                             R (&Bp)[D][D], R (&flp)[3], R (&gv)[D][D], bool want_b, bool want_flip) {
+                                             const int (&lb)[3], const double (&xp)[3], double ioh,
+                                             const double (&vref)[3], double (&pic)[3], R (&Bp)[D][D], R (&flp)[3],
+                                             R (&gv)[D][D], bool want_b, bool want_flip) {
   constexpr int PN = Tiling<D>::PN, NODES = Tiling<D>::NODES;
   R w[3][4], dw[3][4], pd[3][4];
 #pragma unroll
@@ -1019,8 +1063,9 @@ __device__ __forceinline__ void gather_patch(const R* pv, const R* pf, const dou
       dw[a][o] = GRADV ? bspline_dN<DEG>(u) : R(0.0);
       pd[a][o] = (R)(c - xp[a]);
     }
+  R ps[3];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) pic[a] = flp[a] = R(0.0);
+  for (int a = 0; a < 3; ++a) ps[a] = flp[a] = R(0.0);
 #pragma unroll
   for (int r = 0; r < D; ++r)
 #pragma unroll
@@ -1040,7 +1085,7 @@ __device__ __forceinline__ void gather_patch(const R* pv, const R* pf, const dou
 #pragma unroll
         for (int a = 0; a < D; ++a) vi[a] = pv[a * NODES + node];
 #pragma unroll
-        for (int a = 0; a < D; ++a) pic[a] += vi[a] * weight;
+        for (int a = 0; a < D; ++a) ps[a] += vi[a] * weight;
         if (want_b) {
           R wpd[3] = {weight * pd[0][ii], weight * pd[1][jj], D == 3 ? weight * pd[2][kk] : R(0.0)};
 #pragma unroll
@@ -1069,6 +1114,13 @@ __device__ __forceinline__ void gather_patch(const R* pv, const R* pf, const dou
         }
       }
     }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if constexpr (kFP64<R>)
+      pic[a] = ps[a];
+    else
+      pic[a] = vref[a] + (double)ps[a];
+  }
   if (GRADV) {
     const R iohR = (R)ioh;
 #pragma unroll
@@ -1097,8 +1149,11 @@ __global__ void __launch_bounds__(kChunk, MTR_RM_MIN_BLOCKS) k_g2p_t(StepArgsT<R
   __shared__ double crd[3][PN];
   int n0[3];
   load_tile_setup<D>(A, H, t, n0, crd);
-  const R* const src[2] = {A.nv, A.nflip};
-  load_node_patch<D, 2, R>(A, H, n0, src, pv);
+  double vref[3];
+  tile_vref<D, R>(A, H, n0, A.nv, vref);
+  load_velocity_patch<D, R>(A, H, n0, A.nv, vref, pv);
+  const R* const src[1] = {A.nflip};
+  load_node_patch<D, 1, R>(A, H, n0, src, pv + D * NODES);
   __syncthreads();
   const uint32_t Np = A.Np;
   const double dt = H->dt, fr = P.flip_ratio, ioh = P.one_over_dx;
@@ -1107,14 +1162,18 @@ __global__ void __launch_bounds__(kChunk, MTR_RM_MIN_BLOCKS) k_g2p_t(StepArgsT<R
     const uint32_t j = perm[s];
     PLoad<D> p;
     load_particle<D, R>(A.in, Np, j, p);
-    R pic[3], flp[3], Bp[D][D], gv[D][D];
+    double pic[3];
+    R flp[3], Bp[D][D], gv[D][D];
     int lb[3];
     if (local_base<D>(H, p.x, ioh, n0, false, lb)) {
-      gather_patch<D, DEG, true, R>(pv, pv + D * NODES, crd, lb, p.x, ioh, pic, Bp, flp, gv, fr < 0, fr >= -1);
+      gather_patch<D, DEG, true, R>(pv, pv + D * NODES, crd, lb, p.x, ioh, vref, pic, Bp, flp, gv, fr < 0, fr >= -1);
     } else {
       raise_status(H, MTR_STATUS_STENCIL_OOB, p.id);
 #pragma unroll
-      for (int a = 0; a < 3; ++a) pic[a] = flp[a] = R(0.0);
+      for (int a = 0; a < 3; ++a) {
+        pic[a] = 0.0;
+        flp[a] = R(0.0);
+      }
 #pragma unroll
       for (int r = 0; r < D; ++r)
 #pragma unroll
@@ -1128,8 +1187,8 @@ __global__ void __launch_bounds__(kChunk, MTR_RM_MIN_BLOCKS) k_g2p_t(StepArgsT<R
     double xn[3], vn[3];
 #pragma unroll
     for (int a = 0; a < D; ++a) {
-      xn[a] = p.x[a] + dt * (double)pic[a];
-      vn[a] = blend_v(fr, p.v[a], (double)flp[a], (double)pic[a]);
+      xn[a] = p.x[a] + dt * pic[a];
+      vn[a] = blend_v(fr, p.v[a], (double)flp[a], pic[a]);
     }
     if (P.change_particle_positions && xn[0] > 0.8) {  // position_update.cpp:35-41
       xn[0] = -0.1;
@@ -1148,7 +1207,7 @@ __global__ void __launch_bounds__(kChunk, MTR_RM_MIN_BLOCKS) k_g2p_t(StepArgsT<R
     if (P.store_pic_flip) {
 #pragma unroll
       for (int a = 0; a < D; ++a) {
-        A.pic[(size_t)a * Np + s] = pic[a];
+        A.pic[(size_t)a * Np + s] = (R)pic[a];
         A.flip[(size_t)a * Np + s] = (fr >= -1) ? flp[a] : R(0.0);
       }
     }
@@ -1217,8 +1276,11 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgsT<R> A, const uin
   MStage<D, R>* st = reinterpret_cast<MStage<D, R>*>(smem_raw + musl_crd_bytes<D, R>() + musl_patch_bytes<D, R>());
   int n0[3];
   load_tile_setup<D>(A, H, t, n0, crd);
-  const R* const src[2] = {A.nv, A.nflip};
-  load_node_patch<D, 2, R>(A, H, n0, src, pv);
+  double vref[3];
+  tile_vref<D, R>(A, H, n0, A.nv, vref);
+  load_velocity_patch<D, R>(A, H, n0, A.nv, vref, pv);
+  const R* const src[1] = {A.nflip};
+  load_node_patch<D, 1, R>(A, H, n0, src, pv + D * NODES);
   for (int i = threadIdx.x; i < D * NODES; i += blockDim.x) (&vsum[0][0])[i] = R(0.0);
   __syncthreads();
   const uint32_t Np = A.Np;
@@ -1246,15 +1308,20 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgsT<R> A, const uin
           vp[a] = A.in.v[(size_t)a * Np + j];
         }
         const uint32_t pid = A.in.id[j];
-        R pic[3], flp[3], Bp[D][D], gv[D][D];
+        double pic[3];
+        R flp[3], Bp[D][D], gv[D][D];
         int lb[3];
         const bool ok = local_base<D>(H, xp, ioh, n0, false, lb);
         if (ok) {
-          gather_patch<D, DEG, false, R>(pv, pv + D * NODES, crd, lb, xp, ioh, pic, Bp, flp, gv, apic, fr >= -1);
+          gather_patch<D, DEG, false, R>(pv, pv + D * NODES, crd, lb, xp, ioh, vref, pic, Bp, flp, gv, apic,
+                                         fr >= -1);
         } else {
           raise_status(H, MTR_STATUS_STENCIL_OOB, pid);
 #pragma unroll
-          for (int a = 0; a < 3; ++a) pic[a] = flp[a] = R(0.0);
+          for (int a = 0; a < 3; ++a) {
+            pic[a] = 0.0;
+            flp[a] = R(0.0);
+          }
 #pragma unroll
           for (int r = 0; r < D; ++r)
 #pragma unroll
@@ -1262,10 +1329,10 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgsT<R> A, const uin
         }
 #pragma unroll
         for (int a = 0; a < D; ++a) {
-          const double vn = blend_v(fr, vp[a], (double)flp[a], (double)pic[a]);
+          const double vn = blend_v(fr, vp[a], (double)flp[a], pic[a]);
           if constexpr (kFP64<R>) S.x[a] = xp[a];
           S.v[a] = (R)vn;
-          A.out.x[(size_t)a * Np + s] = xp[a] + dt * (double)pic[a];  // positionUpdate: x + dt pic
+          A.out.x[(size_t)a * Np + s] = xp[a] + dt * pic[a];  // positionUpdate: x + dt pic
           A.out.v[(size_t)a * Np + s] = (R)vn;
         }
 #pragma unroll
@@ -1280,7 +1347,7 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgsT<R> A, const uin
         if (P.store_pic_flip) {
 #pragma unroll
           for (int a = 0; a < D; ++a) {
-            A.pic[(size_t)a * Np + s] = pic[a];
+            A.pic[(size_t)a * Np + s] = (R)pic[a];
             A.flip[(size_t)a * Np + s] = (fr >= -1) ? flp[a] : R(0.0);
           }
         }
@@ -1367,7 +1434,7 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgsT<R> A, const uin
 #pragma unroll
     for (int a = 0; a < D; ++a) {
       const R val = vsum[a][n];
-      if (val != R(0.0)) atomicAdd(&A.v2[(size_t)a * cap + l], val);
+      if (val != R(0.0)) atomicAdd(&A.v2[(size_t)a * cap + l], (double)val);
     }
   }
 }
@@ -1383,8 +1450,8 @@ __global__ void __launch_bounds__(256) k_musl_norm(StepArgsT<R> A) {
     const double mi = A.nmass[l];
 #pragma unroll
     for (int a = 0; a < D; ++a) {
-      R* p = &A.v2[(size_t)a * cap + l];
-      *p = (mi > 0) ? (R)((double)*p / (mi / mp)) : R(0.0);
+      double* p = &A.v2[(size_t)a * cap + l];
+      *p = (mi > 0) ? *p / (mi / mp) : 0.0;
     }
   }
 }
@@ -1405,8 +1472,9 @@ __global__ void __launch_bounds__(kChunk, MTR_RM_MIN_BLOCKS) k_defgrad_t(StepArg
   __shared__ double crd[3][PN];
   int n0[3];
   load_tile_setup<D>(A, H, t, n0, crd);
-  const R* const src[1] = {A.v2};
-  load_node_patch<D, 1, R>(A, H, n0, src, pv);
+  double vref[3];
+  tile_vref<D, R>(A, H, n0, A.v2, vref);
+  load_velocity_patch<D, R>(A, H, n0, A.v2, vref, pv);
   __syncthreads();
   const uint32_t Np = A.Np;
   const double dt = H->dt, ioh = A.P->one_over_dx;
@@ -1415,10 +1483,11 @@ __global__ void __launch_bounds__(kChunk, MTR_RM_MIN_BLOCKS) k_defgrad_t(StepArg
     const uint32_t j = perm[s];
     PLoad<D> p;
     load_particle<D, R>(A.in, Np, j, p);
-    R pic[3], flp[3], Bp[D][D], gv[D][D];
+    double pic[3];
+    R flp[3], Bp[D][D], gv[D][D];
     int lb[3];
     if (local_base<D>(H, p.x, ioh, n0, false, lb)) {
-      gather_patch<D, DEG, true, R>(pv, nullptr, crd, lb, p.x, ioh, pic, Bp, flp, gv, false, false);
+      gather_patch<D, DEG, true, R>(pv, nullptr, crd, lb, p.x, ioh, vref, pic, Bp, flp, gv, false, false);
     } else {
       raise_status(H, MTR_STATUS_STENCIL_OOB, p.id);
 #pragma unroll
