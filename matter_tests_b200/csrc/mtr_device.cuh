@@ -203,7 +203,9 @@ __device__ __forceinline__ R bspline_dN(R u) {
 // symmetrising rotation §8.6.2; symSchur2 Alg. 8.5.1).  Output convention of
 // the Eigen::JacobiSVD the reference calls (plasticity.cpp:19,
 // simulation.hpp:232): singular values >= 0 in decreasing order, U and V
-// orthogonal (either may be improper), A = U diag(S) V^T.
+// orthogonal (either may be improper), A = U diag(S) V^T.  The cosines come
+// from one reciprocal square root each instead of a square root and a
+// division (same rotation, rounded differently at the last bit).
 // ---------------------------------------------------------------------------
 template <int D>
 __device__ __forceinline__ void jacobi_rotate(double (&A)[D][D], double (&U)[D][D], double (&V)[D][D], int q, int p,
@@ -212,10 +214,10 @@ __device__ __forceinline__ void jacobi_rotate(double (&A)[D][D], double (&U)[D][
   double c1 = 1.0, s1 = 0.0;
   const double tr = a + e, df = b - c;
   if (fabs(df) >= 2.2250738585072014e-308) {
-    double u = tr / df;
-    double r = sqrt(1.0 + u * u);
-    s1 = 1.0 / r;
-    c1 = u / r;
+    const double u = tr / df;
+    const double ri = rsqrt(1.0 + u * u);  // 1 / sqrt(1 + u^2) in one operation
+    s1 = ri;
+    c1 = u * ri;
   }
   const double m00 = c1 * a - s1 * c;
   const double m01 = c1 * b - s1 * e;
@@ -224,7 +226,7 @@ __device__ __forceinline__ void jacobi_rotate(double (&A)[D][D], double (&U)[D][
   if (m01 != 0.0) {
     double tau = (m11 - m00) / (2.0 * m01);
     double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-    cj = 1.0 / sqrt(1.0 + t * t);
+    cj = rsqrt(1.0 + t * t);
     sj = t * cj;
   }
   const double l00 = c1 * cj - s1 * sj, l01 = c1 * sj + s1 * cj;

@@ -596,9 +596,15 @@ __device__ __forceinline__ bool patch_node(const StepHeader* H, const int (&n0)[
 constexpr int kChunk = 128;
 
 // Minimum resident blocks per SM requested for the tile kernels that run the
-// return mapping (k_g2p_t, k_defgrad_t); it bounds their registers per thread.
-#ifndef MTR_RM_MIN_BLOCKS
-#define MTR_RM_MIN_BLOCKS 1
+// return mapping; it bounds their registers per thread.  Four blocks of 128
+// threads (128 registers, some spilled to L1) measured 15-25% faster for
+// k_defgrad_t than the unbounded two blocks (240 registers) on the 3D collapse;
+// three blocks measured best for k_g2p_t on the 3D Cam-Clay incline.
+#ifndef MTR_DEFGRAD_MIN_BLOCKS
+#define MTR_DEFGRAD_MIN_BLOCKS 4
+#endif
+#ifndef MTR_G2P_MIN_BLOCKS
+#define MTR_G2P_MIN_BLOCKS 3
 #endif
 
 // FP64 stage: the position is kept and node offsets are formed in phase 2.
@@ -1135,7 +1141,7 @@ __device__ __forceinline__ void gather_patch(const R* pv, const R* pf, const dou
 // block per tile, node patch in shared memory.
 // ---------------------------------------------------------------------------
 template <int D, int DEG, typename R>
-__global__ void __launch_bounds__(kChunk, MTR_RM_MIN_BLOCKS) k_g2p_t(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
+__global__ void __launch_bounds__(kChunk, MTR_G2P_MIN_BLOCKS) k_g2p_t(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
   using TL = Tiling<D>;
   constexpr int PN = TL::PN, NODES = TL::NODES;
   StepHeader* H = A.H;
@@ -1459,7 +1465,7 @@ __global__ void __launch_bounds__(256) k_musl_norm(StepArgsT<R> A) {
 // MUSL: deformation update from the normalised re-projected velocity v2 and
 // the old positions (deformation_update.cpp:6), then the return mapping.
 template <int D, int DEG, typename R>
-__global__ void __launch_bounds__(kChunk, MTR_RM_MIN_BLOCKS) k_defgrad_t(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
+__global__ void __launch_bounds__(kChunk, MTR_DEFGRAD_MIN_BLOCKS) k_defgrad_t(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
   using TL = Tiling<D>;
   constexpr int PN = TL::PN, NODES = TL::NODES;
   StepHeader* H = A.H;
