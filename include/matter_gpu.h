@@ -141,6 +141,7 @@ typedef struct mtr_clock {
 } mtr_clock;
 
 typedef struct mtr_ctx mtr_ctx;
+typedef struct mtr_batch mtr_batch;
 
 /* Validates the parameters and derives the constants of Simulation::simulate
  * (simulation.cpp:94-136: Lame constants, dt_max, prefactors, apicDinverse,
@@ -230,6 +231,28 @@ int mtr_active_nodes(mtr_ctx* ctx, uint64_t* active, uint64_t* total);
  * it.  Momenta are dim values. */
 int mtr_balance(mtr_ctx* ctx, double* grid_mass, double* grid_momentum, double* particle_mass,
                 double* particle_momentum);
+
+/* Batched stepping — no counterpart in the reference, which runs one
+ * Simulation per process.  A batch advances several uploaded contexts on one
+ * GPU together: contexts with the same dim, spline degree, precision and
+ * USL/MUSL choice form a group, and every phase of a step is one kernel launch
+ * for the whole group over a device table of the members' buffers, captured
+ * in a CUDA graph.  Each member keeps its own clock, grid, regrowth and end of
+ * simulation; mtr_batch_step(batch, n) advances every member by n steps (or to
+ * its end) and returns when all are there.  Members stay ordinary contexts
+ * (mtr_download, mtr_get_clock, mtr_status ... work as before), but must not
+ * be stepped on their own while the batch exists.  mtr_batch_destroy leaves
+ * the members alive.
+ *
+ * mtr_footprint estimates the device bytes mtr_upload will allocate for Np
+ * particles at positions x (AoS) with these parameters, for admission by
+ * memory budget; the grid may later grow with the scene. */
+int mtr_batch_create(mtr_ctx* const* ctxs, int n, mtr_batch** out);
+int mtr_batch_step(mtr_batch* batch, int nsteps);
+int64_t mtr_batch_launch_count(mtr_batch* batch);
+void* mtr_batch_stream(mtr_batch* batch);
+void mtr_batch_destroy(mtr_batch* batch);
+int mtr_footprint(const mtr_params* params, uint32_t Np, const double* x, uint64_t* bytes);
 
 /* mtr_p2g_noalloc — no counterpart in the reference.  The particle-to-grid
  * transfer (the P2G of p2g.cpp: grid mass = particle mass * sum of weights,

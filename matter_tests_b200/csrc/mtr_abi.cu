@@ -254,6 +254,9 @@ StepArgsT<R> make_args(mtr_ctx* c, int parity) {
   A.sort_blocks = c->sort_blocks;
   A.tile_begin = c->tile_begin;
   A.tile_end = c->tile_end;
+  A.skeys = (c->passes & 1) ? c->keysB : c->keysA;  // where the last radix pass writes
+  A.perm = (c->passes & 1) ? c->valsB : c->valsA;
+  A.out_parity = 1 - parity;
   A.in = typed<R>(c->buf[parity]);
   A.out = typed<R>(c->buf[1 - parity]);
   A.pic = (R*)c->pic;
@@ -445,19 +448,19 @@ void derive_constants(mtr_ctx* c) {  // simulation.cpp:94-136
 
 // The first step's grid extents, as remeshFixedInit(2,2,2) will compute them
 // (remesh.cpp:38-182), to size the initial grid allocation.
-void initial_grid_extent(mtr_ctx* c, const double* x, uint32_t want[3]) {
-  const int d = c->dim;
-  const double dx = c->prm.dx;
+void grid_extent(const mtr_params& p, uint32_t Np, const double* x, uint32_t want[3]) {
+  const int d = p.dim;
+  const double dx = p.dx;
   for (int a = 0; a < 3; ++a) want[a] = 1;
   for (int a = 0; a < d; ++a) {
     double mn = x[a], mx = x[a];
-    for (uint32_t p = 1; p < c->Np; ++p) {
-      double v = x[(size_t)p * d + a];
+    for (uint32_t q = 1; q < Np; ++q) {
+      double v = x[(size_t)q * d + a];
       mn = std::min(mn, v);
       mx = std::max(mx, v);
     }
-    const double g = c->prm.grid_reference_point[a];
-    if (c->prm.grid_reference_point[0] < 1e10) {
+    const double g = p.grid_reference_point[a];
+    if (p.grid_reference_point[0] < 1e10) {
       mn = std::min(mn, g);
       mx = std::max(mx, g);
     }
@@ -465,6 +468,8 @@ void initial_grid_extent(mtr_ctx* c, const double* x, uint32_t want[3]) {
     want[a] = (uint32_t)std::ceil(n * 1.25 + 8.0);
   }
 }
+
+void initial_grid_extent(mtr_ctx* c, const double* x, uint32_t want[3]) { grid_extent(c->prm, c->Np, x, want); }
 
 // SoA device array of the current particle order -> AoS host array in the
 // caller's order (kinds as k_soa_to_aos); f64 marks an FP64 array on either path.
@@ -499,9 +504,188 @@ void get_nodes(mtr_ctx* c, double* host, const void* src, size_t n) {
   for (size_t i = 0; i < n; ++i) host[i] = tmp[i];
 }
 
+// ---------------------------------------------------------------------------
+// Batches: scenes grouped by (dim, spline, precision, MUSL), one launch per
+// step phase and group over a device table of the scenes' arguments.
+// ---------------------------------------------------------------------------
+uint32_t cap_blocks(uint64_t work, uint32_t per_block, uint32_t cap) {
+  const uint64_t b = (work + per_block - 1) / per_block;
+  return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(b, cap));
+}
+
 }  // namespace
 
-// ===========================================================================
+struct mtr_batch_group {
+  int dim = 3, deg = 2, musl = 0;
+  bool fp32 = false;
+  int passes = 1;
+  std::vector<mtr_ctx*> members;
+  void* dargs = nullptr;      // StepArgsT<R>[2][n]
+  uint32_t* doff = nullptr;   // [kBK_KINDS][n + 1]
+  uint32_t total[kBK_KINDS] = {};
+};
+
+struct mtr_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<mtr_ctx*> members;
+  std::vector<mtr_batch_group> groups;
+  cudaGraphExec_t graph = nullptr;
+  bool dirty = true;
+  int64_t launches_last = 0;
+  int launches_per_step = 0;
+};
+
+namespace {
+
+void free_batch_tables(mtr_batch* b) {
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  for (auto& g : b->groups) {
+    dfree(g.dargs);
+    dfree(g.doff);
+    g.dargs = nullptr;
+    g.doff = nullptr;
+  }
+}
+
+template <typename R>
+void build_group_tables(mtr_batch* b, mtr_batch_group& g) {
+  const int n = (int)g.members.size();
+  g.passes = 1;
+  for (mtr_ctx* c : g.members) g.passes = std::max(g.passes, c->passes);
+  std::vector<StepArgsT<R>> args((size_t)2 * n);
+  std::vector<uint32_t> off((size_t)kBK_KINDS * (n + 1), 0u);
+  for (int s = 0; s < n; ++s) {
+    mtr_ctx* c = g.members[s];
+    if (c->passes != g.passes) free_graphs(c);  // its own graphs were captured with fewer passes
+    c->passes = g.passes;                      // extra radix passes over zero digits keep the order
+    for (int par = 0; par < 2; ++par) args[(size_t)par * n + s] = make_args<R>(c, par);
+    const uint32_t cnt[kBK_KINDS] = {
+        (uint32_t)c->npartials,
+        (uint32_t)c->sort_blocks,
+        256u,
+        cap_blocks(c->Np, 256, 148 * 8),
+        cap_blocks(std::max<uint64_t>(c->cap_tiles, g.musl ? (uint64_t)g.dim * c->cap_nodes : 0), 256, 148 * 8),
+        c->cap_tiles,
+        cap_blocks(c->cap_nodes, 256, 148 * 16),
+        1u};
+    for (int k = 0; k < kBK_KINDS; ++k) off[(size_t)k * (n + 1) + s + 1] = off[(size_t)k * (n + 1) + s] + cnt[k];
+  }
+  for (int k = 0; k < kBK_KINDS; ++k) g.total[k] = off[(size_t)k * (n + 1) + n];
+  g.dargs = dalloc<unsigned char>(sizeof(StepArgsT<R>) * args.size());
+  g.doff = dalloc<uint32_t>(off.size());
+  CK(cudaMemcpyAsync(g.dargs, args.data(), sizeof(StepArgsT<R>) * args.size(), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(g.doff, off.data(), sizeof(uint32_t) * off.size(), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+}
+
+template <int D, int DEG, typename R>
+int enqueue_group_step_t(mtr_batch* b, mtr_batch_group& g) {
+  cudaStream_t st = b->stream;
+  BatchView<R> B{(const StepArgsT<R>*)g.dargs, g.doff, (int)g.members.size()};
+  int n = 0;
+  kb_bbox<D, R><<<g.total[kBK_BBOX], 256, 0, st>>>(B);
+  kb_header<D, R><<<g.total[kBK_ONE], 32, 0, st>>>(B);
+  kb_clear<D, R><<<g.total[kBK_CLEAR], 256, 0, st>>>(B);
+  n += 3;
+  for (int pass = 0; pass < g.passes; ++pass) {
+    kb_sort_hist<D, R><<<g.total[kBK_SORT], kSortThreads, 0, st>>>(B, pass);
+    kb_sort_scan<R><<<g.total[kBK_SCAN], 256, 0, st>>>(B);
+    kb_sort_scatter<R><<<g.total[kBK_SORT], kSortThreads, 0, st>>>(B, pass);
+    n += 3;
+  }
+  kb_tile_ranges<R><<<g.total[kBK_TILES], 256, 0, st>>>(B);
+  kb_p2g_w<D, DEG, R><<<g.total[kBK_TILEK], kChunk, p2g_smem_bytes<D, R>(), st>>>(B);
+  kb_grid<D, R><<<g.total[kBK_NODES], 256, 0, st>>>(B);
+  n += 3;
+  if (g.musl) {
+    kb_g2p_musl_w<D, DEG, R><<<g.total[kBK_TILEK], kChunk, musl_smem_bytes<D, R>(), st>>>(B);
+    kb_musl_norm<D, R><<<g.total[kBK_NODES], 256, 0, st>>>(B);
+    kb_defgrad_t<D, DEG, R><<<g.total[kBK_TILEK], kChunk, 0, st>>>(B);
+    n += 3;
+  } else {
+    kb_g2p_t<D, DEG, R><<<g.total[kBK_TILEK], kChunk, 0, st>>>(B);
+    ++n;
+  }
+  kb_tail<D, R><<<g.total[kBK_ONE], 32, 0, st>>>(B);
+  ++n;
+  CK(cudaGetLastError());
+  return n;
+}
+
+template <typename R>
+int enqueue_group_step_r(mtr_batch* b, mtr_batch_group& g) {
+  if (g.dim == 3) return g.deg == 3 ? enqueue_group_step_t<3, 3, R>(b, g) : enqueue_group_step_t<3, 2, R>(b, g);
+  return g.deg == 3 ? enqueue_group_step_t<2, 3, R>(b, g) : enqueue_group_step_t<2, 2, R>(b, g);
+}
+
+template <int D, int DEG, typename R>
+void set_batch_attributes_t() {
+  CK(cudaFuncSetAttribute(kb_p2g_w<D, DEG, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)p2g_smem_bytes<D, R>()));
+  CK(cudaFuncSetAttribute(kb_g2p_musl_w<D, DEG, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)musl_smem_bytes<D, R>()));
+}
+
+void set_batch_attributes(const mtr_batch_group& g) {
+  if (g.fp32) {
+    if (g.dim == 3) g.deg == 3 ? set_batch_attributes_t<3, 3, float>() : set_batch_attributes_t<3, 2, float>();
+    else g.deg == 3 ? set_batch_attributes_t<2, 3, float>() : set_batch_attributes_t<2, 2, float>();
+  } else {
+    if (g.dim == 3) g.deg == 3 ? set_batch_attributes_t<3, 3, double>() : set_batch_attributes_t<3, 2, double>();
+    else g.deg == 3 ? set_batch_attributes_t<2, 3, double>() : set_batch_attributes_t<2, 2, double>();
+  }
+}
+
+constexpr int kBatchGraphSteps = 8;
+
+// (re)builds the device tables of every group and captures kBatchGraphSteps steps
+void rebuild_batch(mtr_batch* b) {
+  free_batch_tables(b);
+  for (auto& g : b->groups) {
+    set_batch_attributes(g);
+    if (g.fp32)
+      build_group_tables<float>(b, g);
+    else
+      build_group_tables<double>(b, g);
+  }
+  cudaGraph_t graph = nullptr;
+  CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  int n = 0;
+  try {
+    for (int s = 0; s < kBatchGraphSteps; ++s)
+      for (auto& g : b->groups) n += g.fp32 ? enqueue_group_step_r<float>(b, g) : enqueue_group_step_r<double>(b, g);
+  } catch (...) {
+    cudaStreamEndCapture(b->stream, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  CK(cudaStreamEndCapture(b->stream, &graph));
+  cudaError_t e = cudaGraphInstantiate(&b->graph, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) throw MtrError{MTR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)};
+  b->launches_per_step = n / kBatchGraphSteps;
+  b->dirty = false;
+}
+
+// reads every member's step header on the batch stream
+void read_batch_headers(mtr_batch* b) {
+  for (mtr_ctx* c : b->members)
+    CK(cudaMemcpyAsync(c->hH, c->dH, sizeof(StepHeader), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+}
+
+void write_batch_headers(mtr_batch* b) {
+  for (mtr_ctx* c : b->members)
+    CK(cudaMemcpyAsync(c->dH, c->hH, sizeof(StepHeader), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+}
+
+}  // namespace
+
 extern "C" {
 
 const char* mtr_last_error(void) { return g_last_error.c_str(); }
@@ -653,6 +837,7 @@ int mtr_upload(mtr_ctx* c, const double* x, const double* v, const double* F, co
     std::memset(c->hH, 0, sizeof(StepHeader));
     c->hH->first_bad = 0xffffffffu;
     c->hH->stop_frame = 0xffffffffu;
+    c->hH->stop_step = 0xffffffffu;
     for (int a = 0; a < 3; ++a) c->hH->gravity[a] = a < d ? c->prm.gravity[a] : 0.0;
     c->hH->done = (0 < c->prm.end_frame) ? 0 : 1;
     for (size_t i = 0; i < c->plates.size(); ++i) c->hH->plates[i] = c->plates[i];
@@ -1059,6 +1244,146 @@ int mtr_balance(mtr_ctx* c, double* grid_mass, double* grid_momentum, double* pa
     }
     return MTR_OK;
   });
+}
+
+int mtr_footprint(const mtr_params* params, uint32_t Np, const double* x, uint64_t* bytes) {
+  return guarded([&]() -> int {
+    if (!params || !x || !bytes || Np == 0) throw MtrError{MTR_ERR_INVALID, "null argument or Np == 0"};
+    const mtr_params& p = *params;
+    if ((p.dim != 2 && p.dim != 3) || !(p.dx > 0)) throw MtrError{MTR_ERR_INVALID, "dim must be 2 or 3, dx > 0"};
+    const uint64_t d = p.dim, dd = d * d, ns = p.dim == 3 ? 6 : 3, n = Np;
+    const uint64_t rs = p.precision == MTR_PREC_MIXED ? 4 : 8;
+    const uint64_t sort_blocks = (n + kSortTile - 1) / kSortTile;
+    uint64_t total = 2 * (8 * d * n + rs * n * (d + 2 * dd + MTR_NUM_SCALARS + ns) + 4 * n)  // particle buffers
+                     + 2 * rs * d * n                                                      // pic, flip
+                     + 5 * 4 * n + 4 * 256 * sort_blocks + 4 * 256                           // sort
+                     + 8 * n * std::max<uint64_t>(dd, MTR_NUM_SCALARS);                       // staging
+    uint32_t want[3];
+    grid_extent(p, Np, x, want);
+    const uint64_t tb = p.dim == 3 ? 4 : 8;
+    uint64_t nodes = 1, tiles = 1, axes = 0;
+    for (int a = 0; a < 3; ++a) {
+      const uint64_t cap = a < p.dim ? std::max<uint32_t>(want[a], 8u) : 1u;
+      nodes *= cap;
+      tiles *= a < p.dim ? (cap + tb - 1) / tb : 1;
+      axes += cap;
+    }
+    total += 8 * axes + rs * (2 + 2 * d) * nodes + 8 * d * nodes + rs * d * nodes + 2 * rs * nodes + 8 * d * nodes +
+             8 * tiles;
+    *bytes = total;
+    return MTR_OK;
+  });
+}
+
+int mtr_batch_create(mtr_ctx* const* ctxs, int n, mtr_batch** out) {
+  return guarded([&]() -> int {
+    if (!ctxs || !out || n <= 0) throw MtrError{MTR_ERR_INVALID, "null argument or n <= 0"};
+    *out = nullptr;
+    for (int i = 0; i < n; ++i) {
+      if (!ctxs[i] || !ctxs[i]->uploaded) throw MtrError{MTR_ERR_STATE, "every member needs mtr_upload first"};
+      if (ctxs[i]->device != ctxs[0]->device) throw MtrError{MTR_ERR_INVALID, "members must share one device"};
+      for (int j = 0; j < i; ++j)
+        if (ctxs[j] == ctxs[i]) throw MtrError{MTR_ERR_INVALID, "a context appears twice"};
+    }
+    mtr_batch* b = new mtr_batch();
+    try {
+      b->device = ctxs[0]->device;
+      CK(cudaSetDevice(b->device));
+      CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+      for (int i = 0; i < n; ++i) {
+        mtr_ctx* c = ctxs[i];
+        CK(cudaStreamSynchronize(c->stream));  // nothing of the member may still run on its own stream
+        b->members.push_back(c);
+        mtr_batch_group* g = nullptr;
+        for (auto& q : b->groups)
+          if (q.dim == c->dim && q.deg == c->deg && q.fp32 == c->fp32 && q.musl == (c->prm.use_musl ? 1 : 0)) g = &q;
+        if (!g) {
+          b->groups.emplace_back();
+          g = &b->groups.back();
+          g->dim = c->dim;
+          g->deg = c->deg;
+          g->fp32 = c->fp32;
+          g->musl = c->prm.use_musl ? 1 : 0;
+        }
+        g->members.push_back(c);
+      }
+    } catch (...) {
+      mtr_batch_destroy(b);
+      throw;
+    }
+    *out = b;
+    return MTR_OK;
+  });
+}
+
+int mtr_batch_step(mtr_batch* b, int nsteps) {
+  return guarded([&]() -> int {
+    if (!b) throw MtrError{MTR_ERR_INVALID, "null batch"};
+    if (nsteps <= 0) return MTR_OK;
+    CK(cudaSetDevice(b->device));
+    read_batch_headers(b);
+    for (mtr_ctx* c : b->members) {  // every member advances nsteps steps (or to its end)
+      StepHeader& H = *c->hH;
+      H.stop_step = (uint32_t)std::min<uint64_t>((uint64_t)H.step + (uint64_t)nsteps, 0xfffffffeull);
+    }
+    write_batch_headers(b);
+    int64_t launches = 0;
+    for (int guard = 0; guard < 64; ++guard) {
+      uint32_t remaining = 0;
+      for (mtr_ctx* c : b->members)
+        if (!c->hH->done && c->hH->step < c->hH->stop_step)
+          remaining = std::max(remaining, c->hH->stop_step - c->hH->step);
+      if (remaining == 0) break;
+      if (b->dirty || !b->graph) rebuild_batch(b);
+      const uint32_t reps = (remaining + kBatchGraphSteps - 1) / kBatchGraphSteps;
+      for (uint32_t r = 0; r < reps; ++r) {
+        CK(cudaGraphLaunch(b->graph, b->stream));
+        launches += (int64_t)b->launches_per_step * kBatchGraphSteps;
+      }
+      read_batch_headers(b);
+      bool regrown = false;
+      for (mtr_ctx* c : b->members) {
+        StepHeader& H = *c->hH;
+        if (!H.abort) continue;
+        uint32_t want[3];
+        for (int a = 0; a < 3; ++a)
+          want[a] = (a < c->dim) ? std::max<uint32_t>(c->cap_axis[a], (uint32_t)std::ceil(H.N[a] * 1.25 + 8.0)) : 1u;
+        for (int a = 0; a < c->dim; ++a)
+          if (H.N[a] >= kMaxAxisNodes || H.N[a] < 4)
+            throw MtrError{MTR_ERR_OOM, "grid extent exploded or collapsed (non-finite particle positions?)"};
+        free_graphs(c);
+        alloc_grid(c, want);
+        CK(cudaStreamSynchronize(c->stream));
+        H.abort = 0;
+        H.status &= ~MTR_STATUS_GRID_OVERFLOW;
+        regrown = true;
+      }
+      if (regrown) {
+        write_batch_headers(b);
+        b->dirty = true;
+      }
+    }
+    for (mtr_ctx* c : b->members) {
+      c->hH->stop_step = 0xffffffffu;
+      c->host_parity = c->hH->cur;
+    }
+    write_batch_headers(b);
+    b->launches_last = launches;
+    return MTR_OK;
+  });
+}
+
+int64_t mtr_batch_launch_count(mtr_batch* b) { return b ? b->launches_last : 0; }
+
+void* mtr_batch_stream(mtr_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+void mtr_batch_destroy(mtr_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  free_batch_tables(b);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
 }
 
 void mtr_ctx_destroy(mtr_ctx* c) {

@@ -45,6 +45,7 @@ struct StepHeader {
   int32_t cur;  // particle buffer (0/1) holding the state after the last completed step
   uint32_t status, first_bad;
   uint32_t stop_frame;  // steps are skipped once frame >= stop_frame (frame-by-frame runs)
+  uint32_t stop_step;   // steps are skipped once step >= stop_step (batched runs)
   double gravity[3];
   double org[3];        // grid.xc, grid.yc, grid.zc
   uint32_t N[3];        // Nx, Ny, Nz (Nz = 1 in 2D)

@@ -75,6 +75,9 @@ struct StepCommon {
   int sort_blocks;
   uint32_t* tile_begin;
   uint32_t* tile_end;
+  const uint32_t* skeys;  // sorted keys and permutation after the last radix pass
+  const uint32_t* perm;
+  int out_parity;         // particle buffer this step writes
 };
 
 template <typename R>
@@ -111,7 +114,7 @@ struct Tiling {
 constexpr size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
 
 __device__ __forceinline__ bool step_inactive(const StepHeader* H) {
-  return H->done || H->abort || H->frame >= H->stop_frame;
+  return H->done || H->abort || H->frame >= H->stop_frame || H->step >= H->stop_step;
 }
 
 __device__ __forceinline__ uint32_t node_index(const StepHeader* H, int i, int j, int k) {
@@ -149,10 +152,10 @@ __device__ __forceinline__ void block_count(unsigned n, unsigned long long* dst)
 // 1. bbox / vmax / sum v partials
 // ---------------------------------------------------------------------------
 template <int D, typename R>
-__global__ void __launch_bounds__(256) k_bbox(StepArgsT<R> A) {
+__device__ __forceinline__ void bbox_body(const StepArgsT<R>& A, const uint32_t bid, const uint32_t nblk) {
   if (step_inactive(A.H)) return;
   double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300}, v2 = 0.0, vs[3] = {0.0, 0.0, 0.0};
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < A.Np; i += gridDim.x * blockDim.x) {
+  for (uint32_t i = bid * blockDim.x + threadIdx.x; i < A.Np; i += nblk * blockDim.x) {
     double vv[3];
 #pragma unroll
     for (int a = 0; a < D; ++a) {
@@ -199,15 +202,20 @@ __global__ void __launch_bounds__(256) k_bbox(StepArgsT<R> A) {
       }
       r.v2 = fmax(r.v2, wp[w].v2);
     }
-    A.partials[blockIdx.x] = r;
+    A.partials[bid] = r;
   }
+}
+
+template <int D, typename R>
+__global__ void __launch_bounds__(256) k_bbox(StepArgsT<R> A) {
+  bbox_body<D, R>(A, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------------------
 // 2. step header: dt (update_dt.cpp:5-66) and grid (remesh.cpp:38-311)
 // ---------------------------------------------------------------------------
 template <int D>
-__global__ void __launch_bounds__(32) k_header(StepCommon A) {
+__device__ __forceinline__ void header_body(const StepCommon& A) {
   StepHeader* H = A.H;
   const DevParams& P = *A.P;
   if (step_inactive(H)) return;
@@ -346,6 +354,11 @@ __global__ void __launch_bounds__(32) k_header(StepCommon A) {
   }
 }
 
+template <int D>
+__global__ void __launch_bounds__(32) k_header(StepCommon A) {
+  header_body<D>(A);
+}
+
 // ---------------------------------------------------------------------------
 // 3. stable LSD radix sort of (blocked cell key, input position)
 // ---------------------------------------------------------------------------
@@ -368,13 +381,13 @@ __device__ __forceinline__ uint32_t cell_key(const StepHeader* H, double ioh, co
 
 // Per-block digit histogram.  The first pass computes the keys from x.
 template <int D, bool FIRST>
-__global__ void __launch_bounds__(kSortThreads) k_sort_hist(StepCommon A, const uint32_t* __restrict__ keys,
-                                                            int shift) {
+__device__ __forceinline__ void sort_hist_body(const StepCommon& A, const uint32_t* __restrict__ keys,
+                                                            int shift, const uint32_t bid, const uint32_t nblk) {
   if (step_inactive(A.H)) return;
   __shared__ uint32_t h[256];
   h[threadIdx.x] = 0;
   __syncthreads();
-  const uint32_t base = blockIdx.x * kSortTile;
+  const uint32_t base = bid * kSortTile;
   const double ioh = A.P->one_over_dx;
 #pragma unroll
   for (int r = 0; r < kSortItems; ++r) {
@@ -394,13 +407,19 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_hist(StepCommon A, const 
     }
   }
   __syncthreads();
-  A.hist[threadIdx.x * A.sort_blocks + blockIdx.x] = h[threadIdx.x];
+  A.hist[threadIdx.x * A.sort_blocks + bid] = h[threadIdx.x];
+}
+
+template <int D, bool FIRST>
+__global__ void __launch_bounds__(kSortThreads) k_sort_hist(StepCommon A, const uint32_t* __restrict__ keys,
+                                                            int shift) {
+  sort_hist_body<D, FIRST>(A, keys, shift, blockIdx.x, gridDim.x);
 }
 
 // Exclusive scan of each digit's row over the blocks; row totals to dtot.
-static __global__ void __launch_bounds__(256) k_sort_scan(StepCommon A) {
+static __device__ __forceinline__ void sort_scan_body(const StepCommon& A, const uint32_t bid, const uint32_t nblk) {
   if (step_inactive(A.H)) return;
-  const int dgt = blockIdx.x;
+  const int dgt = bid;
   uint32_t* row = A.hist + (size_t)dgt * A.sort_blocks;
   __shared__ uint32_t ws[8];
   __shared__ uint32_t carry;
@@ -430,12 +449,16 @@ static __global__ void __launch_bounds__(256) k_sort_scan(StepCommon A) {
   if (threadIdx.x == 0) A.dtot[dgt] = carry;
 }
 
+static __global__ void __launch_bounds__(256) k_sort_scan(StepCommon A) {
+  sort_scan_body(A, blockIdx.x, gridDim.x);
+}
+
 // Stable scatter.  Elements are ranked round by round (256 at a time, in
 // index order) with warp match + per-warp digit counts, which keeps equal
 // digits in input order.
-static __global__ void __launch_bounds__(kSortThreads) k_sort_scatter(StepCommon A, const uint32_t* __restrict__ ksrc,
+static __device__ __forceinline__ void sort_scatter_body(const StepCommon& A, const uint32_t* __restrict__ ksrc,
                                                                const uint32_t* __restrict__ vsrc, uint32_t* kdst,
-                                                               uint32_t* vdst, int shift) {
+                                                               uint32_t* vdst, int shift, const uint32_t bid, const uint32_t nblk) {
   if (step_inactive(A.H)) return;
   __shared__ uint32_t goff[256];
   __shared__ uint32_t run[256];
@@ -454,10 +477,10 @@ static __global__ void __launch_bounds__(kSortThreads) k_sort_scatter(StepCommon
     __syncthreads();
     uint32_t wpre = 0;
     for (int w = 0; w < warp; ++w) wpre += ws[w];
-    goff[tid] = wpre + incl - v + A.hist[(size_t)tid * A.sort_blocks + blockIdx.x];
+    goff[tid] = wpre + incl - v + A.hist[(size_t)tid * A.sort_blocks + bid];
     run[tid] = 0;
   }
-  const uint32_t base = blockIdx.x * kSortTile;
+  const uint32_t base = bid * kSortTile;
   const unsigned lt_mask = (1u << lane) - 1u;
   for (int r = 0; r < kSortItems; ++r) {
 #pragma unroll
@@ -495,17 +518,27 @@ static __global__ void __launch_bounds__(kSortThreads) k_sort_scatter(StepCommon
   }
 }
 
+static __global__ void __launch_bounds__(kSortThreads) k_sort_scatter(StepCommon A, const uint32_t* __restrict__ ksrc,
+                                                               const uint32_t* __restrict__ vsrc, uint32_t* kdst,
+                                                               uint32_t* vdst, int shift) {
+  sort_scatter_body(A, ksrc, vsrc, kdst, vdst, shift, blockIdx.x, gridDim.x);
+}
+
 // ---------------------------------------------------------------------------
 // 4. tile ranges over the sorted keys
 // ---------------------------------------------------------------------------
-static __global__ void __launch_bounds__(256) k_tile_ranges(StepCommon A, const uint32_t* __restrict__ skeys) {
+static __device__ __forceinline__ void tile_ranges_body(const StepCommon& A, const uint32_t* __restrict__ skeys, const uint32_t bid, const uint32_t nblk) {
   if (step_inactive(A.H)) return;
-  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < A.Np; s += gridDim.x * blockDim.x) {
+  for (uint32_t s = bid * blockDim.x + threadIdx.x; s < A.Np; s += nblk * blockDim.x) {
     const uint32_t t = skeys[s] >> 6;
     if (t >= A.cap_tiles) continue;
     if (s == 0 || (skeys[s - 1] >> 6) != t) A.tile_begin[t] = s;
     if (s == A.Np - 1 || (skeys[s + 1] >> 6) != t) A.tile_end[t] = s + 1;
   }
+}
+
+static __global__ void __launch_bounds__(256) k_tile_ranges(StepCommon A, const uint32_t* __restrict__ skeys) {
+  tile_ranges_body(A, skeys, blockIdx.x, gridDim.x);
 }
 
 template <int D>
@@ -648,13 +681,13 @@ constexpr size_t p2g_smem_bytes() {
 }
 
 template <int D, int DEG, typename R>
-__global__ void __launch_bounds__(kChunk) k_p2g_w(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
+__device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t* __restrict__ perm, const uint32_t bid, const uint32_t nblk) {
   using TL = Tiling<D>;
   constexpr int PN = TL::PN, NODES = TL::NODES, NCH = TL::NCH, TB = TL::TB;
   constexpr int NS = Sym<D>::n;
   const StepHeader* H = A.H;
   if (step_inactive(H)) return;
-  const uint32_t t = blockIdx.x;
+  const uint32_t t = bid;
   if (t >= H->ntiles) return;
   const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
   if (pb >= pe) return;
@@ -835,11 +868,16 @@ __global__ void __launch_bounds__(kChunk) k_p2g_w(StepArgsT<R> A, const uint32_t
   }
 }
 
+template <int D, int DEG, typename R>
+__global__ void __launch_bounds__(kChunk) k_p2g_w(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
+  p2g_w_body<D, DEG, R>(A, perm, blockIdx.x, gridDim.x);
+}
+
 // ---------------------------------------------------------------------------
 // 6. grid update, one thread per node (arithmetic in FP64 on both paths)
 // ---------------------------------------------------------------------------
 template <int D, typename R>
-__global__ void __launch_bounds__(256) k_grid(StepArgsT<R> A) {
+__device__ __forceinline__ void grid_body(const StepArgsT<R>& A, const uint32_t bid, const uint32_t nblk) {
   StepHeader* H = A.H;
   if (step_inactive(H)) return;
   const DevParams& P = *A.P;
@@ -853,7 +891,7 @@ __global__ void __launch_bounds__(256) k_grid(StepArgsT<R> A) {
   for (int i = threadIdx.x; i < P.nplates; i += blockDim.x) plates[i] = H->plates[i];
   __syncthreads();
   double sum_m = 0.0, sum_p[3] = {0.0, 0.0, 0.0};  // mass and momentum balance (simulation.cpp:292-333)
-  for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < G; l += gridDim.x * blockDim.x) {
+  for (uint32_t l = bid * blockDim.x + threadIdx.x; l < G; l += nblk * blockDim.x) {
     const double mraw = A.acc[l];
     double v[3] = {0, 0, 0}, vold[3] = {0, 0, 0};
     double fric = 0.0;
@@ -897,6 +935,11 @@ __global__ void __launch_bounds__(256) k_grid(StepArgsT<R> A) {
   block_add(sum_m * P.particle_mass, &H->grid_mass);
 #pragma unroll
   for (int a = 0; a < D; ++a) block_add(sum_p[a] * P.particle_mass, &H->grid_mom[a]);
+}
+
+template <int D, typename R>
+__global__ void __launch_bounds__(256) k_grid(StepArgsT<R> A) {
+  grid_body<D, R>(A, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1141,12 +1184,12 @@ __device__ __forceinline__ void gather_patch(const R* pv, const R* pf, const dou
 // block per tile, node patch in shared memory.
 // ---------------------------------------------------------------------------
 template <int D, int DEG, typename R>
-__global__ void __launch_bounds__(kChunk, MTR_G2P_MIN_BLOCKS) k_g2p_t(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
+__device__ __forceinline__ void g2p_t_body(const StepArgsT<R>& A, const uint32_t* __restrict__ perm, const uint32_t bid, const uint32_t nblk) {
   using TL = Tiling<D>;
   constexpr int PN = TL::PN, NODES = TL::NODES;
   StepHeader* H = A.H;
   if (step_inactive(H)) return;
-  const uint32_t t = blockIdx.x;
+  const uint32_t t = bid;
   if (t >= H->ntiles) return;
   const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
   if (pb >= pe) return;
@@ -1221,6 +1264,11 @@ __global__ void __launch_bounds__(kChunk, MTR_G2P_MIN_BLOCKS) k_g2p_t(StepArgsT<
   block_count(nplastic, &H->plastic_count);
 }
 
+template <int D, int DEG, typename R>
+__global__ void __launch_bounds__(kChunk, MTR_G2P_MIN_BLOCKS) k_g2p_t(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
+  g2p_t_body<D, DEG, R>(A, perm, blockIdx.x, gridDim.x);
+}
+
 // ---------------------------------------------------------------------------
 // 7b. MUSL (musl.cpp:6-96), one block per tile.  Phase 1 (thread per
 // particle): gather pic/B/flip from the shared node patch, blend v, write
@@ -1265,12 +1313,12 @@ constexpr size_t musl_smem_bytes() {
 }
 
 template <int D, int DEG, typename R>
-__global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
+__device__ __forceinline__ void g2p_musl_w_body(const StepArgsT<R>& A, const uint32_t* __restrict__ perm, const uint32_t bid, const uint32_t nblk) {
   using TL = Tiling<D>;
   constexpr int PN = TL::PN, NODES = TL::NODES;
   StepHeader* H = A.H;
   if (step_inactive(H)) return;
-  const uint32_t t = blockIdx.x;
+  const uint32_t t = bid;
   if (t >= H->ntiles) return;
   const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
   if (pb >= pe) return;
@@ -1445,14 +1493,19 @@ __global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgsT<R> A, const uin
   }
 }
 
+template <int D, int DEG, typename R>
+__global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
+  g2p_musl_w_body<D, DEG, R>(A, perm, blockIdx.x, gridDim.x);
+}
+
 // musl.cpp:80-95: v2 /= (m_i / m_p) (zero where m_i == 0)
 template <int D, typename R>
-__global__ void __launch_bounds__(256) k_musl_norm(StepArgsT<R> A) {
+__device__ __forceinline__ void musl_norm_body(const StepArgsT<R>& A, const uint32_t bid, const uint32_t nblk) {
   StepHeader* H = A.H;
   if (step_inactive(H)) return;
   const uint32_t G = H->G, cap = A.cap_nodes;
   const double mp = A.P->particle_mass;
-  for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < G; l += gridDim.x * blockDim.x) {
+  for (uint32_t l = bid * blockDim.x + threadIdx.x; l < G; l += nblk * blockDim.x) {
     const double mi = A.nmass[l];
 #pragma unroll
     for (int a = 0; a < D; ++a) {
@@ -1462,15 +1515,20 @@ __global__ void __launch_bounds__(256) k_musl_norm(StepArgsT<R> A) {
   }
 }
 
+template <int D, typename R>
+__global__ void __launch_bounds__(256) k_musl_norm(StepArgsT<R> A) {
+  musl_norm_body<D, R>(A, blockIdx.x, gridDim.x);
+}
+
 // MUSL: deformation update from the normalised re-projected velocity v2 and
 // the old positions (deformation_update.cpp:6), then the return mapping.
 template <int D, int DEG, typename R>
-__global__ void __launch_bounds__(kChunk, MTR_DEFGRAD_MIN_BLOCKS) k_defgrad_t(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
+__device__ __forceinline__ void defgrad_t_body(const StepArgsT<R>& A, const uint32_t* __restrict__ perm, const uint32_t bid, const uint32_t nblk) {
   using TL = Tiling<D>;
   constexpr int PN = TL::PN, NODES = TL::NODES;
   StepHeader* H = A.H;
   if (step_inactive(H)) return;
-  const uint32_t t = blockIdx.x;
+  const uint32_t t = bid;
   if (t >= H->ntiles) return;
   const uint32_t pb = A.tile_begin[t], pe = A.tile_end[t];
   if (pb >= pe) return;
@@ -1510,11 +1568,16 @@ __global__ void __launch_bounds__(kChunk, MTR_DEFGRAD_MIN_BLOCKS) k_defgrad_t(St
   block_count(nplastic, &H->plastic_count);
 }
 
+template <int D, int DEG, typename R>
+__global__ void __launch_bounds__(kChunk, MTR_DEFGRAD_MIN_BLOCKS) k_defgrad_t(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
+  defgrad_t_body<D, DEG, R>(A, perm, blockIdx.x, gridDim.x);
+}
+
 // ---------------------------------------------------------------------------
 // 8. end of step: moveObjects and the clock of simulate()
 // ---------------------------------------------------------------------------
 template <int D>
-__global__ void k_tail(StepCommon A, int out_parity) {
+__device__ __forceinline__ void tail_body(const StepCommon& A, int out_parity) {
   StepHeader* H = A.H;
   if (step_inactive(H)) return;
   const DevParams& P = *A.P;
@@ -1546,6 +1609,170 @@ __global__ void k_tail(StepCommon A, int out_parity) {
   H->step += 1;
   if (__dsub_rn(__dmul_rn(P.frame_dt, (double)(H->frame + 1)), H->time) < 1e-15) H->frame += 1;
   if (fabs(__dsub_rn(P.final_time, H->time)) < 1e-15 || P.final_time < H->time || !(H->frame < P.end_frame)) H->done = 1;
+}
+
+template <int D>
+__global__ void k_tail(StepCommon A, int out_parity) {
+  tail_body<D>(A, out_parity);
+}
+
+// ---------------------------------------------------------------------------
+// 9. batched steps: the scenes of one group (same dim, spline, precision and
+// USL/MUSL) advance together, one launch per phase for all of them.  Each
+// launch's blocks are laid out scene after scene; a block finds its scene in
+// a per-launch-kind offset table and runs the same body as the single-scene
+// kernel on that scene's arguments.  Both particle-buffer parities of every
+// scene are in the table and the block picks the one its scene's header
+// names, so one captured graph stays valid while scenes advance, stop or
+// regrow independently.
+// ---------------------------------------------------------------------------
+enum BatchKind { kBK_BBOX = 0, kBK_SORT, kBK_SCAN, kBK_TILES, kBK_CLEAR, kBK_TILEK, kBK_NODES, kBK_ONE, kBK_KINDS };
+
+template <typename R>
+struct BatchView {
+  const StepArgsT<R>* args;  // [2][n]: args[c * n + s] = scene s reading particle buffer c
+  const uint32_t* off;       // [kBK_KINDS][n + 1]: first block of each scene, per launch kind
+  int n;
+};
+
+// arguments of this block's scene, its block index b within the scene and the
+// scene's block count nb; null past the last scene
+template <typename R>
+__device__ __forceinline__ const StepArgsT<R>* batch_locate(const BatchView<R>& B, int kind, uint32_t& b,
+                                                            uint32_t& nb) {
+  const uint32_t* o = B.off + (size_t)kind * (B.n + 1);
+  const uint32_t g = blockIdx.x;
+  if (g >= o[B.n]) return nullptr;
+  int lo = 0, hi = B.n - 1;  // last scene whose first block is <= g
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (o[mid] <= g)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  b = g - o[lo];
+  nb = o[lo + 1] - o[lo];
+  const int cur = B.args[lo].H->cur;
+  return B.args + (size_t)(cur & 1) * B.n + lo;
+}
+
+template <int D, typename R>
+__global__ void __launch_bounds__(256) kb_bbox(BatchView<R> B) {
+  uint32_t b, nb;
+  const StepArgsT<R>* A = batch_locate(B, kBK_BBOX, b, nb);
+  if (A) bbox_body<D, R>(*A, b, nb);
+}
+
+template <int D, typename R>
+__global__ void __launch_bounds__(32) kb_header(BatchView<R> B) {
+  uint32_t b, nb;
+  const StepArgsT<R>* A = batch_locate(B, kBK_ONE, b, nb);
+  if (A) header_body<D>(*A);
+}
+
+// zeroes the tile ranges and (MUSL) the re-projection accumulator of an
+// active scene (the single-scene step does this with memsets)
+template <int D, typename R>
+__global__ void __launch_bounds__(256) kb_clear(BatchView<R> B) {
+  uint32_t b, nb;
+  const StepArgsT<R>* A = batch_locate(B, kBK_CLEAR, b, nb);
+  if (!A || step_inactive(A->H)) return;
+  const uint32_t stride = nb * blockDim.x;
+  for (uint32_t i = b * blockDim.x + threadIdx.x; i < A->cap_tiles; i += stride) {
+    A->tile_begin[i] = 0u;
+    A->tile_end[i] = 0u;
+  }
+  if (A->P->use_musl) {
+    const size_t n = (size_t)D * A->cap_nodes;
+    for (size_t i = b * blockDim.x + threadIdx.x; i < n; i += stride) A->v2[i] = 0.0;
+  }
+}
+
+template <int D, typename R>
+__global__ void __launch_bounds__(kSortThreads) kb_sort_hist(BatchView<R> B, int pass) {
+  uint32_t b, nb;
+  const StepArgsT<R>* A = batch_locate(B, kBK_SORT, b, nb);
+  if (!A) return;
+  if (pass == 0)
+    sort_hist_body<D, true>(*A, nullptr, 0, b, nb);
+  else
+    sort_hist_body<D, false>(*A, (pass & 1) ? A->keysB : A->keysA, 8 * pass, b, nb);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) kb_sort_scan(BatchView<R> B) {
+  uint32_t b, nb;
+  const StepArgsT<R>* A = batch_locate(B, kBK_SCAN, b, nb);
+  if (A) sort_scan_body(*A, b, nb);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kSortThreads) kb_sort_scatter(BatchView<R> B, int pass) {
+  uint32_t b, nb;
+  const StepArgsT<R>* A = batch_locate(B, kBK_SORT, b, nb);
+  if (!A) return;
+  const uint32_t* ksrc = pass == 0 ? A->keys0 : ((pass & 1) ? A->keysB : A->keysA);
+  const uint32_t* vsrc = pass == 0 ? nullptr : ((pass & 1) ? A->valsB : A->valsA);
+  uint32_t* kdst = (pass & 1) ? A->keysA : A->keysB;
+  uint32_t* vdst = (pass & 1) ? A->valsA : A->valsB;
+  sort_scatter_body(*A, ksrc, vsrc, kdst, vdst, 8 * pass, b, nb);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) kb_tile_ranges(BatchView<R> B) {
+  uint32_t b, nb;
+  const StepArgsT<R>* A = batch_locate(B, kBK_TILES, b, nb);
+  if (A) tile_ranges_body(*A, A->skeys, b, nb);
+}
+
+template <int D, int DEG, typename R>
+__global__ void __launch_bounds__(kChunk) kb_p2g_w(BatchView<R> B) {
+  uint32_t b, nb;
+  const StepArgsT<R>* A = batch_locate(B, kBK_TILEK, b, nb);
+  if (A) p2g_w_body<D, DEG, R>(*A, A->perm, b, nb);
+}
+
+template <int D, typename R>
+__global__ void __launch_bounds__(256) kb_grid(BatchView<R> B) {
+  uint32_t b, nb;
+  const StepArgsT<R>* A = batch_locate(B, kBK_NODES, b, nb);
+  if (A) grid_body<D, R>(*A, b, nb);
+}
+
+template <int D, int DEG, typename R>
+__global__ void __launch_bounds__(kChunk, MTR_G2P_MIN_BLOCKS) kb_g2p_t(BatchView<R> B) {
+  uint32_t b, nb;
+  const StepArgsT<R>* A = batch_locate(B, kBK_TILEK, b, nb);
+  if (A) g2p_t_body<D, DEG, R>(*A, A->perm, b, nb);
+}
+
+template <int D, int DEG, typename R>
+__global__ void __launch_bounds__(kChunk) kb_g2p_musl_w(BatchView<R> B) {
+  uint32_t b, nb;
+  const StepArgsT<R>* A = batch_locate(B, kBK_TILEK, b, nb);
+  if (A) g2p_musl_w_body<D, DEG, R>(*A, A->perm, b, nb);
+}
+
+template <int D, typename R>
+__global__ void __launch_bounds__(256) kb_musl_norm(BatchView<R> B) {
+  uint32_t b, nb;
+  const StepArgsT<R>* A = batch_locate(B, kBK_NODES, b, nb);
+  if (A) musl_norm_body<D, R>(*A, b, nb);
+}
+
+template <int D, int DEG, typename R>
+__global__ void __launch_bounds__(kChunk, MTR_DEFGRAD_MIN_BLOCKS) kb_defgrad_t(BatchView<R> B) {
+  uint32_t b, nb;
+  const StepArgsT<R>* A = batch_locate(B, kBK_TILEK, b, nb);
+  if (A) defgrad_t_body<D, DEG, R>(*A, A->perm, b, nb);
+}
+
+template <int D, typename R>
+__global__ void __launch_bounds__(32) kb_tail(BatchView<R> B) {
+  uint32_t b, nb;
+  const StepArgsT<R>* A = batch_locate(B, kBK_ONE, b, nb);
+  if (A) tail_body<D>(*A, A->out_parity);
 }
 
 // ---------------------------------------------------------------------------

@@ -239,6 +239,8 @@ __global__ void k_noalloc_setup(StepHeader* H, DevParams* P, const double* gx, c
   H->abort = 0;
   H->frame = 0;
   H->stop_frame = 0xffffffffu;
+  H->step = 0;
+  H->stop_step = 0xffffffffu;
   H->status = 0;
   H->first_bad = 0xffffffffu;
   H->org[0] = gx[0];

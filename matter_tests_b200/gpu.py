@@ -21,8 +21,9 @@ EXPORTS = (
     "mtr_ctx_create", "mtr_upload", "mtr_set_objects", "mtr_step", "mtr_run", "mtr_run_frame", "mtr_download",
     "mtr_download_pic_flip", "mtr_get_grid", "mtr_get_sort", "mtr_get_plates", "mtr_get_clock",
     "mtr_status", "mtr_clear_status", "mtr_sync", "mtr_stream", "mtr_launch_count", "mtr_keep_pic_flip",
-    "mtr_use_graphs", "mtr_profile", "mtr_active_nodes", "mtr_balance", "mtr_ctx_destroy", "mtr_last_error",
-    "mtr_p2g_noalloc",
+    "mtr_use_graphs", "mtr_profile", "mtr_active_nodes", "mtr_balance", "mtr_batch_create", "mtr_batch_step",
+    "mtr_batch_launch_count", "mtr_batch_stream", "mtr_batch_destroy", "mtr_footprint", "mtr_ctx_destroy",
+    "mtr_last_error", "mtr_p2g_noalloc",
 )
 
 _lib = None
@@ -66,6 +67,15 @@ def load_library(path=LIB_PATH):
     lib.mtr_profile.argtypes = [C.c_void_p, C.c_int, _P, C.POINTER(C.c_char_p), C.c_int, C.POINTER(C.c_int)]
     lib.mtr_active_nodes.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     lib.mtr_balance.argtypes = [C.c_void_p, _P, _P, _P, _P]
+    lib.mtr_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]
+    lib.mtr_batch_step.argtypes = [C.c_void_p, C.c_int]
+    lib.mtr_batch_launch_count.argtypes = [C.c_void_p]
+    lib.mtr_batch_launch_count.restype = C.c_int64
+    lib.mtr_batch_stream.argtypes = [C.c_void_p]
+    lib.mtr_batch_stream.restype = C.c_void_p
+    lib.mtr_batch_destroy.argtypes = [C.c_void_p]
+    lib.mtr_batch_destroy.restype = None
+    lib.mtr_footprint.argtypes = [C.POINTER(MtrParams), C.c_uint32, _P, C.POINTER(C.c_uint64)]
     lib.mtr_p2g_noalloc.argtypes = [C.POINTER(MtrParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                     C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32), C.c_void_p,
                                     C.c_void_p, C.c_void_p]
@@ -242,3 +252,45 @@ class GpuSim:
 
 def scalars_dict(sc):
     return {k: sc[:, i] for i, k in enumerate(SCALARS)}
+
+
+class GpuBatch:
+    """Several GpuSim contexts on one GPU stepped together (mtr_batch)."""
+
+    def __init__(self, sims):
+        self.lib = load_library()
+        self.sims = list(sims)
+        arr = (C.c_void_p * len(self.sims))(*[s.h.value if isinstance(s.h, C.c_void_p) else s.h for s in self.sims])
+        h = C.c_void_p()
+        _check(self.lib, "mtr_batch_create", self.lib.mtr_batch_create(arr, len(self.sims), C.byref(h)))
+        self.h = h
+
+    def step(self, n=1):
+        _check(self.lib, "mtr_batch_step", self.lib.mtr_batch_step(self.h, n))
+
+    @property
+    def stream(self):
+        return self.lib.mtr_batch_stream(self.h)
+
+    def launch_count(self):
+        return self.lib.mtr_batch_launch_count(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mtr_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def footprint(params, x):
+    """Device bytes mtr_upload allocates for particles at x (mtr_footprint)."""
+    lib = load_library()
+    x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+    out = C.c_uint64()
+    _check(lib, "mtr_footprint", lib.mtr_footprint(C.byref(params), x.size // params.dim, _ptr(x), C.byref(out)))
+    return out.value
