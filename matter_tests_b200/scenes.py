@@ -176,6 +176,94 @@ def incline3d_mcc(scale=1.0, seed=99, theta_deg=30.0):
     return _finish(sc, dx, 8, 1000.0)
 
 
+def granular_scene(rng, dim, kind, n_target, material, E, phi_deg=30.0, aspect=2.0):
+    """One seeded scene of the ensemble and serving workloads: a column
+    collapse on a SlipFree floor (mu 0.5) or a release block on a 30 deg
+    incline with two Gaussian bumps (SlipFree, mu 0.45); n_target particles
+    (2 x 2 (x 2) jittered per cell, the cell size chosen to match), material
+    "dp" (M = tan phi), "mcc" (Perzyna Cam-Clay, M 1.2, p0 1e4 Pa, 1e-3 s) or
+    "mui" (mu(I): mu_1 0.38, mu_2 0.64); APIC USL, quadratic splines."""
+    ppc = 4 if dim == 2 else 8
+    cells = max(8.0, n_target / ppc)
+    W = 0.2
+    if kind == "collapse":
+        nw = max(2, int(round((cells / aspect) ** (1.0 / dim))))
+        nh = max(2, int(round(aspect * nw)))
+        dx = W / nw
+        hi = [nw * dx, nh * dx] + ([nw * dx] if dim == 3 else [])
+        lo = [0.0] * dim
+    else:
+        # block 2:1:1 (x, height, z)
+        nh = max(2, int(round((cells / 2.0 ** (dim - 1)) ** (1.0 / dim))))
+        dx = W / nh
+        hi = [2 * nh * dx, nh * dx] + ([nh * dx] if dim == 3 else [])
+        lo = [0.0, 0.5 * dx] + ([0.0] if dim == 3 else [])
+        hi[1] += 0.5 * dx
+    x = lattice(lo, hi, dx, 2, rng)
+    p = default_params(dim, 2)
+    p.flip_ratio = -2.0
+    p.E, p.nu = E, 0.3
+    rho = 1550.0
+    if material == "dp":
+        p.plastic_model = PlasticModel.DP
+        p.M = math.tan(phi_deg * math.pi / 180.0)
+    elif material == "mcc":
+        p.plastic_model = PlasticModel.MCCVisc
+        p.hardening_law = HardeningLaw.ExpoImpl
+        p.M, p.beta, p.p0 = 1.2, 0.0, 1e4
+        p.perzyna_exp, p.perzyna_visc = 1.0, 1e-3
+        rho = 1000.0
+    else:
+        p.plastic_model = PlasticModel.DPMui
+        p.mu_1, p.mu_2, p.I_ref = 0.38, 0.64, 0.279
+        p.grain_diameter, p.rho_s = 1e-3, 2500.0
+        rho = 1500.0
+    p.end_frame, p.fps = 1, 1.0
+    sc = Scene(f"{kind}{dim}d_{material}", p, x)
+    if kind == "collapse":
+        p.gravity[1] = -9.81
+        sc.plates = [make_plate(0.0, PlateType.bottom, BC.SlipFree, 0.5)]
+    else:
+        th = 30.0 * math.pi / 180.0
+        p.gravity[0] = 9.81 * math.sin(th)
+        p.gravity[1] = -9.81 * math.cos(th)
+        L = hi[0]
+        bumps = [0.0, 2.0]
+        for k in range(2):
+            bumps += [L * (1.3 + 0.6 * k) + rng.uniform(0, 0.2 * L), float(rng.uniform(0.2, 0.8)) * (hi[2] if dim == 3
+                      else 0.0), 0.3 * (hi[1] - lo[1]), 0.5 * (hi[1] - lo[1])]
+        sc.objects = [make_object(ObjectKind.TerrainGauss, BC.SlipFree, 0.45, bumps)]
+    return _finish(sc, dx, ppc, rho)
+
+
+def ensemble(n=256, seed=777, n_min=5_000, n_max=300_000):
+    """The batched-ensemble workload: n independent DP column collapses,
+    particle counts log-uniform in [n_min, n_max], 3D with probability 1/2,
+    aspect ratio uniform in [0.5, 4], friction angle uniform in [20, 40] deg,
+    E log-uniform in [1e5, 1e7] Pa (seeded)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        npart = int(math.exp(rng.uniform(math.log(n_min), math.log(n_max))))
+        dim = 3 if rng.uniform() < 0.5 else 2
+        aspect = rng.uniform(0.5, 4.0)
+        phi = rng.uniform(20.0, 40.0)
+        E = math.exp(rng.uniform(math.log(1e5), math.log(1e7)))
+        out.append(granular_scene(rng, dim, "collapse", npart, "dp", E, phi, aspect))
+    return out
+
+
+def serving_request(rng, n_min=10_000, n_max=2_000_000):
+    """One request of the serving workload: 2D or 3D, collapse or incline,
+    particle count log-uniform in [n_min, n_max], material DP, MCC or mu(I)."""
+    npart = int(math.exp(rng.uniform(math.log(n_min), math.log(n_max))))
+    dim = 3 if rng.uniform() < 0.5 else 2
+    kind = "collapse" if rng.uniform() < 0.5 else "incline"
+    material = ("dp", "mcc", "mui")[int(rng.integers(0, 3))]
+    E = math.exp(rng.uniform(math.log(1e5), math.log(1e7)))
+    return granular_scene(rng, dim, kind, npart, material, E, rng.uniform(20.0, 40.0), rng.uniform(0.5, 4.0))
+
+
 WORKLOADS = {
     "collapse2d": collapse2d,
     "collapse3d_mui": collapse3d_mui,
