@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--ensemble-size", type=int, default=256, help="scenes of the batched ensemble")
     ap.add_argument("--ensemble-steps", type=int, default=500, help="timed steps of the batched ensemble")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
+    ap.add_argument("--serve-requests", type=int, default=60, help="requests of the serving measurement")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
     return ap.parse_args()
 
 
@@ -503,6 +505,53 @@ def ensemble_measure(args, local):
             "all_scenes_advanced": bool(min(steps_done) >= W + K)}
 
 
+def serve_measure(args, local):
+    """The serving loop: args.serve_requests seeded requests (2D/3D, collapse
+    or incline, 10k-2M particles, DP / Cam-Clay / mu(I), 200 steps each)
+    arriving as a Poisson process at 20 per second, admitted within a 150 GB
+    device-memory budget, mixed precision, stepped together in ticks of 8.
+    Against it: the same requests one after another through the plain FP64
+    single-scene path and the mixed single-scene path (device-timed steps)."""
+    import copy
+    import torch
+    from matter_tests_b200.abi import PREC_FP64, PREC_MIXED
+    from matter_tests_b200.gpu import GpuSim
+    from matter_tests_b200.serve import Server, poisson_requests
+    reqs = poisson_requests(args.serve_requests, rate=20.0, seed=4242, steps=200)
+    srv = Server(budget_bytes=150e9, device=local, tick_steps=8, precision=PREC_MIXED)
+    done = srv.run(reqs)
+    rep = srv.report(done)
+    serial = {}
+    for prec, name in ((PREC_FP64, "fp64"), (PREC_MIXED, "mixed")):
+        ms, ps = 0.0, 0
+        for r in reqs:
+            p = copy.copy(r.scene.params)
+            p.precision = prec
+            g = GpuSim(p, device=local)
+            sc = r.scene
+            g.upload(sc.x, sc.v, sc.F, sc.B, sc.scalars)
+            g.set_objects(sc.plates, sc.objects)
+            st = torch.cuda.ExternalStream(g.stream, device=torch.device("cuda", local))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            g.step(r.steps, check=False)
+            b.record(st)
+            b.synchronize()
+            ms += a.elapsed_time(b)
+            ps += sc.Np * g.clock()["step"]
+            g.close()
+        serial[name] = ps / (ms / 1e3)
+    rep.update({"metric": "served particle-steps/s", "unit": METRIC, "dtype": "f32+f64",
+                "single_scene_fp64": serial["fp64"], "single_scene_mixed": serial["mixed"],
+                "served_over_single_scene_fp64": rep["throughput"] / serial["fp64"],
+                "served_over_single_scene_mixed": rep["throughput"] / serial["mixed"],
+                "config": "Poisson arrivals 20/s (seed 4242), Np log-uniform 10k-2M, 2D/3D collapse or incline, "
+                          "DP/MCC/mu(I), 200 steps, 150 GB budget, ticks of 8 steps",
+                "timed": "throughput = particle-steps of the served requests / (last completion - first "
+                         "arrival), wall clock; single-scene figures are device time of the steps alone"})
+    return rep
+
+
 def gpu_arm(args, world, rank, local):
     import torch
     from matter_tests_b200.abi import PREC_FP64, PREC_MIXED
@@ -525,6 +574,12 @@ def gpu_arm(args, world, rank, local):
             ens = ensemble_measure(args, local)
         except Exception as e:  # reported, not fatal: the headline line still prints
             ens = {"error": f"{type(e).__name__}: {e}"}
+    served = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        try:
+            served = serve_measure(args, local)
+        except Exception as e:  # reported, not fatal: the headline line still prints
+            served = {"error": f"{type(e).__name__}: {e}"}
     clocks = sampler.stop()
     err = mixed_error(sc, st64, st32)
     err["steps"] = args.warmup + args.steps
@@ -547,7 +602,7 @@ def gpu_arm(args, world, rank, local):
                 "fp64": {k: fp64[k] for k in ("value", "ms_per_step", "roofline", "kernel_ms", "e2e",
                                               "gpu_launches", "status_flags")},
                 "mixed_over_fp64": mixed["value"] / fp64["value"],
-                "mixed_error_vs_fp64": err, "ensemble": ens,
+                "mixed_error_vs_fp64": err, "ensemble": ens, "serving": served,
                 "sim_clock": mixed["sim_clock"], "status_flags": mixed["status_flags"]}
         print(json.dumps(line), flush=True)
     return 0

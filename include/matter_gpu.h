@@ -247,6 +247,11 @@ int mtr_balance(mtr_ctx* ctx, double* grid_mass, double* grid_momentum, double* 
  * mtr_footprint estimates the device bytes mtr_upload will allocate for Np
  * particles at positions x (AoS) with these parameters, for admission by
  * memory budget; the grid may later grow with the scene. */
+/* mtr_set_step_limit: the context takes no step past step number last_step
+ * (steps counted from mtr_upload; 0xffffffff = no limit, the default).  Both
+ * mtr_step and mtr_batch_step stop there, so a batch member that needs fewer
+ * steps than the others ends exactly on time. */
+int mtr_set_step_limit(mtr_ctx* ctx, uint32_t last_step);
 int mtr_batch_create(mtr_ctx* const* ctxs, int n, mtr_batch** out);
 int mtr_batch_step(mtr_batch* batch, int nsteps);
 int64_t mtr_batch_launch_count(mtr_batch* batch);

@@ -100,6 +100,7 @@ struct mtr_ctx {
   int64_t launches_last = 0;
   int launches_per_step = 0;
   bool use_graphs = true;
+  uint32_t step_limit = 0xffffffffu;  // mtr_set_step_limit: no step beyond this step count
   // per-launch timing (mtr_profile): an event after every launch of a step
   bool profiling = false;
   std::vector<std::pair<const char*, cudaEvent_t>> marks;
@@ -444,6 +445,7 @@ void derive_constants(mtr_ctx* c) {  // simulation.cpp:94-136
   h.mu_1 = p.mu_1;
   h.mu_2 = p.mu_2;
   h.mui0 = (p.plastic_model == MTR_PM_DPMUI || p.plastic_model == MTR_PM_MCCMUI) ? p.mu_1 : p.M;
+  h.dgamma_tol = p.precision == MTR_PREC_MIXED ? 1e-9 : 0.0;
 }
 
 // The first step's grid extents, as remeshFixedInit(2,2,2) will compute them
@@ -838,6 +840,7 @@ int mtr_upload(mtr_ctx* c, const double* x, const double* v, const double* F, co
     c->hH->first_bad = 0xffffffffu;
     c->hH->stop_frame = 0xffffffffu;
     c->hH->stop_step = 0xffffffffu;
+    c->step_limit = 0xffffffffu;
     for (int a = 0; a < 3; ++a) c->hH->gravity[a] = a < d ? c->prm.gravity[a] : 0.0;
     c->hH->done = (0 < c->prm.end_frame) ? 0 : 1;
     for (size_t i = 0; i < c->plates.size(); ++i) c->hH->plates[i] = c->plates[i];
@@ -899,7 +902,7 @@ int mtr_step(mtr_ctx* c, int nsteps) {
     CK(cudaSetDevice(c->device));
     read_header(c);
     if (c->hH->done) return (c->hH->status & kExitMask) ? MTR_ERR_DEVICE_STATUS : MTR_OK;
-    if (c->hH->frame >= c->hH->stop_frame) return MTR_OK;
+    if (c->hH->frame >= c->hH->stop_frame || c->hH->step >= c->hH->stop_step) return MTR_OK;
     c->host_parity = c->hH->cur;
     int64_t launches = 0;
     int remaining = nsteps;
@@ -939,7 +942,7 @@ int mtr_step(mtr_ctx* c, int nsteps) {
         CK(cudaStreamSynchronize(c->stream));
         continue;
       }
-      if (H.done || H.frame >= H.stop_frame) break;
+      if (H.done || H.frame >= H.stop_frame || H.step >= H.stop_step) break;
     }
     c->launches_last = launches;
     if (c->hH->status & kExitMask) return MTR_ERR_DEVICE_STATUS;
@@ -963,10 +966,11 @@ int mtr_run_frame(mtr_ctx* c, int* frame_done) {
   rc = mtr_get_clock(c, &ck);
   f0 = ck.frame;
   while (rc == MTR_OK) {
+    const uint32_t s0 = ck.step;
     rc = mtr_step(c, 128);
     if (rc != MTR_OK) break;
     rc = mtr_get_clock(c, &ck);
-    if (rc != MTR_OK || ck.done || ck.frame > f0) break;
+    if (rc != MTR_OK || ck.done || ck.frame > f0 || ck.step == s0) break;  // ck.step == s0: step limit reached
   }
   int rc2 = guarded([&]() -> int {
     read_header(c);
@@ -980,14 +984,29 @@ int mtr_run_frame(mtr_ctx* c, int* frame_done) {
 }
 
 int mtr_run(mtr_ctx* c) {
-  for (;;) {
-    int rc = mtr_step(c, 1024);
+  mtr_clock ck{};
+  int rc = mtr_get_clock(c, &ck);
+  while (rc == MTR_OK && !ck.done) {
+    const uint32_t s0 = ck.step;
+    rc = mtr_step(c, 1024);
     if (rc != MTR_OK) return rc;
-    mtr_clock ck;
     rc = mtr_get_clock(c, &ck);
-    if (rc != MTR_OK) return rc;
-    if (ck.done) return MTR_OK;
+    if (rc == MTR_OK && ck.step == s0) break;  // step limit reached
   }
+  return rc;
+}
+
+int mtr_set_step_limit(mtr_ctx* c, uint32_t last_step) {
+  return guarded([&]() -> int {
+    if (!c || !c->uploaded) throw MtrError{MTR_ERR_STATE, "nothing uploaded"};
+    CK(cudaSetDevice(c->device));
+    read_header(c);
+    c->step_limit = last_step;
+    c->hH->stop_step = last_step;
+    write_header(c);
+    CK(cudaStreamSynchronize(c->stream));
+    return MTR_OK;
+  });
 }
 
 int mtr_download(mtr_ctx* c, double* x, double* v, double* F, double* B, double* scalars) {
@@ -1324,7 +1343,8 @@ int mtr_batch_step(mtr_batch* b, int nsteps) {
     read_batch_headers(b);
     for (mtr_ctx* c : b->members) {  // every member advances nsteps steps (or to its end)
       StepHeader& H = *c->hH;
-      H.stop_step = (uint32_t)std::min<uint64_t>((uint64_t)H.step + (uint64_t)nsteps, 0xfffffffeull);
+      H.stop_step = (uint32_t)std::min<uint64_t>(std::min<uint64_t>((uint64_t)H.step + (uint64_t)nsteps, 0xfffffffeull),
+                                                 c->step_limit);
     }
     write_batch_headers(b);
     int64_t launches = 0;
@@ -1364,7 +1384,7 @@ int mtr_batch_step(mtr_batch* b, int nsteps) {
       }
     }
     for (mtr_ctx* c : b->members) {
-      c->hH->stop_step = 0xffffffffu;
+      c->hH->stop_step = c->step_limit;
       c->host_parity = c->hH->cur;
     }
     write_batch_headers(b);

@@ -32,6 +32,11 @@ struct DevParams {
   double E, nu, stress_tolerance, xi, q_max, q_min, p_min, M, q_cohesion, perzyna_exp, perzyna_visc, beta, p0,
       mu_1, mu_2;
   double mui0;  // muI every particle starts from when use_mibf (simulation.cpp:138-145)
+  // a Perzyna plastic multiplier in (-dgamma_tol, 0) is rounding and is taken
+  // as zero rather than reported: 0 on the FP64 path (the reference's checks,
+  // plasticity.cpp:190,286; 1e-14 for Cam-Clay, plasticity.cpp:546-547) and
+  // 1e-9 on the mixed path, whose FP32 strains carry about that much
+  double dgamma_tol;
   mtr_object objects[MTR_MAXO];
 };
 

@@ -426,7 +426,12 @@ __device__ bool return_map(const DevParams& P, double dt, double (&F)[D][D], PSc
       double delta_gamma;
       if (P.perzyna_exp == 1 && P.xi == 0) {
         delta_gamma = (q_trial - q_yield) / (f_mu + q_yield * P.perzyna_visc / dt);
-        if (delta_gamma < 0) flags |= MTR_STATUS_NEG_DGAMMA;
+        if (delta_gamma < 0) {
+          if (delta_gamma > -P.dgamma_tol)
+            delta_gamma = 0;
+          else
+            flags |= MTR_STATUS_NEG_DGAMMA;
+        }
       } else {
         delta_gamma = perzyna_newton(P, dt, q_trial, q_yield, true, s.eps_pl_dev, flags);
       }
@@ -462,7 +467,12 @@ __device__ bool return_map(const DevParams& P, double dt, double (&F)[D][D], PSc
       double delta_gamma;
       if (P.perzyna_exp == 1) {
         delta_gamma = (q_trial - q_yield) / (f_mu + q_yield * P.perzyna_visc / dt);
-        if (delta_gamma < 0) flags |= MTR_STATUS_NEG_DGAMMA;
+        if (delta_gamma < 0) {
+          if (delta_gamma > -P.dgamma_tol)
+            delta_gamma = 0;
+          else
+            flags |= MTR_STATUS_NEG_DGAMMA;
+        }
       } else {
         delta_gamma = perzyna_newton(P, dt, q_trial, q_yield, false, 0.0, flags);
       }
@@ -578,7 +588,7 @@ __device__ bool return_map(const DevParams& P, double dt, double (&F)[D][D], PSc
           if (P.perzyna_exp == 1) {
             delta_gamma = (q_trial - q_yield) / (f_mu + q_yield * P.perzyna_visc / dt);
             if (delta_gamma < 0) {
-              if (delta_gamma > -1e-14)
+              if (delta_gamma > -dmax(1e-14, P.dgamma_tol))
                 delta_gamma = 0;
               else
                 flags |= MTR_STATUS_NEG_DGAMMA;

@@ -21,9 +21,9 @@ EXPORTS = (
     "mtr_ctx_create", "mtr_upload", "mtr_set_objects", "mtr_step", "mtr_run", "mtr_run_frame", "mtr_download",
     "mtr_download_pic_flip", "mtr_get_grid", "mtr_get_sort", "mtr_get_plates", "mtr_get_clock",
     "mtr_status", "mtr_clear_status", "mtr_sync", "mtr_stream", "mtr_launch_count", "mtr_keep_pic_flip",
-    "mtr_use_graphs", "mtr_profile", "mtr_active_nodes", "mtr_balance", "mtr_batch_create", "mtr_batch_step",
-    "mtr_batch_launch_count", "mtr_batch_stream", "mtr_batch_destroy", "mtr_footprint", "mtr_ctx_destroy",
-    "mtr_last_error", "mtr_p2g_noalloc",
+    "mtr_use_graphs", "mtr_profile", "mtr_active_nodes", "mtr_balance", "mtr_set_step_limit",
+    "mtr_batch_create", "mtr_batch_step", "mtr_batch_launch_count", "mtr_batch_stream", "mtr_batch_destroy",
+    "mtr_footprint", "mtr_ctx_destroy", "mtr_last_error", "mtr_p2g_noalloc",
 )
 
 _lib = None
@@ -67,6 +67,7 @@ def load_library(path=LIB_PATH):
     lib.mtr_profile.argtypes = [C.c_void_p, C.c_int, _P, C.POINTER(C.c_char_p), C.c_int, C.POINTER(C.c_int)]
     lib.mtr_active_nodes.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     lib.mtr_balance.argtypes = [C.c_void_p, _P, _P, _P, _P]
+    lib.mtr_set_step_limit.argtypes = [C.c_void_p, C.c_uint32]
     lib.mtr_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]
     lib.mtr_batch_step.argtypes = [C.c_void_p, C.c_int]
     lib.mtr_batch_launch_count.argtypes = [C.c_void_p]
@@ -130,6 +131,10 @@ class GpuSim:
         pa = (MtrPlate * max(1, len(plates)))(*plates)
         oa = (MtrObject * max(1, len(objects)))(*objects)
         _check(self.lib, "mtr_set_objects", self.lib.mtr_set_objects(self.h, pa, len(plates), oa, len(objects)))
+
+    def set_step_limit(self, last_step):
+        """No step past step number last_step (mtr_set_step_limit)."""
+        _check(self.lib, "mtr_set_step_limit", self.lib.mtr_set_step_limit(self.h, int(last_step)))
 
     def keep_pic_flip(self, on=True):
         _check(self.lib, "mtr_keep_pic_flip", self.lib.mtr_keep_pic_flip(self.h, 1 if on else 0))

@@ -1,0 +1,194 @@
+"""Serving loop: scenes arrive as requests, are admitted by their device-memory
+footprint, and every admitted scene advances in one batch (mtr_batch: one
+launch per step phase for all scenes of a group, replayed from a CUDA graph).
+
+Continuous batching: a request that arrives while others run is prepared
+(context created, particles uploaded) on a worker thread while the batch
+keeps stepping, and joins at the next tick; a finished scene leaves at the
+tick it completes, its result is read back and its memory freed on the
+worker, and the memory it frees admits the next waiting request.  A tick
+advances every member by `tick_steps` steps; each member has a step limit,
+so it stops exactly after the steps it asked for.
+
+No counterpart in the reference, which runs one Simulation per process.
+"""
+import collections
+import concurrent.futures as cf
+import copy
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .abi import PREC_MIXED
+from .gpu import GpuBatch, GpuSim, footprint
+
+
+@dataclass
+class Request:
+    rid: int
+    scene: object
+    steps: int
+    arrival: float                 # seconds after the start of the run
+    footprint: int = 0
+    admitted: float = None
+    started: float = None          # first tick it took part in
+    done: float = None
+    result: dict = None
+    sim: object = field(default=None, repr=False)
+
+
+class Server:
+    """Admits requests under `budget_bytes` of device memory and steps all
+    admitted scenes together.  `precision` overrides each scene's precision
+    (None keeps it)."""
+
+    def __init__(self, budget_bytes, device=0, tick_steps=8, precision=PREC_MIXED, keep_result=("x", "v")):
+        self.budget = int(budget_bytes)
+        self.device = device
+        self.tick_steps = int(tick_steps)
+        self.precision = precision
+        self.keep = keep_result
+        self.tick_ms = []        # wall time of each tick
+        self.tick_members = []   # scenes stepped in each tick
+        self.peak_members = 0
+        self.peak_bytes = 0
+
+    # -- worker-thread jobs -------------------------------------------------
+    def _prepare(self, req):
+        sc = req.scene
+        p = copy.copy(sc.params)
+        if self.precision is not None:
+            p.precision = self.precision
+        g = GpuSim(p, device=self.device)
+        g.upload(sc.x, sc.v, sc.F, sc.B, sc.scalars)
+        g.set_objects(sc.plates, sc.objects)
+        g.set_step_limit(req.steps)
+        return g
+
+    def _finish(self, req):
+        st = req.sim.particles()
+        req.result = {k: st[k] for k in self.keep}
+        req.result["clock"] = req.sim.clock()
+        req.result["status"] = req.sim.status()
+        req.sim.close()
+        req.sim = None
+
+    # -- the loop -------------------------------------------------------------
+    def run(self, requests, realtime=True):
+        """Serves `requests` (arrival times relative to the start) and
+        returns them completed.  With realtime=False arrivals are ignored and
+        everything is queued at the start."""
+        queue_in = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        for r in queue_in:
+            if r.footprint == 0:
+                p = copy.copy(r.scene.params)
+                if self.precision is not None:
+                    p.precision = self.precision
+                r.footprint = footprint(p, r.scene.x)
+            if r.footprint > self.budget:
+                raise ValueError(f"request {r.rid} needs {r.footprint} bytes, more than the budget")
+        waiting = collections.deque()
+        preparing = {}      # future -> request
+        finishing = []      # futures
+        active = []
+        used = 0
+        batch = None
+        members_key = None
+        t0 = time.perf_counter()
+        now = lambda: time.perf_counter() - t0
+        done = []
+        with cf.ThreadPoolExecutor(max_workers=1) as pool:
+            while queue_in or waiting or preparing or active:
+                t = now()
+                while queue_in and (not realtime or queue_in[0].arrival <= t):
+                    waiting.append(queue_in.popleft())
+                # admission: first come, first served, within the memory budget
+                while waiting and used + waiting[0].footprint <= self.budget:
+                    r = waiting.popleft()
+                    r.admitted = now()
+                    used += r.footprint
+                    self.peak_bytes = max(self.peak_bytes, used)
+                    preparing[pool.submit(self._prepare, r)] = r
+                for f in [f for f in preparing if f.done()]:
+                    r = preparing.pop(f)
+                    r.sim = f.result()
+                    active.append(r)
+                if not active:
+                    if preparing:
+                        cf.wait(list(preparing), return_when=cf.FIRST_COMPLETED)
+                    elif queue_in:
+                        time.sleep(max(0.0, min(0.05, queue_in[0].arrival - now())))
+                    continue
+                key = tuple(r.rid for r in active)
+                if key != members_key:
+                    if batch is not None:
+                        batch.close()
+                    batch = GpuBatch([r.sim for r in active])
+                    members_key = key
+                ts = now()
+                for r in active:
+                    if r.started is None:
+                        r.started = ts
+                batch.step(self.tick_steps)
+                self.tick_ms.append((now() - ts) * 1e3)
+                self.tick_members.append(len(active))
+                self.peak_members = max(self.peak_members, len(active))
+                still = []
+                for r in active:
+                    ck = r.sim.clock()
+                    if ck["step"] >= r.steps or ck["done"]:
+                        r.done = now()
+                        finishing.append(pool.submit(self._finish, r))
+                        used -= r.footprint
+                        done.append(r)
+                    else:
+                        still.append(r)
+                if len(still) != len(active):
+                    # the members leave the batch before their contexts are freed
+                    batch.close()
+                    batch = None
+                    members_key = None
+                active = still
+            if batch is not None:
+                batch.close()
+            for f in finishing:
+                f.result()
+        self.wall_s = now()
+        return done
+
+    # -- report ---------------------------------------------------------------
+    def report(self, done):
+        lat = np.array([r.done - r.arrival for r in done])
+        wait = np.array([r.admitted - r.arrival for r in done])
+        psteps = sum(r.scene.Np * r.steps for r in done)
+        per_step = np.array(self.tick_ms) / self.tick_steps
+        span = max(r.done for r in done) - min(r.arrival for r in done)
+        return {
+            "requests": len(done),
+            "requests_with_device_status": sum(1 for r in done if r.result and r.result["status"][0]),
+            "particle_steps": psteps,
+            "throughput": psteps / span,
+            "request_latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "queue_wait_s": {"p50": float(np.percentile(wait, 50)), "p99": float(np.percentile(wait, 99))},
+            "step_latency_ms": {"p50": float(np.percentile(per_step, 50)), "p99": float(np.percentile(per_step, 99))},
+            "tick_steps": self.tick_steps,
+            "ticks": len(self.tick_ms),
+            "peak_members": self.peak_members,
+            "mean_members": float(np.mean(self.tick_members)) if self.tick_members else 0.0,
+            "peak_bytes": self.peak_bytes,
+            "budget_bytes": self.budget,
+        }
+
+
+def poisson_requests(n, rate, seed, steps=200, builder=None):
+    """n seeded requests arriving as a Poisson process of `rate` per second."""
+    from . import scenes
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate)
+        sc = (builder or scenes.serving_request)(rng)
+        out.append(Request(rid=i, scene=sc, steps=steps, arrival=t))
+    return out
