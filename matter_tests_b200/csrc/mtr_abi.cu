@@ -267,6 +267,42 @@ StepArgsT<R> make_args(mtr_ctx* c, int parity) {
 
 // Enqueues one step reading buffer `parity` and writing the other.  Returns
 // the number of kernels launched.
+// Plastic models whose return-mapping kernels are also compiled for that
+// model alone (3D; the workloads' models): the model-specific kernel skips
+// the other models' code and stays within the instruction cache.  Any other
+// model runs the generic kernel, which reads the model at run time.
+int rm_specialization(int dim, bool musl, int pm) {
+  if (dim != 3) return -1;
+  if (musl) return pm == MTR_PM_DPMUI ? pm : -1;
+  return (pm == MTR_PM_DP || pm == MTR_PM_MCCVISC) ? pm : -1;
+}
+
+template <int D, int DEG, typename R>
+void launch_defgrad(int spm, uint32_t blocks, cudaStream_t st, const StepArgsT<R>& A, const uint32_t* perm) {
+  if constexpr (D == 3) {
+    if (spm == MTR_PM_DPMUI) {
+      k_defgrad_t<D, DEG, R, MTR_PM_DPMUI><<<blocks, kChunk, 0, st>>>(A, perm);
+      return;
+    }
+  }
+  k_defgrad_t<D, DEG, R><<<blocks, kChunk, 0, st>>>(A, perm);
+}
+
+template <int D, int DEG, typename R>
+void launch_g2p(int spm, uint32_t blocks, cudaStream_t st, const StepArgsT<R>& A, const uint32_t* perm) {
+  if constexpr (D == 3) {
+    if (spm == MTR_PM_DP) {
+      k_g2p_t<D, DEG, R, MTR_PM_DP><<<blocks, kChunk, 0, st>>>(A, perm);
+      return;
+    }
+    if (spm == MTR_PM_MCCVISC) {
+      k_g2p_t<D, DEG, R, MTR_PM_MCCVISC><<<blocks, kChunk, 0, st>>>(A, perm);
+      return;
+    }
+  }
+  k_g2p_t<D, DEG, R><<<blocks, kChunk, 0, st>>>(A, perm);
+}
+
 template <int D, int DEG, typename R>
 int enqueue_step_t(mtr_ctx* c, int parity) {
   cudaStream_t st = c->stream;
@@ -322,11 +358,11 @@ int enqueue_step_t(mtr_ctx* c, int parity) {
     mark(c, "k_g2p_musl");
     k_musl_norm<D, R><<<gblocks, 256, 0, st>>>(A);
     mark(c, "k_musl_norm");
-    k_defgrad_t<D, DEG, R><<<c->cap_tiles, kChunk, 0, st>>>(A, perm);
+    launch_defgrad<D, DEG, R>(rm_specialization(D, true, c->prm.plastic_model), c->cap_tiles, st, A, perm);
     mark(c, "k_defgrad");
     n += 3;
   } else {
-    k_g2p_t<D, DEG, R><<<c->cap_tiles, kChunk, 0, st>>>(A, perm);
+    launch_g2p<D, DEG, R>(rm_specialization(D, false, c->prm.plastic_model), c->cap_tiles, st, A, perm);
     ++n;
     mark(c, "k_g2p");
   }
@@ -519,6 +555,7 @@ uint32_t cap_blocks(uint64_t work, uint32_t per_block, uint32_t cap) {
 
 struct mtr_batch_group {
   int dim = 3, deg = 2, musl = 0;
+  int spm = -1;  // plastic model the return-mapping kernel is compiled for (-1: any)
   bool fp32 = false;
   int passes = 1;
   std::vector<mtr_ctx*> members;
@@ -606,10 +643,26 @@ int enqueue_group_step_t(mtr_batch* b, mtr_batch_group& g) {
   if (g.musl) {
     kb_g2p_musl_w<D, DEG, R><<<g.total[kBK_TILEK], kChunk, musl_smem_bytes<D, R>(), st>>>(B);
     kb_musl_norm<D, R><<<g.total[kBK_NODES], 256, 0, st>>>(B);
-    kb_defgrad_t<D, DEG, R><<<g.total[kBK_TILEK], kChunk, 0, st>>>(B);
+    if constexpr (D == 3) {
+      if (g.spm == MTR_PM_DPMUI)
+        kb_defgrad_t<D, DEG, R, MTR_PM_DPMUI><<<g.total[kBK_TILEK], kChunk, 0, st>>>(B);
+      else
+        kb_defgrad_t<D, DEG, R><<<g.total[kBK_TILEK], kChunk, 0, st>>>(B);
+    } else {
+      kb_defgrad_t<D, DEG, R><<<g.total[kBK_TILEK], kChunk, 0, st>>>(B);
+    }
     n += 3;
   } else {
-    kb_g2p_t<D, DEG, R><<<g.total[kBK_TILEK], kChunk, 0, st>>>(B);
+    if constexpr (D == 3) {
+      if (g.spm == MTR_PM_DP)
+        kb_g2p_t<D, DEG, R, MTR_PM_DP><<<g.total[kBK_TILEK], kChunk, 0, st>>>(B);
+      else if (g.spm == MTR_PM_MCCVISC)
+        kb_g2p_t<D, DEG, R, MTR_PM_MCCVISC><<<g.total[kBK_TILEK], kChunk, 0, st>>>(B);
+      else
+        kb_g2p_t<D, DEG, R><<<g.total[kBK_TILEK], kChunk, 0, st>>>(B);
+    } else {
+      kb_g2p_t<D, DEG, R><<<g.total[kBK_TILEK], kChunk, 0, st>>>(B);
+    }
     ++n;
   }
   kb_tail<D, R><<<g.total[kBK_ONE], 32, 0, st>>>(B);
@@ -1314,15 +1367,18 @@ int mtr_batch_create(mtr_ctx* const* ctxs, int n, mtr_batch** out) {
         CK(cudaStreamSynchronize(c->stream));  // nothing of the member may still run on its own stream
         b->members.push_back(c);
         mtr_batch_group* g = nullptr;
+        const int musl = c->prm.use_musl ? 1 : 0;
+        const int spm = rm_specialization(c->dim, musl != 0, c->prm.plastic_model);
         for (auto& q : b->groups)
-          if (q.dim == c->dim && q.deg == c->deg && q.fp32 == c->fp32 && q.musl == (c->prm.use_musl ? 1 : 0)) g = &q;
+          if (q.dim == c->dim && q.deg == c->deg && q.fp32 == c->fp32 && q.musl == musl && q.spm == spm) g = &q;
         if (!g) {
           b->groups.emplace_back();
           g = &b->groups.back();
           g->dim = c->dim;
           g->deg = c->deg;
           g->fp32 = c->fp32;
-          g->musl = c->prm.use_musl ? 1 : 0;
+          g->musl = musl;
+          g->spm = spm;
         }
         g->members.push_back(c);
       }

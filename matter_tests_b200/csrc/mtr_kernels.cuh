@@ -1010,7 +1010,7 @@ __device__ __forceinline__ double blend_v(double fr, double v, double fl, double
 
 // F_trial = F + dt * gradv * F (deformation_update.cpp:42-44), then the
 // return mapping; writes F, scalars and tau into the out buffer at slot s.
-template <int D, typename R>
+template <int D, typename R, int PM>
 __device__ __forceinline__ void defgrad_and_store(const StepArgsT<R>& A, uint32_t s, double dt, PLoad<D>& p,
                                                   const R (&gv)[D][D], uint32_t& flags, bool& plastic) {
   double T1[D][D], T2[D][D];
@@ -1024,7 +1024,7 @@ __device__ __forceinline__ void defgrad_and_store(const StepArgsT<R>& A, uint32_
 #pragma unroll
     for (int c = 0; c < D; ++c) p.F[r][c] = p.F[r][c] + T2[r][c];
   double tau[Sym<D>::n];
-  plastic = return_map<D>(*A.P, dt, p.F, p.s, tau, flags);
+  plastic = return_map<D, PM>(*A.P, dt, p.F, p.s, tau, flags);
   store_defgrad<D, R>(A.out, A.Np, s, p.F, p.s, tau);
 }
 
@@ -1183,7 +1183,7 @@ __device__ __forceinline__ void gather_patch(const R* pv, const R* pf, const dou
 // 7a. USL: G2P + deformation update + return mapping + position update, one
 // block per tile, node patch in shared memory.
 // ---------------------------------------------------------------------------
-template <int D, int DEG, typename R>
+template <int D, int DEG, typename R, int PM>
 __device__ __forceinline__ void g2p_t_body(const StepArgsT<R>& A, const uint32_t* __restrict__ perm, const uint32_t bid, const uint32_t nblk) {
   using TL = Tiling<D>;
   constexpr int PN = TL::PN, NODES = TL::NODES;
@@ -1230,7 +1230,7 @@ __device__ __forceinline__ void g2p_t_body(const StepArgsT<R>& A, const uint32_t
     }
     uint32_t f = 0;
     bool plastic = false;
-    defgrad_and_store<D, R>(A, s, dt, p, gv, f, plastic);
+    defgrad_and_store<D, R, PM>(A, s, dt, p, gv, f, plastic);
     if (f) raise_status(H, f, p.id);
     nplastic += plastic ? 1u : 0u;
     double xn[3], vn[3];
@@ -1264,9 +1264,9 @@ __device__ __forceinline__ void g2p_t_body(const StepArgsT<R>& A, const uint32_t
   block_count(nplastic, &H->plastic_count);
 }
 
-template <int D, int DEG, typename R>
+template <int D, int DEG, typename R, int PM = -1>
 __global__ void __launch_bounds__(kChunk, MTR_G2P_MIN_BLOCKS) k_g2p_t(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
-  g2p_t_body<D, DEG, R>(A, perm, blockIdx.x, gridDim.x);
+  g2p_t_body<D, DEG, R, PM>(A, perm, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1522,7 +1522,7 @@ __global__ void __launch_bounds__(256) k_musl_norm(StepArgsT<R> A) {
 
 // MUSL: deformation update from the normalised re-projected velocity v2 and
 // the old positions (deformation_update.cpp:6), then the return mapping.
-template <int D, int DEG, typename R>
+template <int D, int DEG, typename R, int PM>
 __device__ __forceinline__ void defgrad_t_body(const StepArgsT<R>& A, const uint32_t* __restrict__ perm, const uint32_t bid, const uint32_t nblk) {
   using TL = Tiling<D>;
   constexpr int PN = TL::PN, NODES = TL::NODES;
@@ -1561,16 +1561,16 @@ __device__ __forceinline__ void defgrad_t_body(const StepArgsT<R>& A, const uint
     }
     uint32_t f = 0;
     bool plastic = false;
-    defgrad_and_store<D, R>(A, s, dt, p, gv, f, plastic);
+    defgrad_and_store<D, R, PM>(A, s, dt, p, gv, f, plastic);
     if (f) raise_status(H, f, p.id);
     nplastic += plastic ? 1u : 0u;
   }
   block_count(nplastic, &H->plastic_count);
 }
 
-template <int D, int DEG, typename R>
+template <int D, int DEG, typename R, int PM = -1>
 __global__ void __launch_bounds__(kChunk, MTR_DEFGRAD_MIN_BLOCKS) k_defgrad_t(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
-  defgrad_t_body<D, DEG, R>(A, perm, blockIdx.x, gridDim.x);
+  defgrad_t_body<D, DEG, R, PM>(A, perm, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1740,11 +1740,11 @@ __global__ void __launch_bounds__(256) kb_grid(BatchView<R> B) {
   if (A) grid_body<D, R>(*A, b, nb);
 }
 
-template <int D, int DEG, typename R>
+template <int D, int DEG, typename R, int PM = -1>
 __global__ void __launch_bounds__(kChunk, MTR_G2P_MIN_BLOCKS) kb_g2p_t(BatchView<R> B) {
   uint32_t b, nb;
   const StepArgsT<R>* A = batch_locate(B, kBK_TILEK, b, nb);
-  if (A) g2p_t_body<D, DEG, R>(*A, A->perm, b, nb);
+  if (A) g2p_t_body<D, DEG, R, PM>(*A, A->perm, b, nb);
 }
 
 template <int D, int DEG, typename R>
@@ -1761,11 +1761,11 @@ __global__ void __launch_bounds__(256) kb_musl_norm(BatchView<R> B) {
   if (A) musl_norm_body<D, R>(*A, b, nb);
 }
 
-template <int D, int DEG, typename R>
+template <int D, int DEG, typename R, int PM = -1>
 __global__ void __launch_bounds__(kChunk, MTR_DEFGRAD_MIN_BLOCKS) kb_defgrad_t(BatchView<R> B) {
   uint32_t b, nb;
   const StepArgsT<R>* A = batch_locate(B, kBK_TILEK, b, nb);
-  if (A) defgrad_t_body<D, DEG, R>(*A, A->perm, b, nb);
+  if (A) defgrad_t_body<D, DEG, R, PM>(*A, A->perm, b, nb);
 }
 
 template <int D, typename R>

@@ -277,10 +277,14 @@ __device__ void initial_tau(const DevParams& P, const double (&F)[D][D], double*
 // Simulation::plasticity for one particle (plasticity.cpp:11-665).
 // F: in = Fe_trial, out = the particle's new F.  Returns true when the
 // particle was projected (the reference's plastic_count).
-template <int D>
+// PM >= 0 compiles the function for that plastic model only (the step's
+// model is then known at compile time and the other models' code is not
+// emitted: a smaller kernel that fits the instruction cache); PM = -1 reads
+// the model from P at run time.
+template <int D, int PM = -1>
 __device__ bool return_map(const DevParams& P, double dt, double (&F)[D][D], PScalars& s, double* tau,
                            uint32_t& flags) {
-  const int pm = P.plastic_model;
+  const int pm = PM >= 0 ? PM : P.plastic_model;
   if (pm == MTR_PM_NOPLASTICITY) {
     if (P.elastic_model == MTR_EL_NEOHOOKEAN) {
       neohookean_tau<D>(P, F, tau);
