@@ -150,6 +150,17 @@ class ClockSampler:
                 "power_w_max": max((float(r[3]) for r in rows if r[3].replace(".", "").isdigit()), default=None)}
 
 
+# DRAM bytes (read + write) per launch of the tile kernels on the 3D mu(I)
+# collapse at full size, from one ncu capture of each
+# (profiles/p2g_musl_defgrad_collapse3d_mui.md, dram__bytes_read.sum +
+# dram__bytes_write.sum); reported as the roofline's traffic for that workload
+MEASURED_TRAFFIC = {
+    ("k_p2g", "fp64"): 189.2e6, ("k_p2g", "mixed"): 112.0e6,
+    ("k_g2p_musl", "fp64"): 148.4e6, ("k_g2p_musl", "mixed"): 86.5e6,
+    ("k_defgrad", "fp64"): 308.2e6, ("k_defgrad", "mixed"): 160.7e6,
+}
+
+
 def hbm_peak():
     try:
         with open(PEAKS_FILE) as f:
@@ -390,10 +401,14 @@ def measure(args, world, rank, local, sc, precision, sampler=None):
            "timed": "mtr_upload (pinned host) + mtr_step(K) + mtr_download, wall clock"}
     status, _ = g.status()
     g.close()
+    traffic = None
+    if args.workload == "collapse3d_mui" and args.scale == 1.0:
+        traffic = MEASURED_TRAFFIC.get((dom, "mixed" if precision == PREC_MIXED else "fp64"))
     out = {"value": value, "ms_per_step": ms_max / args.steps,
            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                        "traffic": None, "peak_source": peak_kind,
+                        "traffic": traffic, "traffic_source": "ncu capture, profiles/" if traffic else None,
+                        "peak_source": peak_kind,
                         "kernel_ms": dom_ms, "kernel_algorithmic_bytes": dom_bytes,
                         "step_algorithmic_GBps": whole, "step_frac": whole / peak,
                         "active_nodes": Ga, "grid_nodes": G},
