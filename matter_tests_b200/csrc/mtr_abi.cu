@@ -482,6 +482,7 @@ void derive_constants(mtr_ctx* c) {  // simulation.cpp:94-136
   h.mu_2 = p.mu_2;
   h.mui0 = (p.plastic_model == MTR_PM_DPMUI || p.plastic_model == MTR_PM_MCCMUI) ? p.mu_1 : p.M;
   h.dgamma_tol = p.precision == MTR_PREC_MIXED ? 1e-9 : 0.0;
+  h.svd_rel = p.precision == MTR_PREC_MIXED ? 1e-12 : 2.220446049250313e-16;
 }
 
 // The first step's grid extents, as remeshFixedInit(2,2,2) will compute them

@@ -32,6 +32,10 @@ struct DevParams {
   double E, nu, stress_tolerance, xi, q_max, q_min, p_min, M, q_cohesion, perzyna_exp, perzyna_visc, beta, p0,
       mu_1, mu_2;
   double mui0;  // muI every particle starts from when use_mibf (simulation.cpp:138-145)
+  // Jacobi SVD stopping size relative to the largest diagonal entry: FP64
+  // epsilon on the FP64 path; 1e-12 on the mixed path, whose FP32 F - I
+  // holds the strain to about 1e-10 (smaller off-diagonals carry no data)
+  double svd_rel;
   // a Perzyna plastic multiplier in (-dgamma_tol, 0) is rounding and is taken
   // as zero rather than reported: 0 on the FP64 path (the reference's checks,
   // plasticity.cpp:190,286; 1e-14 for Cam-Clay, plasticity.cpp:546-547) and
@@ -211,7 +215,9 @@ __device__ __forceinline__ R bspline_dN(R u) {
 // simulation.hpp:232): singular values >= 0 in decreasing order, U and V
 // orthogonal (either may be improper), A = U diag(S) V^T.  The cosines come
 // from one reciprocal square root each instead of a square root and a
-// division (same rotation, rounded differently at the last bit).
+// division (same rotation, rounded differently at the last bit).  `rel` is
+// the off-diagonal size (relative to the largest diagonal entry) below which
+// a pair counts as diagonal: FP64 epsilon by default.
 // ---------------------------------------------------------------------------
 template <int D>
 __device__ __forceinline__ void jacobi_rotate(double (&A)[D][D], double (&U)[D][D], double (&V)[D][D], int q, int p,
@@ -262,8 +268,8 @@ __device__ __forceinline__ void jacobi_rotate(double (&A)[D][D], double (&U)[D][
 }
 
 template <int D>
-__device__ __forceinline__ bool jacobi_needs(const double (&A)[D][D], int q, int p, double maxdiag) {
-  double thr = dmax(2.2250738585072014e-308, 2.0 * 2.220446049250313e-16 * maxdiag);
+__device__ __forceinline__ bool jacobi_needs(const double (&A)[D][D], int q, int p, double maxdiag, double rel) {
+  double thr = dmax(2.2250738585072014e-308, 2.0 * rel * maxdiag);
   return fabs(A[p][q]) > thr || fabs(A[q][p]) > thr;
 }
 
@@ -284,7 +290,8 @@ __device__ __forceinline__ void col_swap(double (&U)[D][D], double (&V)[D][D], d
 }
 
 template <int D>
-__device__ void svd(const double (&Ain)[D][D], double (&U)[D][D], double (&S)[D], double (&V)[D][D]) {
+__device__ void svd(const double (&Ain)[D][D], double (&U)[D][D], double (&S)[D], double (&V)[D][D],
+                    double rel = 2.220446049250313e-16) {
   double A[D][D];
   double scale = 0.0;
 #pragma unroll
@@ -304,16 +311,16 @@ __device__ void svd(const double (&Ain)[D][D], double (&U)[D][D], double (&S)[D]
   for (int i = 0; i < D; ++i) maxdiag = dmax(maxdiag, fabs(A[i][i]));
   for (int sweep = 0; sweep < 32; ++sweep) {
     bool rotated = false;
-    if (jacobi_needs<D>(A, 0, 1, maxdiag)) {
+    if (jacobi_needs<D>(A, 0, 1, maxdiag, rel)) {
       jacobi_rotate<D>(A, U, V, 0, 1, maxdiag);
       rotated = true;
     }
     if constexpr (D == 3) {
-      if (jacobi_needs<D>(A, 0, 2, maxdiag)) {
+      if (jacobi_needs<D>(A, 0, 2, maxdiag, rel)) {
         jacobi_rotate<D>(A, U, V, 0, 2, maxdiag);
         rotated = true;
       }
-      if (jacobi_needs<D>(A, 1, 2, maxdiag)) {
+      if (jacobi_needs<D>(A, 1, 2, maxdiag, rel)) {
         jacobi_rotate<D>(A, U, V, 1, 2, maxdiag);
         rotated = true;
       }
