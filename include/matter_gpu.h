@@ -98,7 +98,7 @@ typedef struct mtr_params {
   int32_t hardening_law;    /* enum mtr_hardening_law                            */
   int32_t use_pradhana, use_mises_q, use_mibf, use_musl;
   int32_t gravity_special;
-  int32_t pbc;              /* must be 0 (periodic BCs are not part of this path) */
+  int32_t pbc;              /* periodic in x over [0, L[0]] (pbc.cpp, remesh.cpp:14-36) */
   uint32_t end_frame;
   int32_t change_particle_positions; /* hard-coded teleport hook, position_update.cpp:35-41 */
   double fps, cfl, cfl_elastic, flip_ratio, rho, gravity_time;
@@ -111,6 +111,7 @@ typedef struct mtr_params {
   double perzyna_exp, perzyna_visc;
   double beta, p0;
   double rho_s, grain_diameter, I_ref, mu_1, mu_2;
+  double L[3];              /* Lx, Ly, Lz: the periodic box of pbc (simulation.hpp:60-66) */
 } mtr_params;
 
 /* ObjectPlate state (object_plate.hpp:13-24, 136-190). v_object[2] unused in 2D. */

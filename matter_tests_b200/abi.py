@@ -82,6 +82,7 @@ class MtrParams(C.Structure):
         ("beta", C.c_double), ("p0", C.c_double),
         ("rho_s", C.c_double), ("grain_diameter", C.c_double), ("I_ref", C.c_double),
         ("mu_1", C.c_double), ("mu_2", C.c_double),
+        ("L", C.c_double * 3),
     ]
 
 
@@ -124,6 +125,8 @@ def default_params(dim=3, spline_deg=2):
     p.rho_s, p.grain_diameter, p.I_ref = 2500.0, 1e-3, 0.279
     p.mu_1 = math.tan(20.9 * math.pi / 180.0)
     p.mu_2 = math.tan(32.8 * math.pi / 180.0)
+    for a in range(3):
+        p.L[a] = 1.0  # Lx = Ly = Lz = 1 (simulation.hpp:60-66)
     return p
 
 

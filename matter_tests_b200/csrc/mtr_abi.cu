@@ -55,6 +55,12 @@ void dfree(void* p) {
   if (p) cudaFree(p);
 }
 
+// blocks for `work` items at `per_block` each, at least 1 and at most `cap`
+uint32_t cap_blocks(uint64_t work, uint32_t per_block, uint32_t cap) {
+  const uint64_t b = (work + per_block - 1) / per_block;
+  return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(b, cap));
+}
+
 int nsym(int d) { return d == 3 ? 6 : 3; }
 
 }  // namespace
@@ -347,6 +353,11 @@ int enqueue_step_t(mtr_ctx* c, int parity) {
   k_p2g_w<D, DEG, R><<<c->cap_tiles, kChunk, p2g_smem_bytes<D, R>(), st>>>(A, perm);
   ++n;
   mark(c, "k_p2g");
+  if (c->prm.pbc) {
+    k_p2g_periodic<D, DEG, R><<<cap_blocks(c->Np, 256, 148 * 8), 256, 0, st>>>(A);
+    ++n;
+    mark(c, "k_p2g_periodic");
+  }
   const uint32_t gblocks = std::min<uint32_t>((c->cap_nodes + 255) / 256, 148 * 16);
   k_grid<D, R><<<gblocks, 256, 0, st>>>(A);
   ++n;
@@ -483,6 +494,8 @@ void derive_constants(mtr_ctx* c) {  // simulation.cpp:94-136
   h.mui0 = (p.plastic_model == MTR_PM_DPMUI || p.plastic_model == MTR_PM_MCCMUI) ? p.mu_1 : p.M;
   h.dgamma_tol = p.precision == MTR_PREC_MIXED ? 1e-9 : 0.0;
   h.svd_rel = p.precision == MTR_PREC_MIXED ? 1e-12 : 2.220446049250313e-16;
+  h.pbc = p.pbc ? 1 : 0;
+  for (int a = 0; a < 3; ++a) h.L[a] = p.L[a];
 }
 
 // The first step's grid extents, as remeshFixedInit(2,2,2) will compute them
@@ -491,6 +504,10 @@ void grid_extent(const mtr_params& p, uint32_t Np, const double* x, uint32_t wan
   const int d = p.dim;
   const double dx = p.dx;
   for (int a = 0; a < 3; ++a) want[a] = 1;
+  if (p.pbc) {  // the fixed grid of remeshFixed(4): [-5 dx (y: -dx), L + 6 dx)
+    for (int a = 0; a < d; ++a) want[a] = (uint32_t)std::ceil(p.L[a] / dx + 12.0) + 2;
+    return;
+  }
   for (int a = 0; a < d; ++a) {
     double mn = x[a], mx = x[a];
     for (uint32_t q = 1; q < Np; ++q) {
@@ -547,10 +564,6 @@ void get_nodes(mtr_ctx* c, double* host, const void* src, size_t n) {
 // Batches: scenes grouped by (dim, spline, precision, MUSL), one launch per
 // step phase and group over a device table of the scenes' arguments.
 // ---------------------------------------------------------------------------
-uint32_t cap_blocks(uint64_t work, uint32_t per_block, uint32_t cap) {
-  const uint64_t b = (work + per_block - 1) / per_block;
-  return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(b, cap));
-}
 
 }  // namespace
 
@@ -755,7 +768,10 @@ int mtr_ctx_create(const mtr_params* params, int device, mtr_ctx** out) {
     if (p.spline_deg != 2 && p.spline_deg != 3) throw MtrError{MTR_ERR_INVALID, "spline_deg must be 2 or 3"};
     if (p.precision != MTR_PREC_FP64 && p.precision != MTR_PREC_MIXED)
       throw MtrError{MTR_ERR_INVALID, "precision must be MTR_PREC_FP64 or MTR_PREC_MIXED"};
-    if (p.pbc) throw MtrError{MTR_ERR_INVALID, "periodic boundaries are not part of this path"};
+    if (p.pbc && (p.use_mibf || p.plastic_model == MTR_PM_SNOW))  // pbc.cpp copies x, v, F, B only
+      throw MtrError{MTR_ERR_INVALID, "periodic boundaries do not combine with use_mibf or the Snow model"};
+    if (p.pbc && !(p.L[0] > 0 && p.L[1] > 0 && (p.dim == 2 || p.L[2] > 0)))
+      throw MtrError{MTR_ERR_INVALID, "periodic boundaries need L > 0"};
     if (p.plastic_model < 0 || p.plastic_model > MTR_PM_SNOW) throw MtrError{MTR_ERR_INVALID, "invalid plastic model"};
     if (p.elastic_model != MTR_EL_HENCKY && p.elastic_model != MTR_EL_NEOHOOKEAN)
       throw MtrError{MTR_ERR_INVALID, "invalid elastic model"};
@@ -1355,6 +1371,7 @@ int mtr_batch_create(mtr_ctx* const* ctxs, int n, mtr_batch** out) {
     for (int i = 0; i < n; ++i) {
       if (!ctxs[i] || !ctxs[i]->uploaded) throw MtrError{MTR_ERR_STATE, "every member needs mtr_upload first"};
       if (ctxs[i]->device != ctxs[0]->device) throw MtrError{MTR_ERR_INVALID, "members must share one device"};
+      if (ctxs[i]->prm.pbc) throw MtrError{MTR_ERR_INVALID, "periodic scenes step on their own, not in a batch"};
       for (int j = 0; j < i; ++j)
         if (ctxs[j] == ctxs[i]) throw MtrError{MTR_ERR_INVALID, "a context appears twice"};
     }

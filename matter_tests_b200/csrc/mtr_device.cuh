@@ -36,6 +36,8 @@ struct DevParams {
   // epsilon on the FP64 path; 1e-12 on the mixed path, whose FP32 F - I
   // holds the strain to about 1e-10 (smaller off-diagonals carry no data)
   double svd_rel;
+  int pbc;       // periodic in x over [0, L[0]] (pbc.cpp)
+  double L[3];   // Lx, Ly, Lz (simulation.hpp:60-66)
   // a Perzyna plastic multiplier in (-dgamma_tol, 0) is rounding and is taken
   // as zero rather than reported: 0 on the FP64 path (the reference's checks,
   // plasticity.cpp:190,286; 1e-14 for Cam-Clay, plasticity.cpp:546-547) and

@@ -241,7 +241,7 @@ __device__ __forceinline__ void header_body(const StepCommon& A) {
     }
     v2 = fmax(v2, __shfl_xor_sync(0xffffffffu, v2, off));
   }
-  __shared__ double s_low[3], s_high[3];
+  __shared__ double s_low[3], s_high[3], s_stop[3];
   __shared__ int s_ok;
   if (lane == 0) {
     // balances of this step (read back by mtr_balance)
@@ -270,7 +270,14 @@ __device__ __forceinline__ void header_body(const StepCommon& A) {
     }
     // remesh
     const double dx = P.dx;
-    if (H->step == 0) {  // remeshFixedInit(2,2,2)
+    if (P.pbc) {  // remeshFixed(4), remesh.cpp:14-36: the same fixed grid every step
+      const double e1 = 5.0, e2 = 6.0;  // 1 + extra_nodes, 2 + extra_nodes
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        s_low[a] = a == 1 ? -dx : __dmul_rn(-dx, e1);
+        s_stop[a] = __dadd_rn(P.L[a], __dmul_rn(e2, dx));
+      }
+    } else if (H->step == 0) {  // remeshFixedInit(2,2,2)
       if (P.grid_ref[0] < 1e10) {
 #pragma unroll
         for (int a = 0; a < D; ++a) {
@@ -313,6 +320,10 @@ __device__ __forceinline__ void header_body(const StepCommon& A) {
         s_high[a] = hi;
       }
     }
+    if (!P.pbc) {
+#pragma unroll
+      for (int a = 0; a < D; ++a) s_stop[a] = __dadd_rn(s_high[a], dx);
+    }
     s_ok = 1;
   }
   __syncwarp();
@@ -321,7 +332,7 @@ __device__ __forceinline__ void header_body(const StepCommon& A) {
     const double dx = P.dx;
     double* ax = lane == 0 ? A.gx : (lane == 1 ? A.gy : A.gz);
     const uint32_t cap = A.cap_axis[lane];
-    const double stop = __dadd_rn(s_high[lane], dx);
+    const double stop = s_stop[lane];
     uint32_t n = 0;
     // counted exactly up to kMaxAxisNodes so the host can size the regrowth in
     // one go; the bound also ends the loop for non-finite extents
@@ -874,6 +885,108 @@ __global__ void __launch_bounds__(kChunk) k_p2g_w(StepArgsT<R> A, const uint32_t
 }
 
 // ---------------------------------------------------------------------------
+// 5b. periodic copies (pbc.cpp:37-85): a particle within 4 dx of x = Lx (else
+// of x = 0) also scatters mass, momentum and force from x - Lx (else x + Lx),
+// with the same stencil and formulas as P2G (p2g.cpp:6-100,
+// explicit_euler_update.cpp:15-77).  Few particles have a copy; each one is a
+// thread with global atomics.
+// ---------------------------------------------------------------------------
+template <int D, int DEG, typename R>
+__global__ void __launch_bounds__(256) k_p2g_periodic(StepArgsT<R> A) {
+  const StepHeader* H = A.H;
+  if (step_inactive(H)) return;
+  const DevParams& P = *A.P;
+  constexpr int NS = Sym<D>::n, KN = D == 3 ? 4 : 1;
+  const uint32_t Np = A.Np, cap = A.cap_nodes;
+  const double ioh = P.one_over_dx, lim = 4.0 * P.dx, Lx = P.L[0], apicD = P.apicDinverse;
+  const bool apic = P.flip_ratio < 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < Np; i += gridDim.x * blockDim.x) {
+    double xp[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int a = 0; a < D; ++a) xp[a] = A.in.x[(size_t)a * Np + i];
+    double diff = Lx - xp[0];
+    if (diff < lim && diff > 0) {
+      xp[0] = -diff;
+    } else {
+      diff = xp[0];
+      if (!(diff < lim && diff >= 0)) continue;
+      xp[0] = Lx + diff;
+    }
+    double vp[3] = {0.0, 0.0, 0.0}, Bm[D][D], tau[NS];
+#pragma unroll
+    for (int a = 0; a < D; ++a) vp[a] = A.in.v[(size_t)a * Np + i];
+#pragma unroll
+    for (int r = 0; r < D; ++r)
+#pragma unroll
+      for (int c = 0; c < D; ++c) Bm[r][c] = apic ? (double)A.in.B[(size_t)(r * D + c) * Np + i] : 0.0;
+#pragma unroll
+    for (int q = 0; q < NS; ++q) tau[q] = A.in.tau[(size_t)q * Np + i];
+    int base[3] = {0, 0, 0};
+    bool oob = false;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      int b = (int)floor((xp[a] - H->org[a]) * ioh) - 1;
+      b = b < 0 ? 0 : b;  // p2g.cpp:21-24 clamps at zero
+      base[a] = b;
+      if (b + 3 >= (int)H->N[a]) oob = true;
+    }
+    if (oob) {
+      raise_status(A.H, MTR_STATUS_STENCIL_OOB, A.in.id[i]);
+      continue;
+    }
+    double w[3][4], dw[3][4], crd[3][4];
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      const double* ax = a == 0 ? A.gx : (a == 1 ? A.gy : A.gz);
+#pragma unroll
+      for (int o = 0; o < 4; ++o) {
+        crd[a][o] = ax[base[a] + o];
+        const double u = (xp[a] - crd[a][o]) * ioh;
+        w[a][o] = bspline_N<DEG>(u);
+        dw[a][o] = bspline_dN<DEG>(u);
+      }
+    }
+#pragma unroll
+    for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+        for (int kk = 0; kk < KN; ++kk) {
+          const uint32_t l = node_index(H, base[0] + ii, base[1] + jj, D == 3 ? base[2] + kk : 0);
+          const double wxy = w[0][ii] * w[1][jj];
+          const double weight = D == 3 ? wxy * w[2][kk] : wxy;
+          if (weight > 1e-25) {
+            atomicAdd(&A.acc[l], (R)weight);
+            const double pd[3] = {crd[0][ii] - xp[0], crd[1][jj] - xp[1], D == 3 ? crd[2][kk] - xp[2] : 0.0};
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+              double bv = Bm[a][0] * pd[0];
+#pragma unroll
+              for (int c = 1; c < D; ++c) bv += Bm[a][c] * pd[c];
+              atomicAdd(&A.acc[(size_t)(1 + a) * cap + l], (R)(weight * (vp[a] + apicD * bv)));
+            }
+          }
+          double g[3];
+          if constexpr (D == 3) {
+            g[0] = dw[0][ii] * w[1][jj] * w[2][kk] * ioh;
+            g[1] = w[0][ii] * dw[1][jj] * w[2][kk] * ioh;
+            g[2] = w[0][ii] * w[1][jj] * dw[2][kk] * ioh;
+          } else {
+            g[0] = dw[0][ii] * w[1][jj] * ioh;
+            g[1] = w[0][ii] * dw[1][jj] * ioh;
+          }
+#pragma unroll
+          for (int a = 0; a < D; ++a) {
+            double f = sym_at<D>(tau, a, 0) * g[0];
+#pragma unroll
+            for (int c = 1; c < D; ++c) f += sym_at<D>(tau, a, c) * g[c];
+            if (f != 0.0) atomicAdd(&A.acc[(size_t)(1 + D + a) * cap + l], (R)f);
+          }
+        }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // 6. grid update, one thread per node (arithmetic in FP64 on both paths)
 // ---------------------------------------------------------------------------
 template <int D, typename R>
@@ -999,6 +1112,21 @@ __device__ __forceinline__ void store_defgrad(const PBufT<R>& b, uint32_t Np, ui
   b.sc[(size_t)MTR_SCALAR_MUI * Np + s] = (R)sc.muI;
 #pragma unroll
   for (int q = 0; q < Sym<D>::n; ++q) b.tau[(size_t)q * Np + s] = (R)tau[q];
+}
+
+// the end of positionUpdate (position_update.cpp:26-41): periodic wrap in x,
+// then the hard-coded teleport hook
+__device__ __forceinline__ void wrap_and_teleport(const DevParams& P, double (&xn)[3]) {
+  if (P.pbc) {
+    if (xn[0] > P.L[0])
+      xn[0] = xn[0] - P.L[0];
+    else if (xn[0] < 0)
+      xn[0] = P.L[0] + xn[0];
+  }
+  if (P.change_particle_positions && xn[0] > 0.8) {
+    xn[0] = -0.1;
+    xn[1] += 0.27;
+  }
 }
 
 // velocity blend of position_update.cpp:14-24 / musl.cpp:15-22
@@ -1239,10 +1367,7 @@ __device__ __forceinline__ void g2p_t_body(const StepArgsT<R>& A, const uint32_t
       xn[a] = p.x[a] + dt * pic[a];
       vn[a] = blend_v(fr, p.v[a], (double)flp[a], pic[a]);
     }
-    if (P.change_particle_positions && xn[0] > 0.8) {  // position_update.cpp:35-41
-      xn[0] = -0.1;
-      xn[1] += 0.27;
-    }
+    wrap_and_teleport(P, xn);
 #pragma unroll
     for (int a = 0; a < D; ++a) {
       A.out.x[(size_t)a * Np + s] = xn[a];
@@ -1381,14 +1506,18 @@ __device__ __forceinline__ void g2p_musl_w_body(const StepArgsT<R>& A, const uin
 #pragma unroll
             for (int c = 0; c < D; ++c) Bp[r][c] = R(0.0);
         }
+        double xn[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int a = 0; a < D; ++a) {
           const double vn = blend_v(fr, vp[a], (double)flp[a], pic[a]);
           if constexpr (kFP64<R>) S.x[a] = xp[a];
           S.v[a] = (R)vn;
-          A.out.x[(size_t)a * Np + s] = xp[a] + dt * pic[a];  // positionUpdate: x + dt pic
+          xn[a] = xp[a] + dt * pic[a];  // positionUpdate: x + dt pic
           A.out.v[(size_t)a * Np + s] = (R)vn;
         }
+        wrap_and_teleport(P, xn);
+#pragma unroll
+        for (int a = 0; a < D; ++a) A.out.x[(size_t)a * Np + s] = xn[a];
 #pragma unroll
         for (int r = 0; r < D; ++r)
 #pragma unroll

@@ -152,11 +152,6 @@ bool Simulation::prepare_device() {
     mtr_ctx_destroy(ctx_);
     ctx_ = nullptr;
   }
-  if (pbc) {
-    debug("Periodic boundaries are not part of the B200 step.");
-    exit = 1;
-    return false;
-  }
   if (particles.x.size() < Np || Np == 0) {
     debug("No particles: set Np and sim.particles (or call sampleParticles) before simulate().");
     exit = 1;
@@ -175,7 +170,14 @@ bool Simulation::prepare_device() {
   p.use_mibf = use_mibf;
   p.use_musl = use_musl;
   p.gravity_special = gravity_special;
-  p.pbc = 0;
+  p.pbc = pbc;
+  p.L[0] = Lx;
+  p.L[1] = Ly;
+#ifdef THREEDIM
+  p.L[2] = Lz;
+#else
+  p.L[2] = 1.0;
+#endif
   p.end_frame = end_frame;
   p.change_particle_positions = change_particle_positions;
   p.fps = fps;

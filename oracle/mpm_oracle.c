@@ -38,6 +38,10 @@ typedef struct orc {
   double *x, *v, *pic, *flip, *F, *B, *dPsidF, *Fe;
   double *eps_pl_dev, *eps_pl_vol, *eps_pl_vol_pradhana, *delta_gamma, *viscosity, *muI;
   uint32_t* keys; /* blocked cell key of each particle at the last step (GPU sort key) */
+  /* periodic ghosts of this step (PBCAddParticles, pbc.cpp:37-85): source particle and position */
+  uint32_t ng;
+  uint32_t* gsrc;
+  double* gpos;
   /* grid, data_structures.hpp:49-66 */
   double *gx, *gy, *gz;
   uint32_t Nx, Ny, Nz, G;
@@ -352,6 +356,49 @@ static void particle_bbox(const orc* s, double* mn, double* mx) {
     }
 }
 
+/* remeshFixed(extra_nodes), remesh.cpp:14-36: the fixed grid of periodic runs */
+static void remesh_fixed(orc* s, unsigned int extra) {
+  double dx = s->P.dx;
+  double e1 = (double)(1 + extra), e2 = (double)(2 + extra);
+  s->gx = arange(-dx * e1, s->P.L[0] + e2 * dx, dx, &s->Nx, s->gx, &s->cap_axis[0]);
+  s->gy = arange(-dx, s->P.L[1] + e2 * dx, dx, &s->Ny, s->gy, &s->cap_axis[1]);
+  if (s->dim == 3)
+    s->gz = arange(-dx * e1, s->P.L[2] + e2 * dx, dx, &s->Nz, s->gz, &s->cap_axis[2]);
+  else
+    s->Nz = 1;
+  s->xc = s->gx[0];
+  s->yc = s->gy[0];
+  s->zc = s->dim == 3 ? s->gz[0] : 0.0;
+  s->G = s->Nx * s->Ny * s->Nz;
+}
+
+/* PBCAddParticles(safety_factor), pbc.cpp:37-85: a particle within
+ * safety_factor * dx of x = Lx (else of x = 0) gets a copy shifted by -Lx
+ * (else +Lx); copies follow the particles in index order */
+static void pbc_add(orc* s, unsigned int safety_factor) {
+  int d = s->dim;
+  double Lx = s->P.L[0], lim = safety_factor * s->P.dx;
+  s->ng = 0;
+  s->gsrc = (uint32_t*)realloc(s->gsrc, (s->Np ? s->Np : 1) * sizeof(uint32_t));
+  s->gpos = (double*)realloc(s->gpos, (size_t)(s->Np ? s->Np : 1) * d * sizeof(double));
+  for (uint32_t p = 0; p < s->Np; ++p) {
+    const double* x = s->x + (size_t)p * d;
+    double xg0;
+    double diff = Lx - x[0];
+    if (diff < lim && diff > 0) {
+      xg0 = -diff;
+    } else {
+      diff = x[0];
+      if (!(diff < lim && diff >= 0)) continue;
+      xg0 = Lx + diff;
+    }
+    double* g = s->gpos + (size_t)s->ng * d;
+    for (int a = 0; a < d; ++a) g[a] = x[a];
+    g[0] = xg0;
+    s->gsrc[s->ng++] = p;
+  }
+}
+
 /* remeshFixedInit(2,2,2), remesh.cpp:38-182 */
 static void remesh_init(orc* s) {
   int d = s->dim;
@@ -486,8 +533,9 @@ static void update_dt(orc* s) {
 static void p2g(orc* s) {
   int d = s->dim;
   double org[3] = {s->xc, s->yc, s->zc};
-  for (uint32_t p = 0; p < s->Np; ++p) {
-    const double* xp = s->x + (size_t)p * d;
+  for (uint32_t it = 0; it < s->Np + s->ng; ++it) {  /* particles, then periodic copies */
+    const uint32_t p = it < s->Np ? it : s->gsrc[it - s->Np];
+    const double* xp = it < s->Np ? s->x + (size_t)p * d : s->gpos + (size_t)(it - s->Np) * d;
     const double* vp = s->v + (size_t)p * d;
     M3 Bp;
     m_load(d, s->B + (size_t)p * d * d, Bp);
@@ -878,7 +926,8 @@ static void explicit_euler(orc* s, double* force) {
   int d = s->dim;
   double org[3] = {s->xc, s->yc, s->zc};
   memset(force, 0, (size_t)s->G * d * sizeof(double));
-  for (uint32_t p = 0; p < s->Np; ++p) {
+  for (uint32_t it = 0; it < s->Np + s->ng; ++it) {  /* particles, then periodic copies */
+    const uint32_t p = it < s->Np ? it : s->gsrc[it - s->Np];
     M3 Fe, dPsidF, tau;
     m_load(d, s->F + (size_t)p * d * d, Fe);
     if (s->P.plastic_model == MTR_PM_SNOW) {
@@ -893,7 +942,7 @@ static void explicit_euler(orc* s, double* force) {
         hencky_piola(s, Fe, dPsidF);
       m_mul_bt(d, dPsidF, Fe, tau);
     }
-    const double* xp = s->x + (size_t)p * d;
+    const double* xp = it < s->Np ? s->x + (size_t)p * d : s->gpos + (size_t)(it - s->Np) * d;
     int base[3] = {0, 0, 0};
     for (int a = 0; a < d; ++a) {
       int b = (int)floor((xp[a] - org[a]) * s->one_over_dx) - 1;
@@ -1785,13 +1834,19 @@ static void deformation_update(orc* s) {
   }
 }
 
-/* positionUpdate, position_update.cpp:6-46 (PBC excluded) */
+/* positionUpdate, position_update.cpp:6-46 */
 static void position_update(orc* s) {
   int d = s->dim;
   for (uint32_t p = 0; p < s->Np; ++p) {
     double* x = s->x + (size_t)p * d;
     for (int a = 0; a < d; ++a) x[a] = x[a] + s->dt * s->pic[(size_t)p * d + a];
     if (!s->P.use_musl) blend_v(s, p);
+    if (s->P.pbc) { /* position_update.cpp:26-33 */
+      if (x[0] > s->P.L[0])
+        x[0] = x[0] - s->P.L[0];
+      else if (x[0] < 0)
+        x[0] = s->P.L[0] + x[0];
+    }
     if (s->P.change_particle_positions) { /* position_update.cpp:35-41 */
       if (x[0] > 0.8) {
         x[0] = -0.1;
@@ -1927,15 +1982,20 @@ int orc_step(orc* s, int nsteps) {
   for (int it = 0; it < nsteps; ++it) {
     if (s->done || s->exit_flag || s->frame >= s->P.end_frame) break;
     update_dt(s);
-    if (s->step == 0)
+    if (s->P.pbc) { /* simulation.cpp:222-233 */
+      if (s->step == 0) remesh_fixed(s, 4);
+    } else if (s->step == 0) {
       remesh_init(s);
-    else
+    } else {
       remesh_cont(s);
+    }
     resize_grid(s);
     compute_keys(s);
+    if (s->P.pbc) pbc_add(s, 4);
     p2g(s);
     force = (double*)realloc(force, (size_t)s->G * d * sizeof(double) + 8);
     explicit_euler(s, force);
+    s->ng = 0; /* PBCDelParticles, pbc.cpp:87-101 */
     g2p(s);
     if (s->P.use_musl) musl(s);
     deformation_update(s);
@@ -2014,7 +2074,7 @@ void orc_destroy(orc* s) {
   if (!s) return;
   free(s->x); free(s->v); free(s->pic); free(s->flip); free(s->F); free(s->B); free(s->dPsidF);
   free(s->Fe); free(s->eps_pl_dev); free(s->eps_pl_vol); free(s->eps_pl_vol_pradhana);
-  free(s->delta_gamma); free(s->viscosity); free(s->muI); free(s->keys);
+  free(s->delta_gamma); free(s->viscosity); free(s->muI); free(s->keys); free(s->gsrc); free(s->gpos);
   free(s->gx); free(s->gy); free(s->gz); free(s->gmass); free(s->gv); free(s->gflip); free(s->gfric);
   free(s);
 }

@@ -130,7 +130,12 @@ void* ref_create(const mtr_params* P, int n_threads) {
   s.change_particle_positions = P->change_particle_positions;
   s.use_mibf = P->use_mibf;
   s.use_musl = P->use_musl;
-  s.pbc = false;
+  s.pbc = P->pbc != 0;
+  s.Lx = P->L[0];
+  s.Ly = P->L[1];
+#ifdef THREEDIM
+  s.Lz = P->L[2];
+#endif
   for (int a = 0; a < kDim; ++a) {
     s.gravity(a) = P->gravity[a];
     s.grid_reference_point(a) = P->grid_reference_point[a];

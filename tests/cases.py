@@ -113,6 +113,23 @@ def box_plates(scene, bc, friction, moving=False):
     return scene
 
 
+def periodic(dim=3, deg=2, n=6, musl=0, flip_ratio=-2.0, seed=3):
+    """A block filling a periodic box in x (pbc, pbc.cpp): it moves +x at
+    1.5 m/s so particles cross x = Lx and re-enter at x = 0, under a light
+    gravity, clear of the fixed grid's y (and z) edges."""
+    sc = apply(block(dim, deg, n=n, seed=seed, gravity=(0.4, -1.0, 0.0)), plastic_model=PM.DP, M=0.6,
+               use_musl=musl, flip_ratio=flip_ratio)
+    p = sc.params
+    p.pbc = 1
+    p.L[0], p.L[1], p.L[2] = n * p.dx, 0.1, 0.08
+    sc.x[:, 1] += 0.03
+    if dim == 3:
+        sc.x[:, 2] += 0.01
+    sc.v[:, 0] += 1.5
+    sc.plates, sc.objects = [], []
+    return sc
+
+
 def object_cases(dim):
     """Analytic objects (object_*.hpp) placed so they intersect a block at the origin."""
     cases = {

@@ -70,7 +70,10 @@ def test_invalid_parameters_are_rejected(lib):
     assert lib.mtr_ctx_create(C.byref(p), 0, C.byref(h)) == abi.MTR_ERR_INVALID
     assert b"Hencky" in lib.mtr_last_error()
     p = abi.default_params(3, 2)
-    p.pbc = 1
+    p.pbc, p.use_mibf = 1, 1  # pbc.cpp copies x, v, F, B only: no friction field for the copies
+    assert lib.mtr_ctx_create(C.byref(p), 0, C.byref(h)) == abi.MTR_ERR_INVALID
+    p = abi.default_params(3, 2)
+    p.pbc, p.L[2] = 1, 0.0
     assert lib.mtr_ctx_create(C.byref(p), 0, C.byref(h)) == abi.MTR_ERR_INVALID
 
 

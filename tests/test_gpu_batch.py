@@ -131,6 +131,15 @@ def test_batch_members_stop_at_their_own_end_and_regrow_their_own_grid():
         g.close()
 
 
+def test_periodic_scenes_are_refused():
+    from matter_tests_b200.gpu import GpuBatch, MtrFailure
+    sims = [make_sim(scene_set()[0]), make_sim(cases.periodic(3, 2))]
+    with pytest.raises(MtrFailure):
+        GpuBatch(sims)
+    for g in sims:
+        g.close()
+
+
 @pytest.mark.parametrize("prec", [PREC_FP64, PREC_MIXED])
 def test_footprint_matches_the_upload(prec):
     """mtr_footprint predicts what mtr_upload allocates (within the driver's

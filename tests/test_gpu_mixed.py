@@ -93,6 +93,12 @@ def test_mixed_objects_and_mibf():
     check_one_step(sc, [])
 
 
+@pytest.mark.parametrize("dim,deg,musl", [(3, 2, 0), (2, 3, 1)])
+def test_mixed_one_step_periodic(dim, deg, musl):
+    sc = cases.periodic(dim, deg, n=6 if dim == 3 else 10, musl=musl)
+    check_one_step(sc, [])
+
+
 @pytest.mark.parametrize("prec,tol", [(PREC_FP64, 1e-12), (PREC_MIXED, 2e-6)])
 @pytest.mark.parametrize("transfer", ["apic_usl", "aflip_musl", "picflip_usl"])
 def test_mass_and_momentum_balance(prec, tol, transfer):

@@ -129,3 +129,15 @@ def test_grid_regrowth():
     g, o = run_gpu(sc, 60), run_oracle(sc, 60)
     assert g["c"]["step"] == 60
     compare_states(g, o, 1e-8, sens=oracle_sensitivity(sc, 60))
+
+
+@pytest.mark.parametrize("dim,deg,musl,fr", [(3, 2, 0, -2.0), (3, 3, 1, -0.95), (2, 2, 0, 0.9), (2, 3, 1, -2.0)])
+@pytest.mark.parametrize("nsteps", [1, 12])
+def test_periodic(dim, deg, musl, fr, nsteps):
+    """Periodic boundaries in x: the fixed grid, the periodic copies in P2G and
+    the wrap of positions, while particles cross x = Lx."""
+    sc = cases.periodic(dim, deg, n=6 if dim == 3 else 10, musl=musl, flip_ratio=fr)
+    g, o = run_gpu(sc, nsteps), run_oracle(sc, nsteps)
+    compare_states(g, o, REL_ONE_STEP if nsteps == 1 else 1e-9, sens=oracle_sensitivity(sc, nsteps))
+    x0 = g["p"]["x"][:, 0]
+    assert x0.min() >= 0.0 and x0.max() <= sc.params.L[0]

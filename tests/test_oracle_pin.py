@@ -103,3 +103,13 @@ def test_end_of_simulation_clock():
     o, r = _run_both(sc, 10)
     _assert_identical(o, r)
     assert o["n"] == 4 and o["c"]["done"] == 1
+
+
+@pytest.mark.parametrize("deg,musl,fr", [(2, 0, -2.0), (3, 1, -0.95), (2, 0, 0.9)])
+def test_periodic_bitexact(deg, musl, fr):
+    """Periodic boundaries (remeshFixed(4), PBCAddParticles(4) and the wrap in
+    positionUpdate) over 12 steps in which particles cross x = Lx."""
+    sc = cases.periodic(3, deg, musl=musl, flip_ratio=fr)
+    o, r = _run_both(sc, 12)
+    _assert_identical(o, r)
+    assert o["p"]["x"][:, 0].min() >= 0.0 and o["p"]["x"][:, 0].max() <= sc.params.L[0]
