@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
     ap.add_argument("--serve-requests", type=int, default=60, help="requests of the serving measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default tile-kernel block shapes (128 threads) instead of tuning them")
+    ap.add_argument("--tune-reps", type=int, default=3, help="rounds of trial steps per candidate block shape")
     return ap.parse_args()
 
 
@@ -343,6 +346,8 @@ def measure(args, world, rank, local, sc, precision, sampler=None):
     g.upload(sc.x, sc.v, sc.F, sc.B, sc.scalars)
     g.set_objects(sc.plates, sc.objects)
     g.step(args.warmup)
+    # block shapes of the tile kernels, tuned on the warmed-up scene (setup, untimed)
+    shapes = g.tile_threads if args.no_autotune else g.autotune(args.tune_reps)
     stream = torch.cuda.ExternalStream(g.stream, device=torch.device("cuda", local))
     barrier(world)
     torch.cuda.synchronize(local)
@@ -413,7 +418,7 @@ def measure(args, world, rank, local, sc, precision, sampler=None):
                         "step_algorithmic_GBps": whole, "step_frac": whole / peak,
                         "active_nodes": Ga, "grid_nodes": G},
            "kernel_ms": {k: round(v / max(1, sum(1 for n, _ in slots if n == k)), 5) for k, v in agg.items()},
-           "profiled_step_ms": step_ms, "e2e": e2e, "gpu_launches": launches,
+           "profiled_step_ms": step_ms, "e2e": e2e, "gpu_launches": launches, "tile_threads": shapes,
            "sim_clock": {"step": ck["step"], "time": ck["time"]}, "status_flags": status}
     return out, state
 
@@ -471,17 +476,28 @@ def ensemble_measure(args, local):
         g.set_objects(sc.plates, sc.objects)
         return g
 
+    def timed(b, k):
+        st = torch.cuda.ExternalStream(b.stream, device=torch.device("cuda", local))
+        torch.cuda.synchronize(local)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        b.step(k)
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
     sims = [make(sc) for sc in scs]
     batch = GpuBatch(sims)
     batch.step(W)
-    stream = torch.cuda.ExternalStream(batch.stream, device=torch.device("cuda", local))
-    torch.cuda.synchronize(local)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    batch.step(K)
-    ev1.record(stream)
-    ev1.synchronize()
-    ms = ev0.elapsed_time(ev1)
+    default_shapes = None
+    if not args.no_autotune:
+        # the default shapes first, on K/4 steps, then the tuned shapes
+        kd = max(8, K // 4)
+        default_shapes = {"value": ntot * kd / (timed(batch, kd) / 1e3), "steps": kd,
+                          "groups": batch.groups()}
+        batch.autotune(args.tune_reps)
+    groups = batch.groups()
+    ms = timed(batch, K)
     launches = batch.launch_count()
     lat = []
     for _ in range(max(8, K // 8)):
@@ -497,6 +513,8 @@ def ensemble_measure(args, local):
     for sc in scs:
         g = make(sc)
         g.step(W)
+        if not args.no_autotune:
+            g.autotune(args.tune_reps)
         st = torch.cuda.ExternalStream(g.stream, device=torch.device("cuda", local))
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(st)
@@ -515,6 +533,7 @@ def ensemble_measure(args, local):
             "serial": {"value": serial, "ms_total": serial_ms,
                        "timed": "each scene alone through its own context and graphs, CUDA events"},
             "batched_over_serial": value / serial, "gpu_launches": launches, "dtype": "f32+f64",
+            "groups": groups, "default_shapes": default_shapes,
             "config": "seeded DP column collapses: Np log-uniform 5k-300k, P(3D) 0.5, aspect U(0.5,4), "
                       "friction angle U(20,40) deg, E log-uniform 1e5-1e7 Pa, APIC USL, quadratic",
             "all_scenes_advanced": bool(min(steps_done) >= W + K)}
@@ -614,8 +633,9 @@ def gpu_arm(args, world, rank, local):
                 "roofline": mixed["roofline"], "kernel_ms": mixed["kernel_ms"],
                 "profiled_step_ms": mixed["profiled_step_ms"], "cpu_baseline": cpu, "e2e": mixed["e2e"],
                 "gpu_launches": mixed["gpu_launches"] + fp64["gpu_launches"], "clocks": clocks,
+                "tile_threads": mixed["tile_threads"],
                 "fp64": {k: fp64[k] for k in ("value", "ms_per_step", "roofline", "kernel_ms", "e2e",
-                                              "gpu_launches", "status_flags")},
+                                              "gpu_launches", "status_flags", "tile_threads")},
                 "mixed_over_fp64": mixed["value"] / fp64["value"],
                 "mixed_error_vs_fp64": err, "ensemble": ens, "serving": served,
                 "sim_clock": mixed["sim_clock"], "status_flags": mixed["status_flags"]}

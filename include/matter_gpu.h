@@ -260,6 +260,64 @@ void* mtr_batch_stream(mtr_batch* batch);
 void mtr_batch_destroy(mtr_batch* batch);
 int mtr_footprint(const mtr_params* params, uint32_t Np, const double* x, uint64_t* bytes);
 
+/* Frame output (Simulation::saveParticleData, save_data.cpp:7-171).
+ * mtr_frame_begin enqueues, behind the steps already issued, a kernel that
+ * writes one row of FP64 columns per particle in the original particle order
+ * — the columns of the reference's particle file, in its order:
+ *   x y [z] vx vy [vz] p q Je [eps_pl_vol eps_pl_dev delta_gamma] [muI] [viscosity]
+ * (p = -tr(tau)/dim, q = sqrt(c tau_dev:tau_dev), c = 3/2 with use_mises_q
+ * else 1/2, Je = det F; the plastic triple with any plastic model, muI with
+ * DPVisc/MCCVisc and use_mibf or a mu(I) model, viscosity with a mu(I)
+ * model) — and copies them to pinned host memory on a second stream.  It
+ * returns at once: the context can go on stepping while the copy runs and the
+ * caller writes the previous file.  mtr_frame_wait waits (bounded) for that
+ * copy and returns the rows (valid until the next mtr_frame_begin), their
+ * count and width, and the clock of the snapshot.  mtr_frame_columns writes
+ * the column names (static strings) and returns their number.
+ * mtr_get_grid_friction: the grid friction of the last step (Grid::friction,
+ * use_mibf only; the grid file's `friction` column, save_data.cpp:247-255). */
+int mtr_frame_columns(mtr_ctx* ctx, const char** names, int max_names);
+int mtr_frame_begin(mtr_ctx* ctx);
+int mtr_frame_wait(mtr_ctx* ctx, double timeout_seconds, const double** rows, uint32_t* n, int* ncols,
+                   mtr_clock* clock);
+int mtr_get_grid_friction(mtr_ctx* ctx, double* friction);
+
+/* Block shapes of the tile kernels — no counterpart in the reference, whose
+ * loops are OpenMP-scheduled over particles.  Each step phase that walks the
+ * particles of a grid tile runs one thread block per tile; its size is chosen
+ * per context (or per batch group) among 64, 128 and 256 threads, by slot:
+ *   threads[MTR_TILE_P2G]     P2G with the stress force (default 128)
+ *   threads[MTR_TILE_MUSL]    MUSL G2P and re-scatter (default 128)
+ *   threads[MTR_TILE_G2P]     USL G2P, deformation update, return mapping (64..128)
+ *   threads[MTR_TILE_DEFGRAD] MUSL deformation update, return mapping (default 128)
+ * Results do not depend on the shapes beyond the order of floating-point
+ * atomic sums.  mtr_autotune times `reps` rounds of trial steps of the
+ * context's current state with each candidate shape and keeps the fastest
+ * per slot (a slot keeps its shape unless another is more than 2% faster).
+ * A trial step runs every kernel of a step except the commit, so the particle
+ * state, the clock, the plates and the counters are the same afterwards; a
+ * grid that must grow is grown as the next step would.  A context that has
+ * ended keeps its shapes.  mtr_batch_autotune does the same for every group of
+ * a batch at once; mtr_batch_get_group reports a group's key, size and shapes.
+ * Groups start with the shapes of their first member. */
+#define MTR_TILE_P2G 0
+#define MTR_TILE_MUSL 1
+#define MTR_TILE_G2P 2
+#define MTR_TILE_DEFGRAD 3
+typedef struct mtr_group_info {
+  int32_t dim, spline_deg, fp32, musl;
+  int32_t plastic_model_kernel; /* model the return mapping is compiled for, -1: any */
+  int32_t members;
+  int32_t tile_threads[4];
+} mtr_group_info;
+int mtr_autotune(mtr_ctx* ctx, int reps, int* threads /* [4] out, may be NULL */);
+int mtr_set_tile_threads(mtr_ctx* ctx, const int* threads /* [4] */);
+int mtr_get_tile_threads(mtr_ctx* ctx, int* threads /* [4] */);
+int mtr_batch_autotune(mtr_batch* batch, int reps);
+int mtr_batch_groups(mtr_batch* batch);
+int mtr_batch_get_group(mtr_batch* batch, int group, mtr_group_info* info);
+int mtr_batch_set_tile_threads(mtr_batch* batch, int group, const int* threads /* [4] */);
+
 /* mtr_p2g_noalloc — no counterpart in the reference.  The particle-to-grid
  * transfer (the P2G of p2g.cpp: grid mass = particle mass * sum of weights,
  * grid velocity = sum of w (v_p + B_p D^-1 (x_i - x_p)) / sum of w) of one

@@ -105,6 +105,15 @@ class MtrClock(C.Structure):
                 ("frame", C.c_uint32), ("done", C.c_int32), ("reserved", C.c_int32)]
 
 
+class MtrGroupInfo(C.Structure):
+    _fields_ = [("dim", C.c_int32), ("spline_deg", C.c_int32), ("fp32", C.c_int32), ("musl", C.c_int32),
+                ("plastic_model_kernel", C.c_int32), ("members", C.c_int32), ("tile_threads", C.c_int32 * 4)]
+
+
+# slots of the tile-kernel block shapes (MTR_TILE_*)
+TILE_SLOTS = ("p2g", "musl", "g2p", "defgrad")
+
+
 def default_params(dim=3, spline_deg=2):
     """Defaults of Simulation's public fields (simulation.hpp:36-106)."""
     import math

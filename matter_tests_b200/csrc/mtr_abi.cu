@@ -18,6 +18,7 @@
 #include <cstring>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/matter_gpu.h"
@@ -63,6 +64,57 @@ uint32_t cap_blocks(uint64_t work, uint32_t per_block, uint32_t cap) {
 
 int nsym(int d) { return d == 3 ? 6 : 3; }
 
+// Events recorded after launches on one stream (per-launch timing): an entry
+// per launch, events reused from a pool.
+struct EventMarks {
+  bool on = false;
+  std::vector<std::pair<const char*, cudaEvent_t>> list;
+  std::vector<int> tag;  // caller's tag of each entry (the batch group)
+  std::vector<cudaEvent_t> pool;
+  size_t next = 0;
+  void record(const char* name, cudaStream_t st, int t = 0) {
+    if (!on) return;
+    if (next == pool.size()) {
+      cudaEvent_t e;
+      CK(cudaEventCreate(&e));
+      pool.push_back(e);
+    }
+    cudaEvent_t e = pool[next++];
+    CK(cudaEventRecord(e, st));
+    list.emplace_back(name, e);
+    tag.push_back(t);
+  }
+  void reset() {
+    list.clear();
+    tag.clear();
+    next = 0;
+  }
+  // milliseconds between entry i - 1 and entry i
+  float since_previous(size_t i) const {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, list[i - 1].second, list[i].second));
+    return ms;
+  }
+  ~EventMarks() {
+    for (cudaEvent_t e : pool) cudaEventDestroy(e);
+  }
+};
+
+// Block shapes of the tile kernels (threads per tile block), one per kernel
+// slot: P2G, MUSL G2P + re-scatter, USL G2P, MUSL deformation update.
+enum { kSlotP2G = 0, kSlotMUSL = 1, kSlotG2P = 2, kSlotDefgrad = 3, kTileSlots = 4 };
+// mark names that end each slot's kernel in a step
+const char* const kSlotMark[kTileSlots] = {"k_p2g", "k_g2p_musl", "k_g2p", "k_defgrad"};
+// largest block of each slot (k_g2p_t is register-bounded per 128 threads)
+const int kSlotMax[kTileSlots] = {kMaxTileThreads, kMaxTileThreads, kChunk, kMaxTileThreads};
+const int kTileCandidates[3] = {64, 128, 256};
+
+bool valid_tile_threads(const int* t) {
+  for (int i = 0; i < kTileSlots; ++i)
+    if (t[i] < 32 || t[i] > kSlotMax[i] || t[i] % 32 != 0) return false;
+  return true;
+}
+
 }  // namespace
 
 struct mtr_ctx {
@@ -107,11 +159,23 @@ struct mtr_ctx {
   int launches_per_step = 0;
   bool use_graphs = true;
   uint32_t step_limit = 0xffffffffu;  // mtr_set_step_limit: no step beyond this step count
-  // per-launch timing (mtr_profile): an event after every launch of a step
-  bool profiling = false;
-  std::vector<std::pair<const char*, cudaEvent_t>> marks;
-  std::vector<cudaEvent_t> event_pool;
-  size_t event_next = 0;
+  int tile_threads[kTileSlots] = {kChunk, kChunk, kChunk, kChunk};
+  // a trial step runs every kernel of a step but the commit (k_tail): the
+  // particle buffer it reads and the clock stay as they were
+  bool trial = false;
+  // per-launch timing (mtr_profile, mtr_autotune): an event after every launch of a step
+  EventMarks marks;
+  // frame output (mtr_frame_begin / mtr_frame_wait): rows built on the device
+  // behind the steps, copied to pinned host memory on a copy stream while the
+  // next steps run
+  double* frame_dev = nullptr;
+  double* frame_host = nullptr;
+  size_t frame_cap = 0;  // doubles in each
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t frame_ready = nullptr, frame_copied = nullptr;
+  bool frame_pending = false;
+  uint32_t frame_n = 0;
+  int frame_ncols = 0;
 };
 
 namespace {
@@ -191,24 +255,14 @@ void alloc_grid(mtr_ctx* c, const uint32_t want[3]) {
   c->passes = (int)((keybits + 7) / 8);
 }
 
-void mark(mtr_ctx* c, const char* name) {
-  if (!c->profiling) return;
-  if (c->event_next == c->event_pool.size()) {
-    cudaEvent_t e;
-    CK(cudaEventCreate(&e));
-    c->event_pool.push_back(e);
-  }
-  cudaEvent_t e = c->event_pool[c->event_next++];
-  CK(cudaEventRecord(e, c->stream));
-  c->marks.emplace_back(name, e);
-}
+void mark(mtr_ctx* c, const char* name) { c->marks.record(name, c->stream); }
 
 template <int D, int DEG, typename R>
 void set_kernel_attributes_t() {
   CK(cudaFuncSetAttribute(k_p2g_w<D, DEG, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)p2g_smem_bytes<D, R>()));
+                          (int)p2g_smem_bytes<D, R>(kMaxTileThreads)));
   CK(cudaFuncSetAttribute(k_g2p_musl_w<D, DEG, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)musl_smem_bytes<D, R>()));
+                          (int)musl_smem_bytes<D, R>(kMaxTileThreads)));
 }
 
 void set_kernel_attributes(bool fp32) {
@@ -284,29 +338,31 @@ int rm_specialization(int dim, bool musl, int pm) {
 }
 
 template <int D, int DEG, typename R>
-void launch_defgrad(int spm, uint32_t blocks, cudaStream_t st, const StepArgsT<R>& A, const uint32_t* perm) {
+void launch_defgrad(int spm, uint32_t blocks, int threads, cudaStream_t st, const StepArgsT<R>& A,
+                    const uint32_t* perm) {
   if constexpr (D == 3) {
     if (spm == MTR_PM_DPMUI) {
-      k_defgrad_t<D, DEG, R, MTR_PM_DPMUI><<<blocks, kChunk, 0, st>>>(A, perm);
+      k_defgrad_t<D, DEG, R, MTR_PM_DPMUI><<<blocks, threads, 0, st>>>(A, perm);
       return;
     }
   }
-  k_defgrad_t<D, DEG, R><<<blocks, kChunk, 0, st>>>(A, perm);
+  k_defgrad_t<D, DEG, R><<<blocks, threads, 0, st>>>(A, perm);
 }
 
 template <int D, int DEG, typename R>
-void launch_g2p(int spm, uint32_t blocks, cudaStream_t st, const StepArgsT<R>& A, const uint32_t* perm) {
+void launch_g2p(int spm, uint32_t blocks, int threads, cudaStream_t st, const StepArgsT<R>& A,
+                const uint32_t* perm) {
   if constexpr (D == 3) {
     if (spm == MTR_PM_DP) {
-      k_g2p_t<D, DEG, R, MTR_PM_DP><<<blocks, kChunk, 0, st>>>(A, perm);
+      k_g2p_t<D, DEG, R, MTR_PM_DP><<<blocks, threads, 0, st>>>(A, perm);
       return;
     }
     if (spm == MTR_PM_MCCVISC) {
-      k_g2p_t<D, DEG, R, MTR_PM_MCCVISC><<<blocks, kChunk, 0, st>>>(A, perm);
+      k_g2p_t<D, DEG, R, MTR_PM_MCCVISC><<<blocks, threads, 0, st>>>(A, perm);
       return;
     }
   }
-  k_g2p_t<D, DEG, R><<<blocks, kChunk, 0, st>>>(A, perm);
+  k_g2p_t<D, DEG, R><<<blocks, threads, 0, st>>>(A, perm);
 }
 
 template <int D, int DEG, typename R>
@@ -350,7 +406,8 @@ int enqueue_step_t(mtr_ctx* c, int parity) {
   k_tile_ranges<<<std::min<uint32_t>((c->Np + 255) / 256, 148 * 8), 256, 0, st>>>(A, skeys);
   ++n;
   mark(c, "k_tile_ranges");
-  k_p2g_w<D, DEG, R><<<c->cap_tiles, kChunk, p2g_smem_bytes<D, R>(), st>>>(A, perm);
+  const int* tt = c->tile_threads;
+  k_p2g_w<D, DEG, R><<<c->cap_tiles, tt[kSlotP2G], p2g_smem_bytes<D, R>(tt[kSlotP2G]), st>>>(A, perm);
   ++n;
   mark(c, "k_p2g");
   if (c->prm.pbc) {
@@ -365,21 +422,25 @@ int enqueue_step_t(mtr_ctx* c, int parity) {
   if (c->prm.use_musl) {
     CK(cudaMemsetAsync(c->v2, 0, sizeof(double) * D * c->cap_nodes, st));
     mark(c, "memset(v2)");
-    k_g2p_musl_w<D, DEG, R><<<c->cap_tiles, kChunk, musl_smem_bytes<D, R>(), st>>>(A, perm);
+    k_g2p_musl_w<D, DEG, R><<<c->cap_tiles, tt[kSlotMUSL], musl_smem_bytes<D, R>(tt[kSlotMUSL]), st>>>(A, perm);
     mark(c, "k_g2p_musl");
     k_musl_norm<D, R><<<gblocks, 256, 0, st>>>(A);
     mark(c, "k_musl_norm");
-    launch_defgrad<D, DEG, R>(rm_specialization(D, true, c->prm.plastic_model), c->cap_tiles, st, A, perm);
+    launch_defgrad<D, DEG, R>(rm_specialization(D, true, c->prm.plastic_model), c->cap_tiles, tt[kSlotDefgrad], st,
+                              A, perm);
     mark(c, "k_defgrad");
     n += 3;
   } else {
-    launch_g2p<D, DEG, R>(rm_specialization(D, false, c->prm.plastic_model), c->cap_tiles, st, A, perm);
+    launch_g2p<D, DEG, R>(rm_specialization(D, false, c->prm.plastic_model), c->cap_tiles, tt[kSlotG2P], st, A,
+                          perm);
     ++n;
     mark(c, "k_g2p");
   }
-  k_tail<D><<<1, 32, 0, st>>>(A, 1 - parity);
-  ++n;
-  mark(c, "k_tail");
+  if (!c->trial) {
+    k_tail<D><<<1, 32, 0, st>>>(A, 1 - parity);
+    ++n;
+    mark(c, "k_tail");
+  }
   CK(cudaGetLastError());
   return n;
 }
@@ -414,6 +475,46 @@ void build_graphs(mtr_ctx* c) {
     if (e != cudaSuccess) throw MtrError{MTR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)};
     c->launches_per_step = n / kGraphSteps;
   }
+}
+
+// Columns of the particle frame file (save_data.cpp:7-171) for these parameters.
+unsigned frame_columns(const mtr_params& p, std::vector<const char*>* names) {
+  static const char* const xs[3] = {"x", "y", "z"};
+  static const char* const vs[3] = {"vx", "vy", "vz"};
+  unsigned cols = 0;
+  const int pm = p.plastic_model;
+  if (pm != MTR_PM_NOPLASTICITY) cols |= kFramePlastic;
+  if (((pm == MTR_PM_DPVISC || pm == MTR_PM_MCCVISC) && p.use_mibf) || pm == MTR_PM_DPMUI || pm == MTR_PM_MCCMUI)
+    cols |= kFrameMuI;
+  if (pm == MTR_PM_DPMUI || pm == MTR_PM_MCCMUI) cols |= kFrameViscosity;
+  if (names) {
+    names->clear();
+    for (int a = 0; a < p.dim; ++a) names->push_back(xs[a]);
+    for (int a = 0; a < p.dim; ++a) names->push_back(vs[a]);
+    for (const char* n : {"p", "q", "Je"}) names->push_back(n);
+    if (cols & kFramePlastic)
+      for (const char* n : {"eps_pl_vol", "eps_pl_dev", "delta_gamma"}) names->push_back(n);
+    if (cols & kFrameMuI) names->push_back("muI");
+    if (cols & kFrameViscosity) names->push_back("viscosity");
+  }
+  return cols;
+}
+
+// The header kernel aborted a step because the grid outgrew its capacity
+// (H.N holds the extents it needed): reallocates the grid with 25% headroom and
+// clears the abort in the host copy of the header (the caller writes it back).
+void regrow_grid(mtr_ctx* c, StepHeader& H) {
+  uint32_t want[3];
+  for (int a = 0; a < 3; ++a)
+    want[a] = (a < c->dim) ? std::max<uint32_t>(c->cap_axis[a], (uint32_t)std::ceil(H.N[a] * 1.25 + 8.0)) : 1u;
+  for (int a = 0; a < c->dim; ++a)
+    if (H.N[a] >= kMaxAxisNodes || H.N[a] < 4)
+      throw MtrError{MTR_ERR_OOM, "grid extent exploded or collapsed (non-finite particle positions?)"};
+  free_graphs(c);
+  alloc_grid(c, want);
+  CK(cudaStreamSynchronize(c->stream));
+  H.abort = 0;
+  H.status &= ~MTR_STATUS_GRID_OVERFLOW;
 }
 
 void read_header(mtr_ctx* c) {
@@ -576,6 +677,7 @@ struct mtr_batch_group {
   void* dargs = nullptr;      // StepArgsT<R>[2][n]
   uint32_t* doff = nullptr;   // [kBK_KINDS][n + 1]
   uint32_t total[kBK_KINDS] = {};
+  int tile_threads[kTileSlots] = {kChunk, kChunk, kChunk, kChunk};
 };
 
 struct mtr_batch {
@@ -587,6 +689,8 @@ struct mtr_batch {
   bool dirty = true;
   int64_t launches_last = 0;
   int launches_per_step = 0;
+  bool trial = false;  // trial steps: no kb_tail (see mtr_ctx::trial)
+  EventMarks marks;    // tagged with the group index
 };
 
 namespace {
@@ -636,9 +740,10 @@ void build_group_tables(mtr_batch* b, mtr_batch_group& g) {
 }
 
 template <int D, int DEG, typename R>
-int enqueue_group_step_t(mtr_batch* b, mtr_batch_group& g) {
+int enqueue_group_step_t(mtr_batch* b, mtr_batch_group& g, int gi) {
   cudaStream_t st = b->stream;
   BatchView<R> B{(const StepArgsT<R>*)g.dargs, g.doff, (int)g.members.size()};
+  const int* tt = g.tile_threads;
   int n = 0;
   kb_bbox<D, R><<<g.total[kBK_BBOX], 256, 0, st>>>(B);
   kb_header<D, R><<<g.total[kBK_ONE], 32, 0, st>>>(B);
@@ -651,52 +756,73 @@ int enqueue_group_step_t(mtr_batch* b, mtr_batch_group& g) {
     n += 3;
   }
   kb_tile_ranges<R><<<g.total[kBK_TILES], 256, 0, st>>>(B);
-  kb_p2g_w<D, DEG, R><<<g.total[kBK_TILEK], kChunk, p2g_smem_bytes<D, R>(), st>>>(B);
+  b->marks.record("kb_tile_ranges", st, gi);
+  kb_p2g_w<D, DEG, R><<<g.total[kBK_TILEK], tt[kSlotP2G], p2g_smem_bytes<D, R>(tt[kSlotP2G]), st>>>(B);
+  b->marks.record(kSlotMark[kSlotP2G], st, gi);
   kb_grid<D, R><<<g.total[kBK_NODES], 256, 0, st>>>(B);
+  b->marks.record("kb_grid", st, gi);
   n += 3;
   if (g.musl) {
-    kb_g2p_musl_w<D, DEG, R><<<g.total[kBK_TILEK], kChunk, musl_smem_bytes<D, R>(), st>>>(B);
+    kb_g2p_musl_w<D, DEG, R><<<g.total[kBK_TILEK], tt[kSlotMUSL], musl_smem_bytes<D, R>(tt[kSlotMUSL]), st>>>(B);
+    b->marks.record(kSlotMark[kSlotMUSL], st, gi);
     kb_musl_norm<D, R><<<g.total[kBK_NODES], 256, 0, st>>>(B);
+    b->marks.record("kb_musl_norm", st, gi);
+    const int td = tt[kSlotDefgrad];
     if constexpr (D == 3) {
       if (g.spm == MTR_PM_DPMUI)
-        kb_defgrad_t<D, DEG, R, MTR_PM_DPMUI><<<g.total[kBK_TILEK], kChunk, 0, st>>>(B);
+        kb_defgrad_t<D, DEG, R, MTR_PM_DPMUI><<<g.total[kBK_TILEK], td, 0, st>>>(B);
       else
-        kb_defgrad_t<D, DEG, R><<<g.total[kBK_TILEK], kChunk, 0, st>>>(B);
+        kb_defgrad_t<D, DEG, R><<<g.total[kBK_TILEK], td, 0, st>>>(B);
     } else {
-      kb_defgrad_t<D, DEG, R><<<g.total[kBK_TILEK], kChunk, 0, st>>>(B);
+      kb_defgrad_t<D, DEG, R><<<g.total[kBK_TILEK], td, 0, st>>>(B);
     }
+    b->marks.record(kSlotMark[kSlotDefgrad], st, gi);
     n += 3;
   } else {
+    const int tg = tt[kSlotG2P];
     if constexpr (D == 3) {
       if (g.spm == MTR_PM_DP)
-        kb_g2p_t<D, DEG, R, MTR_PM_DP><<<g.total[kBK_TILEK], kChunk, 0, st>>>(B);
+        kb_g2p_t<D, DEG, R, MTR_PM_DP><<<g.total[kBK_TILEK], tg, 0, st>>>(B);
       else if (g.spm == MTR_PM_MCCVISC)
-        kb_g2p_t<D, DEG, R, MTR_PM_MCCVISC><<<g.total[kBK_TILEK], kChunk, 0, st>>>(B);
+        kb_g2p_t<D, DEG, R, MTR_PM_MCCVISC><<<g.total[kBK_TILEK], tg, 0, st>>>(B);
       else
-        kb_g2p_t<D, DEG, R><<<g.total[kBK_TILEK], kChunk, 0, st>>>(B);
+        kb_g2p_t<D, DEG, R><<<g.total[kBK_TILEK], tg, 0, st>>>(B);
     } else {
-      kb_g2p_t<D, DEG, R><<<g.total[kBK_TILEK], kChunk, 0, st>>>(B);
+      kb_g2p_t<D, DEG, R><<<g.total[kBK_TILEK], tg, 0, st>>>(B);
     }
+    b->marks.record(kSlotMark[kSlotG2P], st, gi);
     ++n;
   }
-  kb_tail<D, R><<<g.total[kBK_ONE], 32, 0, st>>>(B);
-  ++n;
+  if (!b->trial) {
+    kb_tail<D, R><<<g.total[kBK_ONE], 32, 0, st>>>(B);
+    ++n;
+  }
   CK(cudaGetLastError());
   return n;
 }
 
 template <typename R>
-int enqueue_group_step_r(mtr_batch* b, mtr_batch_group& g) {
-  if (g.dim == 3) return g.deg == 3 ? enqueue_group_step_t<3, 3, R>(b, g) : enqueue_group_step_t<3, 2, R>(b, g);
-  return g.deg == 3 ? enqueue_group_step_t<2, 3, R>(b, g) : enqueue_group_step_t<2, 2, R>(b, g);
+int enqueue_group_step_r(mtr_batch* b, mtr_batch_group& g, int gi) {
+  if (g.dim == 3)
+    return g.deg == 3 ? enqueue_group_step_t<3, 3, R>(b, g, gi) : enqueue_group_step_t<3, 2, R>(b, g, gi);
+  return g.deg == 3 ? enqueue_group_step_t<2, 3, R>(b, g, gi) : enqueue_group_step_t<2, 2, R>(b, g, gi);
+}
+
+int enqueue_batch_step(mtr_batch* b) {
+  int n = 0;
+  for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+    mtr_batch_group& g = b->groups[gi];
+    n += g.fp32 ? enqueue_group_step_r<float>(b, g, (int)gi) : enqueue_group_step_r<double>(b, g, (int)gi);
+  }
+  return n;
 }
 
 template <int D, int DEG, typename R>
 void set_batch_attributes_t() {
   CK(cudaFuncSetAttribute(kb_p2g_w<D, DEG, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)p2g_smem_bytes<D, R>()));
+                          (int)p2g_smem_bytes<D, R>(kMaxTileThreads)));
   CK(cudaFuncSetAttribute(kb_g2p_musl_w<D, DEG, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)musl_smem_bytes<D, R>()));
+                          (int)musl_smem_bytes<D, R>(kMaxTileThreads)));
 }
 
 void set_batch_attributes(const mtr_batch_group& g) {
@@ -725,8 +851,7 @@ void rebuild_batch(mtr_batch* b) {
   CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   int n = 0;
   try {
-    for (int s = 0; s < kBatchGraphSteps; ++s)
-      for (auto& g : b->groups) n += g.fp32 ? enqueue_group_step_r<float>(b, g) : enqueue_group_step_r<double>(b, g);
+    for (int s = 0; s < kBatchGraphSteps; ++s) n += enqueue_batch_step(b);
   } catch (...) {
     cudaStreamEndCapture(b->stream, &graph);
     if (graph) cudaGraphDestroy(graph);
@@ -752,6 +877,51 @@ void write_batch_headers(mtr_batch* b) {
     CK(cudaMemcpyAsync(c->dH, c->hH, sizeof(StepHeader), cudaMemcpyHostToDevice, b->stream));
   CK(cudaStreamSynchronize(b->stream));
 }
+
+// Block-shape tuning.  best[slot][k] is the shortest time seen for the slot's
+// kernel with candidate k (infinity: not measured).  A slot keeps `current`
+// unless another candidate was more than 2% faster, so timing noise does not
+// flip an equal choice.
+struct TuneTimes {
+  double best[kTileSlots][3];
+  TuneTimes() {
+    for (auto& r : best)
+      for (double& v : r) v = 1e300;
+  }
+  void add(const char* name, float ms, int k) {
+    for (int sl = 0; sl < kTileSlots; ++sl)
+      if (std::strcmp(name, kSlotMark[sl]) == 0) best[sl][k] = std::min(best[sl][k], (double)ms);
+  }
+  void choose(int* threads) const {
+    for (int sl = 0; sl < kTileSlots; ++sl) {
+      int cur = -1, arg = -1;
+      for (int k = 0; k < 3; ++k) {
+        if (kTileCandidates[k] > kSlotMax[sl] || best[sl][k] >= 1e300) continue;
+        if (kTileCandidates[k] == threads[sl]) cur = k;
+        if (arg < 0 || best[sl][k] < best[sl][arg]) arg = k;
+      }
+      if (arg < 0) continue;  // the slot's kernel does not run in this step
+      if (cur >= 0 && best[sl][cur] <= 1.02 * best[sl][arg]) continue;
+      threads[sl] = kTileCandidates[arg];
+    }
+  }
+};
+
+// the candidate shapes of round k for every slot
+void set_candidate(int* threads, int k) {
+  for (int sl = 0; sl < kTileSlots; ++sl) threads[sl] = std::min(kTileCandidates[k], kSlotMax[sl]);
+}
+
+// Restores flags changed for trial steps even when a step throws.
+struct TrialScope {
+  bool* trial;
+  bool* marks_on;
+  TrialScope(bool* t, bool* m) : trial(t), marks_on(m) {}
+  ~TrialScope() {
+    *trial = false;
+    *marks_on = false;
+  }
+};
 
 }  // namespace
 
@@ -998,16 +1168,7 @@ int mtr_step(mtr_ctx* c, int nsteps) {
       const int executed = (int)(H.step - step0) + ((H.status & kExitMask) && H.done ? 1 : 0);
       remaining -= executed;
       if (H.abort) {  // grid outgrew its capacity: regrow and resume
-        uint32_t want[3];
-        for (int a = 0; a < 3; ++a)
-          want[a] = (a < c->dim) ? std::max<uint32_t>(c->cap_axis[a], (uint32_t)std::ceil(H.N[a] * 1.25 + 8.0)) : 1u;
-        for (int a = 0; a < c->dim; ++a)
-          if (H.N[a] >= kMaxAxisNodes || H.N[a] < 4)
-            throw MtrError{MTR_ERR_OOM, "grid extent exploded or collapsed (non-finite particle positions?)"};
-        free_graphs(c);
-        alloc_grid(c, want);
-        H.abort = 0;
-        H.status &= ~MTR_STATUS_GRID_OVERFLOW;
+        regrow_grid(c, H);
         write_header(c);
         CK(cudaStreamSynchronize(c->stream));
         continue;
@@ -1267,31 +1428,27 @@ int mtr_profile(mtr_ctx* c, int nsteps, double* slot_ms, const char** slot_names
     int parity = c->hH->cur;
     std::vector<double> acc;
     std::vector<const char*> names;
-    c->profiling = true;
+    c->marks.on = true;
     int done_steps = 0;
     try {
       for (int s = 0; s < nsteps; ++s) {
-        c->marks.clear();
-        c->event_next = 0;
+        c->marks.reset();
         enqueue_step(c, parity);
         parity ^= 1;
         CK(cudaStreamSynchronize(c->stream));
+        const auto& L = c->marks.list;
         if (acc.empty()) {
-          acc.assign(c->marks.size() - 1, 0.0);
-          for (size_t i = 1; i < c->marks.size(); ++i) names.push_back(c->marks[i].first);
+          acc.assign(L.size() - 1, 0.0);
+          for (size_t i = 1; i < L.size(); ++i) names.push_back(L[i].first);
         }
-        for (size_t i = 1; i < c->marks.size() && i - 1 < acc.size(); ++i) {
-          float ms = 0.f;
-          CK(cudaEventElapsedTime(&ms, c->marks[i - 1].second, c->marks[i].second));
-          acc[i - 1] += ms;
-        }
+        for (size_t i = 1; i < L.size() && i - 1 < acc.size(); ++i) acc[i - 1] += c->marks.since_previous(i);
         ++done_steps;
       }
     } catch (...) {
-      c->profiling = false;
+      c->marks.on = false;
       throw;
     }
-    c->profiling = false;
+    c->marks.on = false;
     read_header(c);
     if (c->hH->abort) throw MtrError{MTR_ERR_STATE, "grid regrowth during profiling; step first"};
     *nslots = (int)acc.size();
@@ -1299,6 +1456,185 @@ int mtr_profile(mtr_ctx* c, int nsteps, double* slot_ms, const char** slot_names
       if (slot_ms) slot_ms[i] = acc[i] / done_steps;
       if (slot_names) slot_names[i] = names[i];
     }
+    return MTR_OK;
+  });
+}
+
+int mtr_frame_columns(mtr_ctx* c, const char** names, int max_names) {
+  if (!c) return MTR_ERR_INVALID;
+  std::vector<const char*> n;
+  frame_columns(c->prm, &n);
+  for (int i = 0; names && i < (int)n.size() && i < max_names; ++i) names[i] = n[i];
+  return (int)n.size();
+}
+
+int mtr_frame_begin(mtr_ctx* c) {
+  return guarded([&]() -> int {
+    if (!c || !c->uploaded) throw MtrError{MTR_ERR_STATE, "nothing uploaded"};
+    CK(cudaSetDevice(c->device));
+    if (!c->copy_stream) {
+      CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&c->frame_ready, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&c->frame_copied, cudaEventDisableTiming));
+    }
+    if (c->frame_pending) CK(cudaEventSynchronize(c->frame_copied));  // frame_dev is about to be rewritten
+    c->frame_pending = false;
+    std::vector<const char*> names;
+    const unsigned cols = frame_columns(c->prm, &names);
+    const int ncols = (int)names.size();
+    const size_t need = (size_t)c->Np * ncols + 8;
+    if (need > c->frame_cap) {
+      dfree(c->frame_dev);
+      if (c->frame_host) cudaFreeHost(c->frame_host);
+      c->frame_dev = nullptr;
+      c->frame_host = nullptr;
+      c->frame_cap = 0;
+      c->frame_dev = dalloc<double>(need);
+      void* h = nullptr;
+      if (cudaMallocHost(&h, sizeof(double) * need) != cudaSuccess) throw MtrError{MTR_ERR_OOM, "cudaMallocHost"};
+      c->frame_host = (double*)h;
+      c->frame_cap = need;
+    }
+    const uint32_t Np = c->Np, blocks = (Np + 255) / 256;
+    double* clock = c->frame_dev + (size_t)Np * ncols;
+    if (c->fp32) {
+      auto launch = [&](auto dimc) {
+        constexpr int D = decltype(dimc)::value;
+        k_frame_rows<D, float><<<blocks, 256, 0, c->stream>>>(typed<float>(c->buf[0]), typed<float>(c->buf[1]), c->dH,
+                                                               c->dP, Np, cols, (uint32_t)ncols, c->frame_dev, clock);
+      };
+      c->dim == 3 ? launch(std::integral_constant<int, 3>{}) : launch(std::integral_constant<int, 2>{});
+    } else {
+      auto launch = [&](auto dimc) {
+        constexpr int D = decltype(dimc)::value;
+        k_frame_rows<D, double><<<blocks, 256, 0, c->stream>>>(typed<double>(c->buf[0]), typed<double>(c->buf[1]),
+                                                                c->dH, c->dP, Np, cols, (uint32_t)ncols, c->frame_dev,
+                                                                clock);
+      };
+      c->dim == 3 ? launch(std::integral_constant<int, 3>{}) : launch(std::integral_constant<int, 2>{});
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->frame_ready, c->stream));
+    CK(cudaStreamWaitEvent(c->copy_stream, c->frame_ready, 0));
+    CK(cudaMemcpyAsync(c->frame_host, c->frame_dev, sizeof(double) * ((size_t)Np * ncols + 5), cudaMemcpyDeviceToHost,
+                       c->copy_stream));
+    CK(cudaEventRecord(c->frame_copied, c->copy_stream));
+    c->frame_pending = true;
+    c->frame_n = Np;
+    c->frame_ncols = ncols;
+    return MTR_OK;
+  });
+}
+
+int mtr_frame_wait(mtr_ctx* c, double timeout_seconds, const double** rows, uint32_t* n, int* ncols,
+                   mtr_clock* clock) {
+  return guarded([&]() -> int {
+    if (!c) throw MtrError{MTR_ERR_INVALID, "null context"};
+    if (!c->frame_pending) throw MtrError{MTR_ERR_STATE, "no frame snapshot in flight (mtr_frame_begin first)"};
+    CK(cudaSetDevice(c->device));
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+      const cudaError_t e = cudaEventQuery(c->frame_copied);
+      if (e == cudaSuccess) break;
+      if (e != cudaErrorNotReady) CK(e);
+      if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > timeout_seconds)
+        throw MtrError{MTR_ERR_TIMEOUT, "frame snapshot not copied within the timeout"};
+      std::this_thread::sleep_for(std::chrono::microseconds(200));
+    }
+    c->frame_pending = false;
+    const double* ck = c->frame_host + (size_t)c->frame_n * c->frame_ncols;
+    if (rows) *rows = c->frame_host;
+    if (n) *n = c->frame_n;
+    if (ncols) *ncols = c->frame_ncols;
+    if (clock) {
+      clock->time = ck[0];
+      clock->dt = ck[1];
+      clock->step = (uint32_t)ck[2];
+      clock->frame = (uint32_t)ck[3];
+      clock->done = (int32_t)ck[4];
+      clock->reserved = 0;
+    }
+    return MTR_OK;
+  });
+}
+
+int mtr_get_grid_friction(mtr_ctx* c, double* friction) {
+  return guarded([&]() -> int {
+    if (!c || !c->uploaded || !friction) throw MtrError{MTR_ERR_STATE, "nothing uploaded"};
+    if (!c->prm.use_mibf) throw MtrError{MTR_ERR_INVALID, "grid friction exists with use_mibf only"};
+    CK(cudaSetDevice(c->device));
+    read_header(c);
+    if (c->hH->G > c->cap_nodes) throw MtrError{MTR_ERR_STATE, "no completed step"};
+    get_nodes(c, friction, c->nfric, c->hH->G);
+    return MTR_OK;
+  });
+}
+
+int mtr_set_tile_threads(mtr_ctx* c, const int* threads) {
+  return guarded([&]() -> int {
+    if (!c || !threads) throw MtrError{MTR_ERR_INVALID, "null argument"};
+    if (!valid_tile_threads(threads)) throw MtrError{MTR_ERR_INVALID, "tile threads: multiples of 32, 32..256 (USL G2P: ..128)"};
+    CK(cudaSetDevice(c->device));
+    std::copy(threads, threads + kTileSlots, c->tile_threads);
+    free_graphs(c);
+    return MTR_OK;
+  });
+}
+
+int mtr_get_tile_threads(mtr_ctx* c, int* threads) {
+  if (!c || !threads) return MTR_ERR_INVALID;
+  std::copy(c->tile_threads, c->tile_threads + kTileSlots, threads);
+  return MTR_OK;
+}
+
+int mtr_autotune(mtr_ctx* c, int reps, int* threads) {
+  return guarded([&]() -> int {
+    if (!c || reps <= 0) throw MtrError{MTR_ERR_INVALID, "null context or reps <= 0"};
+    if (!c->uploaded) throw MtrError{MTR_ERR_STATE, "mtr_autotune before mtr_upload"};
+    CK(cudaSetDevice(c->device));
+    read_header(c);
+    StepHeader saved = *c->hH;
+    const bool active = !saved.done && saved.frame < saved.stop_frame && saved.step < saved.stop_step;
+    if (active) {
+      const int parity = saved.cur;
+      TrialScope scope(&c->trial, &c->marks.on);
+      // an untimed trial first; it also meets a grid overflow the next step would meet
+      bool ready = false;
+      for (int attempt = 0; attempt < 8 && !ready; ++attempt) {
+        c->trial = true;
+        enqueue_step(c, parity);
+        read_header(c);
+        if (c->hH->abort) {
+          regrow_grid(c, *c->hH);
+          *c->hH = saved;
+          write_header(c);
+          CK(cudaStreamSynchronize(c->stream));
+        } else {
+          ready = true;
+        }
+      }
+      if (!ready) throw MtrError{MTR_ERR_STATE, "grid kept growing during tuning"};
+      TuneTimes tt;
+      int chosen[kTileSlots];
+      std::copy(c->tile_threads, c->tile_threads + kTileSlots, chosen);
+      c->marks.on = true;
+      for (int r = 0; r < reps; ++r)
+        for (int k = 0; k < 3; ++k) {
+          set_candidate(c->tile_threads, k);
+          c->marks.reset();
+          enqueue_step(c, parity);
+          CK(cudaStreamSynchronize(c->stream));
+          const auto& L = c->marks.list;
+          for (size_t i = 1; i < L.size(); ++i) tt.add(L[i].first, c->marks.since_previous(i), k);
+        }
+      tt.choose(chosen);
+      std::copy(chosen, chosen + kTileSlots, c->tile_threads);
+      *c->hH = saved;  // the trial steps leave no trace: clock, plates, counters as before
+      write_header(c);
+      CK(cudaStreamSynchronize(c->stream));
+      free_graphs(c);
+    }
+    if (threads) std::copy(c->tile_threads, c->tile_threads + kTileSlots, threads);
     return MTR_OK;
   });
 }
@@ -1397,6 +1733,7 @@ int mtr_batch_create(mtr_ctx* const* ctxs, int n, mtr_batch** out) {
           g->fp32 = c->fp32;
           g->musl = musl;
           g->spm = spm;
+          std::copy(c->tile_threads, c->tile_threads + kTileSlots, g->tile_threads);
         }
         g->members.push_back(c);
       }
@@ -1439,17 +1776,7 @@ int mtr_batch_step(mtr_batch* b, int nsteps) {
       for (mtr_ctx* c : b->members) {
         StepHeader& H = *c->hH;
         if (!H.abort) continue;
-        uint32_t want[3];
-        for (int a = 0; a < 3; ++a)
-          want[a] = (a < c->dim) ? std::max<uint32_t>(c->cap_axis[a], (uint32_t)std::ceil(H.N[a] * 1.25 + 8.0)) : 1u;
-        for (int a = 0; a < c->dim; ++a)
-          if (H.N[a] >= kMaxAxisNodes || H.N[a] < 4)
-            throw MtrError{MTR_ERR_OOM, "grid extent exploded or collapsed (non-finite particle positions?)"};
-        free_graphs(c);
-        alloc_grid(c, want);
-        CK(cudaStreamSynchronize(c->stream));
-        H.abort = 0;
-        H.status &= ~MTR_STATUS_GRID_OVERFLOW;
+        regrow_grid(c, H);
         regrown = true;
       }
       if (regrown) {
@@ -1463,6 +1790,102 @@ int mtr_batch_step(mtr_batch* b, int nsteps) {
     }
     write_batch_headers(b);
     b->launches_last = launches;
+    return MTR_OK;
+  });
+}
+
+int mtr_batch_groups(mtr_batch* b) { return b ? (int)b->groups.size() : MTR_ERR_INVALID; }
+
+int mtr_batch_get_group(mtr_batch* b, int group, mtr_group_info* info) {
+  if (!b || !info || group < 0 || group >= (int)b->groups.size()) return MTR_ERR_INVALID;
+  const mtr_batch_group& g = b->groups[group];
+  info->dim = g.dim;
+  info->spline_deg = g.deg;
+  info->fp32 = g.fp32 ? 1 : 0;
+  info->musl = g.musl;
+  info->plastic_model_kernel = g.spm;
+  info->members = (int)g.members.size();
+  std::copy(g.tile_threads, g.tile_threads + kTileSlots, info->tile_threads);
+  return MTR_OK;
+}
+
+int mtr_batch_set_tile_threads(mtr_batch* b, int group, const int* threads) {
+  return guarded([&]() -> int {
+    if (!b || !threads || group < 0 || group >= (int)b->groups.size()) throw MtrError{MTR_ERR_INVALID, "bad group"};
+    if (!valid_tile_threads(threads)) throw MtrError{MTR_ERR_INVALID, "tile threads: multiples of 32, 32..256 (USL G2P: ..128)"};
+    std::copy(threads, threads + kTileSlots, b->groups[group].tile_threads);
+    b->dirty = true;
+    return MTR_OK;
+  });
+}
+
+int mtr_batch_autotune(mtr_batch* b, int reps) {
+  return guarded([&]() -> int {
+    if (!b || reps <= 0) throw MtrError{MTR_ERR_INVALID, "null batch or reps <= 0"};
+    CK(cudaSetDevice(b->device));
+    if (b->dirty || !b->graph) rebuild_batch(b);
+    read_batch_headers(b);
+    std::vector<StepHeader> saved;
+    bool any = false;
+    for (mtr_ctx* c : b->members) {
+      saved.push_back(*c->hH);
+      StepHeader& H = *c->hH;
+      // one step of every member that still runs; the others stay inactive
+      const bool run = !H.done && H.frame < H.stop_frame && H.step < c->step_limit;
+      H.stop_step = run ? H.step + 1 : H.step;
+      any = any || run;
+    }
+    std::vector<StepHeader> trial_headers;
+    for (mtr_ctx* c : b->members) trial_headers.push_back(*c->hH);
+    write_batch_headers(b);
+    if (any) {
+      TrialScope scope(&b->trial, &b->marks.on);
+      bool ready = false;
+      for (int attempt = 0; attempt < 8 && !ready; ++attempt) {
+        b->trial = true;
+        enqueue_batch_step(b);
+        b->trial = false;
+        read_batch_headers(b);
+        bool regrown = false;
+        for (size_t i = 0; i < b->members.size(); ++i) {
+          mtr_ctx* c = b->members[i];
+          if (!c->hH->abort) continue;
+          regrow_grid(c, *c->hH);
+          regrown = true;
+        }
+        if (regrown) {
+          for (size_t i = 0; i < b->members.size(); ++i) *b->members[i]->hH = trial_headers[i];
+          write_batch_headers(b);
+          rebuild_batch(b);
+        } else {
+          ready = true;
+        }
+      }
+      if (!ready) throw MtrError{MTR_ERR_STATE, "grid kept growing during tuning"};
+      std::vector<TuneTimes> tt(b->groups.size());
+      std::vector<std::vector<int>> chosen;
+      for (auto& g : b->groups) chosen.emplace_back(g.tile_threads, g.tile_threads + kTileSlots);
+      b->marks.on = true;
+      b->trial = true;
+      for (int r = 0; r < reps; ++r)
+        for (int k = 0; k < 3; ++k) {
+          for (auto& g : b->groups) set_candidate(g.tile_threads, k);
+          b->marks.reset();
+          b->marks.record("start", b->stream, -1);
+          enqueue_batch_step(b);
+          CK(cudaStreamSynchronize(b->stream));
+          const auto& L = b->marks.list;
+          for (size_t i = 1; i < L.size(); ++i)
+            if (b->marks.tag[i] == b->marks.tag[i - 1]) tt[b->marks.tag[i]].add(L[i].first, b->marks.since_previous(i), k);
+        }
+      for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+        tt[gi].choose(chosen[gi].data());
+        std::copy(chosen[gi].begin(), chosen[gi].end(), b->groups[gi].tile_threads);
+      }
+    }
+    for (size_t i = 0; i < b->members.size(); ++i) *b->members[i]->hH = saved[i];
+    write_batch_headers(b);
+    b->dirty = true;
     return MTR_OK;
   });
 }
@@ -1484,9 +1907,16 @@ void mtr_ctx_destroy(mtr_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->copy_stream) {
+    cudaStreamSynchronize(c->copy_stream);
+    cudaStreamDestroy(c->copy_stream);
+    cudaEventDestroy(c->frame_ready);
+    cudaEventDestroy(c->frame_copied);
+  }
+  dfree(c->frame_dev);
+  if (c->frame_host) cudaFreeHost(c->frame_host);
   free_graphs(c);
   free_grid(c);
-  for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
   for (void* p : c->pallocs) dfree(p);
   for (void* p : {(void*)c->keys0, (void*)c->keysA, (void*)c->valsA, (void*)c->keysB, (void*)c->valsB,
                   (void*)c->hist, (void*)c->dtot, (void*)c->partials, (void*)c->staging, (void*)c->dP, (void*)c->dH})

@@ -625,7 +625,8 @@ __device__ __forceinline__ bool patch_node(const StepHeader* H, const int (&n0)[
 // ---------------------------------------------------------------------------
 // 5. P2G + stress force, warp-cooperative, one block per tile.
 //
-// A tile block walks its sorted particles in chunks of kChunk.  Phase 1, one
+// A tile block walks its sorted particles in chunks of blockDim.x (64, 128 or
+// 256 threads, chosen per scene at run time by measurement).  Phase 1, one
 // thread per particle, loads the particle and stages its stencil weights and
 // gradients in shared memory.  Phase 2: lane groups (3D: 16 lanes, 2D: 4 lanes)
 // take consecutive staged particles; a lane owns one stencil column of the
@@ -637,19 +638,25 @@ __device__ __forceinline__ bool patch_node(const StepHeader* H, const int (&n0)[
 // a group on one address.  The patch is flushed with one global atomic per
 // node and channel.
 // ---------------------------------------------------------------------------
-constexpr int kChunk = 128;
+constexpr int kChunk = 128;  // default block size of the tile kernels
+// Largest block of the tile kernels.  The scatter kernels stage one particle
+// per thread, so their shared memory grows with the block; k_g2p_t stays at
+// kChunk threads at most (its register bound below is per 128-thread block).
+constexpr int kMaxTileThreads = 256;
 
-// Minimum resident blocks per SM requested for the tile kernels that run the
-// return mapping; it bounds their registers per thread.  Four blocks of 128
-// threads (128 registers, some spilled to L1) measured 15-25% faster for
-// k_defgrad_t than the unbounded two blocks (240 registers) on the 3D collapse;
-// three blocks measured best for k_g2p_t on the 3D Cam-Clay incline.
+// Minimum resident blocks of 128 threads per SM requested for the tile kernels
+// that run the return mapping; it bounds their registers per thread.  Four
+// blocks of 128 threads (128 registers, some spilled to L1) measured 15-25%
+// faster for k_defgrad_t than the unbounded two blocks (240 registers) on the
+// 3D collapse; three blocks measured best for k_g2p_t on the 3D Cam-Clay incline.
 #ifndef MTR_DEFGRAD_MIN_BLOCKS
 #define MTR_DEFGRAD_MIN_BLOCKS 4
 #endif
 #ifndef MTR_G2P_MIN_BLOCKS
 #define MTR_G2P_MIN_BLOCKS 3
 #endif
+// the same register bound for blocks of up to kMaxTileThreads threads
+#define MTR_DEFGRAD_BOUNDS kMaxTileThreads, (MTR_DEFGRAD_MIN_BLOCKS * kChunk / kMaxTileThreads)
 
 // FP64 stage: the position is kept and node offsets are formed in phase 2.
 template <int D, typename R = double>
@@ -687,8 +694,8 @@ constexpr size_t p2g_patch_bytes() {
   return align16(sizeof(R) * Tiling<D>::NCH * Tiling<D>::NODES);
 }
 template <int D, typename R>
-constexpr size_t p2g_smem_bytes() {
-  return p2g_crd_bytes<D, R>() + p2g_patch_bytes<D, R>() + sizeof(PStage<D, R>) * kChunk;
+constexpr size_t p2g_smem_bytes(int threads) {
+  return p2g_crd_bytes<D, R>() + p2g_patch_bytes<D, R>() + sizeof(PStage<D, R>) * (size_t)threads;
 }
 
 template <int D, int DEG, typename R>
@@ -733,7 +740,7 @@ __device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t
   // meet on one patch node (interleaving them made both groups flush the same
   // cell at once, which measured slower despite fewer bank conflicts)
   const int kbeg = warp * 32 + (lane / LPP) * LPP, kend = kbeg + LPP;
-  for (uint32_t c0 = pb; c0 < pe; c0 += kChunk) {
+  for (uint32_t c0 = pb; c0 < pe; c0 += blockDim.x) {
     {  // phase 1: stage one particle per thread
       const uint32_t s = c0 + threadIdx.x;
       PStage<D, R>& S = st[threadIdx.x];
@@ -880,7 +887,7 @@ __device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t
 }
 
 template <int D, int DEG, typename R>
-__global__ void __launch_bounds__(kChunk) k_p2g_w(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
+__global__ void __launch_bounds__(kMaxTileThreads) k_p2g_w(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
   p2g_w_body<D, DEG, R>(A, perm, blockIdx.x, gridDim.x);
 }
 
@@ -1433,8 +1440,8 @@ constexpr size_t musl_patch_bytes() {
   return align16(sizeof(R) * 3 * D * Tiling<D>::NODES);
 }
 template <int D, typename R>
-constexpr size_t musl_smem_bytes() {
-  return musl_crd_bytes<D, R>() + musl_patch_bytes<D, R>() + sizeof(MStage<D, R>) * kChunk;
+constexpr size_t musl_smem_bytes(int threads) {
+  return musl_crd_bytes<D, R>() + musl_patch_bytes<D, R>() + sizeof(MStage<D, R>) * (size_t)threads;
 }
 
 template <int D, int DEG, typename R>
@@ -1473,7 +1480,7 @@ __device__ __forceinline__ void g2p_musl_w_body(const StepArgsT<R>& A, const uin
   const int iz = D == 3 ? (q & 3) : 0;
   // consecutive particles per lane group, as in k_p2g_w
   const int kbeg = warp * 32 + (lane / LPP) * LPP, kend = kbeg + LPP;
-  for (uint32_t c0 = pb; c0 < pe; c0 += kChunk) {
+  for (uint32_t c0 = pb; c0 < pe; c0 += blockDim.x) {
     {  // phase 1
       const uint32_t s = c0 + threadIdx.x;
       MStage<D, R>& S = st[threadIdx.x];
@@ -1623,7 +1630,7 @@ __device__ __forceinline__ void g2p_musl_w_body(const StepArgsT<R>& A, const uin
 }
 
 template <int D, int DEG, typename R>
-__global__ void __launch_bounds__(kChunk) k_g2p_musl_w(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
+__global__ void __launch_bounds__(kMaxTileThreads) k_g2p_musl_w(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
   g2p_musl_w_body<D, DEG, R>(A, perm, blockIdx.x, gridDim.x);
 }
 
@@ -1698,7 +1705,7 @@ __device__ __forceinline__ void defgrad_t_body(const StepArgsT<R>& A, const uint
 }
 
 template <int D, int DEG, typename R, int PM = -1>
-__global__ void __launch_bounds__(kChunk, MTR_DEFGRAD_MIN_BLOCKS) k_defgrad_t(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
+__global__ void __launch_bounds__(MTR_DEFGRAD_BOUNDS) k_defgrad_t(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
   defgrad_t_body<D, DEG, R, PM>(A, perm, blockIdx.x, gridDim.x);
 }
 
@@ -1856,7 +1863,7 @@ __global__ void __launch_bounds__(256) kb_tile_ranges(BatchView<R> B) {
 }
 
 template <int D, int DEG, typename R>
-__global__ void __launch_bounds__(kChunk) kb_p2g_w(BatchView<R> B) {
+__global__ void __launch_bounds__(kMaxTileThreads) kb_p2g_w(BatchView<R> B) {
   uint32_t b, nb;
   const StepArgsT<R>* A = batch_locate(B, kBK_TILEK, b, nb);
   if (A) p2g_w_body<D, DEG, R>(*A, A->perm, b, nb);
@@ -1877,7 +1884,7 @@ __global__ void __launch_bounds__(kChunk, MTR_G2P_MIN_BLOCKS) kb_g2p_t(BatchView
 }
 
 template <int D, int DEG, typename R>
-__global__ void __launch_bounds__(kChunk) kb_g2p_musl_w(BatchView<R> B) {
+__global__ void __launch_bounds__(kMaxTileThreads) kb_g2p_musl_w(BatchView<R> B) {
   uint32_t b, nb;
   const StepArgsT<R>* A = batch_locate(B, kBK_TILEK, b, nb);
   if (A) g2p_musl_w_body<D, DEG, R>(*A, A->perm, b, nb);
@@ -1891,7 +1898,7 @@ __global__ void __launch_bounds__(256) kb_musl_norm(BatchView<R> B) {
 }
 
 template <int D, int DEG, typename R, int PM = -1>
-__global__ void __launch_bounds__(kChunk, MTR_DEFGRAD_MIN_BLOCKS) kb_defgrad_t(BatchView<R> B) {
+__global__ void __launch_bounds__(MTR_DEFGRAD_BOUNDS) kb_defgrad_t(BatchView<R> B) {
   uint32_t b, nb;
   const StepArgsT<R>* A = batch_locate(B, kBK_TILEK, b, nb);
   if (A) defgrad_t_body<D, DEG, R, PM>(*A, A->perm, b, nb);
@@ -1965,6 +1972,83 @@ __global__ void k_soa_to_aos(uint32_t Np, const R* __restrict__ src, const uint3
 #pragma unroll
     for (int q = 0; q < MTR_NUM_SCALARS; ++q) dst[(size_t)i * MTR_NUM_SCALARS + q] = src[(size_t)q * Np + s];
   }
+}
+
+// ---------------------------------------------------------------------------
+// Frame output (Simulation::saveParticleData, save_data.cpp:7-171): one row of
+// FP64 columns per particle, in the original particle order, with the
+// columns and their order of the reference's particle file:
+//   x[D], v[D], p, q, Je,
+//   eps_pl_vol, eps_pl_dev, delta_gamma   (kFrameCols & kFramePlastic)
+//   muI                                    (kFrameCols & kFrameMuI)
+//   viscosity                              (kFrameCols & kFrameViscosity)
+// p = -tr(tau)/D, q = sqrt(c tau_dev : tau_dev) with c = 3/2 (use_mises_q) or
+// 1/2, Je = det F (save_data.cpp:14-35).  tau is the particle's carried
+// Kirchhoff stress, which the step computes from the final F exactly as
+// HenckyPiola(F) F^T / NeoHookeanPiola(F) F^T.  The particle buffer read is
+// the current one of the header (H->cur), so the kernel can be enqueued
+// behind any number of steps.  The clock of the snapshot goes to clock[0..4]:
+// time, dt, step, frame, done.
+// ---------------------------------------------------------------------------
+enum : unsigned { kFramePlastic = 1u, kFrameMuI = 2u, kFrameViscosity = 4u };
+
+template <int D, typename R>
+__global__ void __launch_bounds__(256) k_frame_rows(PBufT<R> b0, PBufT<R> b1, const StepHeader* __restrict__ H,
+                                                    const DevParams* __restrict__ P, uint32_t Np, unsigned cols,
+                                                    uint32_t ncols, double* __restrict__ rows,
+                                                    double* __restrict__ clock) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s == 0) {
+    clock[0] = H->time;
+    clock[1] = H->dt;
+    clock[2] = (double)H->step;
+    clock[3] = (double)H->frame;
+    clock[4] = (double)H->done;
+  }
+  if (s >= Np) return;
+  const PBufT<R>& b = H->cur ? b1 : b0;
+  constexpr int NS = Sym<D>::n;
+  PLoad<D> p;
+  load_particle<D, R>(b, Np, s, p);
+  double tau[NS];
+#pragma unroll
+  for (int q = 0; q < NS; ++q) tau[q] = (double)b.tau[(size_t)q * Np + s];
+  double tr = 0.0;
+#pragma unroll
+  for (int a = 0; a < D; ++a) tr += tau[a];
+  const double pressure = -tr / D;
+  double dd = 0.0;
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      const double t = sym_at<D>(tau, i, j) + (i == j ? pressure : 0.0);
+      dd += t * t;
+    }
+  const double q = sqrt((P->use_mises_q ? 1.5 : 0.5) * dd);
+  const double(&F)[D][D] = p.F;
+  double Je;
+  if constexpr (D == 3)
+    Je = F[0][0] * (F[1][1] * F[2][2] - F[2][1] * F[1][2]) - F[1][0] * (F[0][1] * F[2][2] - F[2][1] * F[0][2]) +
+         F[2][0] * (F[0][1] * F[1][2] - F[1][1] * F[0][2]);
+  else
+    Je = F[0][0] * F[1][1] - F[1][0] * F[0][1];
+  double* row = rows + (size_t)p.id * ncols;
+  int c = 0;
+#pragma unroll
+  for (int a = 0; a < D; ++a) row[c++] = p.x[a];
+#pragma unroll
+  for (int a = 0; a < D; ++a) row[c++] = p.v[a];
+  row[c++] = pressure;
+  row[c++] = q;
+  row[c++] = Je;
+  if (cols & kFramePlastic) {
+    row[c++] = p.s.eps_pl_vol;
+    row[c++] = p.s.eps_pl_dev;
+    row[c++] = (double)b.sc[(size_t)MTR_SCALAR_DELTA_GAMMA * Np + s];
+  }
+  if (cols & kFrameMuI) row[c++] = p.s.muI;
+  if (cols & kFrameViscosity) row[c++] = p.s.viscosity;
 }
 
 // node array of type R -> FP64 (grid read-back of the FP32 path)

@@ -8,7 +8,7 @@ import os
 
 import numpy as np
 
-from .abi import MtrClock, MtrObject, MtrParams, MtrPlate, ERROR_NAMES, MTR_OK, SCALARS
+from .abi import MtrClock, MtrGroupInfo, MtrObject, MtrParams, MtrPlate, ERROR_NAMES, MTR_OK, SCALARS, TILE_SLOTS
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmatter_gpu.so")
@@ -24,6 +24,9 @@ EXPORTS = (
     "mtr_use_graphs", "mtr_profile", "mtr_active_nodes", "mtr_balance", "mtr_set_step_limit",
     "mtr_batch_create", "mtr_batch_step", "mtr_batch_launch_count", "mtr_batch_stream", "mtr_batch_destroy",
     "mtr_footprint", "mtr_ctx_destroy", "mtr_last_error", "mtr_p2g_noalloc",
+    "mtr_autotune", "mtr_set_tile_threads", "mtr_get_tile_threads", "mtr_batch_autotune", "mtr_batch_groups",
+    "mtr_batch_get_group", "mtr_batch_set_tile_threads", "mtr_frame_columns", "mtr_frame_begin",
+    "mtr_frame_wait", "mtr_get_grid_friction",
 )
 
 _lib = None
@@ -80,6 +83,19 @@ def load_library(path=LIB_PATH):
     lib.mtr_p2g_noalloc.argtypes = [C.POINTER(MtrParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                     C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32), C.c_void_p,
                                     C.c_void_p, C.c_void_p]
+    _I4 = C.POINTER(C.c_int)
+    lib.mtr_autotune.argtypes = [C.c_void_p, C.c_int, _I4]
+    lib.mtr_set_tile_threads.argtypes = [C.c_void_p, _I4]
+    lib.mtr_get_tile_threads.argtypes = [C.c_void_p, _I4]
+    lib.mtr_batch_autotune.argtypes = [C.c_void_p, C.c_int]
+    lib.mtr_batch_groups.argtypes = [C.c_void_p]
+    lib.mtr_batch_get_group.argtypes = [C.c_void_p, C.c_int, C.POINTER(MtrGroupInfo)]
+    lib.mtr_batch_set_tile_threads.argtypes = [C.c_void_p, C.c_int, _I4]
+    lib.mtr_frame_columns.argtypes = [C.c_void_p, C.POINTER(C.c_char_p), C.c_int]
+    lib.mtr_frame_begin.argtypes = [C.c_void_p]
+    lib.mtr_frame_wait.argtypes = [C.c_void_p, C.c_double, C.POINTER(_P), C.POINTER(C.c_uint32),
+                                   C.POINTER(C.c_int), C.POINTER(MtrClock)]
+    lib.mtr_get_grid_friction.argtypes = [C.c_void_p, _P]
     lib.mtr_ctx_destroy.argtypes = [C.c_void_p]
     lib.mtr_ctx_destroy.restype = None
     lib.mtr_last_error.restype = C.c_char_p
@@ -141,6 +157,27 @@ class GpuSim:
 
     def use_graphs(self, on=True):
         _check(self.lib, "mtr_use_graphs", self.lib.mtr_use_graphs(self.h, 1 if on else 0))
+
+    # -- block shapes of the tile kernels ---------------------------------
+    def autotune(self, reps=3):
+        """Times trial steps with 64, 128 and 256 threads per tile block and
+        keeps the fastest per kernel (mtr_autotune); returns {slot: threads}."""
+        t = (C.c_int * 4)()
+        _check(self.lib, "mtr_autotune", self.lib.mtr_autotune(self.h, int(reps), t))
+        return dict(zip(TILE_SLOTS, list(t)))
+
+    @property
+    def tile_threads(self):
+        t = (C.c_int * 4)()
+        _check(self.lib, "mtr_get_tile_threads", self.lib.mtr_get_tile_threads(self.h, t))
+        return dict(zip(TILE_SLOTS, list(t)))
+
+    @tile_threads.setter
+    def tile_threads(self, shapes):
+        cur = self.tile_threads
+        cur.update(shapes)
+        t = (C.c_int * 4)(*[cur[k] for k in TILE_SLOTS])
+        _check(self.lib, "mtr_set_tile_threads", self.lib.mtr_set_tile_threads(self.h, t))
 
     # -- stepping -------------------------------------------------------
     def step(self, n=1, check=True):
@@ -218,6 +255,33 @@ class GpuSim:
         return {"dims": (nx, ny, nz), "x": gx, "y": gy, "z": gz, "mass": m, "v": v.reshape(G, d),
                 "flip": fl.reshape(G, d)}
 
+    # -- frame output -----------------------------------------------------
+    def frame_columns(self):
+        names = (C.c_char_p * 32)()
+        n = self.lib.mtr_frame_columns(self.h, names, 32)
+        if n < 0:
+            _check(self.lib, "mtr_frame_columns", n)
+        return [names[i].decode() for i in range(n)]
+
+    def frame_begin(self):
+        """Snapshot of the particle file's rows behind the issued steps (mtr_frame_begin)."""
+        _check(self.lib, "mtr_frame_begin", self.lib.mtr_frame_begin(self.h))
+
+    def frame_wait(self, timeout=600.0):
+        """(rows [Np, ncols] copied out of the pinned buffer, column names, clock)."""
+        rows, n, nc, ck = _P(), C.c_uint32(), C.c_int(), MtrClock()
+        _check(self.lib, "mtr_frame_wait", self.lib.mtr_frame_wait(self.h, timeout, C.byref(rows), C.byref(n),
+                                                                   C.byref(nc), C.byref(ck)))
+        a = np.ctypeslib.as_array(rows, shape=(n.value * nc.value,)).reshape(n.value, nc.value).copy()
+        return a, self.frame_columns(), {"time": ck.time, "dt": ck.dt, "step": ck.step, "frame": ck.frame,
+                                         "done": ck.done}
+
+    def grid_friction(self):
+        G = int(np.prod(self.grid()["dims"]))
+        out = np.zeros(G)
+        _check(self.lib, "mtr_get_grid_friction", self.lib.mtr_get_grid_friction(self.h, _ptr(out)))
+        return out
+
     def sort_state(self):
         n = self.Np
         keys, perm, ids = (np.zeros(n, dtype=np.uint32) for _ in range(3))
@@ -279,6 +343,28 @@ class GpuBatch:
 
     def launch_count(self):
         return self.lib.mtr_batch_launch_count(self.h)
+
+    def autotune(self, reps=3):
+        """mtr_batch_autotune; returns groups()."""
+        _check(self.lib, "mtr_batch_autotune", self.lib.mtr_batch_autotune(self.h, int(reps)))
+        return self.groups()
+
+    def groups(self):
+        """Each group's key, member count and tile-kernel block shapes."""
+        out = []
+        for g in range(self.lib.mtr_batch_groups(self.h)):
+            info = MtrGroupInfo()
+            _check(self.lib, "mtr_batch_get_group", self.lib.mtr_batch_get_group(self.h, g, C.byref(info)))
+            out.append({"dim": info.dim, "spline_deg": info.spline_deg, "fp32": bool(info.fp32),
+                        "musl": bool(info.musl), "plastic_model_kernel": info.plastic_model_kernel,
+                        "members": info.members, "tile_threads": dict(zip(TILE_SLOTS, list(info.tile_threads)))})
+        return out
+
+    def set_tile_threads(self, group, shapes):
+        cur = self.groups()[group]["tile_threads"]
+        cur.update(shapes)
+        t = (C.c_int * 4)(*[cur[k] for k in TILE_SLOTS])
+        _check(self.lib, "mtr_batch_set_tile_threads", self.lib.mtr_batch_set_tile_threads(self.h, group, t))
 
     def close(self):
         if getattr(self, "h", None):

@@ -86,6 +86,7 @@ const char* status_text(uint32_t f) {
 Simulation::Simulation() {}
 
 Simulation::~Simulation() {
+  finish_frame_output();
   if (ctx_) mtr_ctx_destroy(ctx_);
 }
 
@@ -367,6 +368,7 @@ void Simulation::simulate() {
     int frame_done = 0;
     const int rc = mtr_run_frame(ctx_, &frame_done);
     if (rc != MTR_OK) {
+      finish_frame_output();
       report_device_error(rc, "step");
       download_state();
       return;
@@ -380,21 +382,20 @@ void Simulation::simulate() {
     if (frame_done) {
       std::cout << "End of frame " << frame << std::endl;
       if (save_sim) {
-        download_state();
-        saveParticleData();
         if (save_grid) saveGridData();
+        save_frame_async();
       }
     }
     if (ck.done) {
       std::cout << "The simulation ended at time = " << time << std::endl;
       if (save_sim) {
-        download_state();
-        saveParticleData();
         if (save_grid) saveGridData();
+        save_frame_async();
       }
       break;
     }
   }
+  finish_frame_output();
   const auto end = std::chrono::steady_clock::now();
   runtime_total = std::chrono::duration_cast<std::chrono::milliseconds>(end - begin).count();
   download_state();
@@ -503,21 +504,69 @@ void Simulation::saveAvgData() {
   f3 << J << "\n";
 }
 
-// Binary little-endian PLY writer (the reference writes the same properties
-// through tinyply, save_data.cpp:7-171).
+// Binary little-endian PLY files with one `vertex` element of FP64
+// properties, one row per vertex: the layout the reference writes through
+// tinyply (save_data.cpp:7-171), with its property names and order.
 namespace {
+void write_ply_header(std::ofstream& out, size_t n, const std::vector<std::string>& names) {
+  out << "ply\nformat binary_little_endian 1.0\nelement vertex " << n << "\n";
+  for (const auto& c : names) out << "property double " << c << "\n";
+  out << "end_header\n";
+}
+
 void write_ply(const std::string& path, size_t n, const std::vector<std::pair<std::string, const double*>>& cols) {
   std::ofstream out(path, std::ios::binary);
-  out << "ply\nformat binary_little_endian 1.0\nelement vertex " << n << "\n";
-  for (const auto& c : cols) out << "property double " << c.first << "\n";
-  out << "end_header\n";
+  std::vector<std::string> names;
+  for (const auto& c : cols) names.push_back(c.first);
+  write_ply_header(out, n, names);
   std::vector<double> row(cols.size());
   for (size_t i = 0; i < n; ++i) {
     for (size_t k = 0; k < cols.size(); ++k) row[k] = cols[k].second[i];
     out.write(reinterpret_cast<const char*>(row.data()), sizeof(double) * row.size());
   }
 }
+
+// rows: n rows of names.size() doubles, already in file order
+void write_ply_rows(const std::string& path, size_t n, const std::vector<std::string>& names, const double* rows) {
+  std::ofstream out(path, std::ios::binary);
+  write_ply_header(out, n, names);
+  out.write(reinterpret_cast<const char*>(rows), (std::streamsize)(sizeof(double) * n * names.size()));
+}
 }  // namespace
+
+// Snapshot of the particle file's rows, taken on the GPU behind the frame's
+// steps (mtr_frame_begin); a writer thread waits for the copy and writes the
+// file while the next frame steps.  At most one file is in flight.
+void Simulation::save_frame_async() {
+  finish_frame_output();
+  const int rc = mtr_frame_begin(ctx_);
+  if (rc != MTR_OK) {
+    report_device_error(rc, "mtr_frame_begin");
+    return;
+  }
+  const std::string path = directory + sim_name + "/particles_f" + std::to_string(frame) + ".ply";
+  const std::string marker = directory + sim_name + "/last_written.txt";
+  const unsigned int f = frame;
+  mtr_ctx* ctx = ctx_;
+  frame_writer_ = std::thread([ctx, path, marker, f]() {
+    const double* rows = nullptr;
+    uint32_t n = 0;
+    int ncols = 0;
+    mtr_clock ck;
+    if (mtr_frame_wait(ctx, 3600.0, &rows, &n, &ncols, &ck) != MTR_OK) {
+      std::cerr << "frame " << f << " not written: " << mtr_last_error() << std::endl;
+      return;
+    }
+    std::vector<const char*> cn(ncols);
+    mtr_frame_columns(ctx, cn.data(), ncols);
+    write_ply_rows(path, n, std::vector<std::string>(cn.begin(), cn.end()), rows);
+    std::ofstream(marker) << f << "\n";
+  });
+}
+
+void Simulation::finish_frame_output() {
+  if (frame_writer_.joinable()) frame_writer_.join();
+}
 
 void Simulation::saveParticleData(std::string extra) {
   const size_t n = Np;
@@ -540,20 +589,24 @@ void Simulation::saveParticleData(std::string extra) {
     dev[p] = std::sqrt((use_mises_q ? 1.5 : 0.5) * selfDoubleDot(tau_dev));
     Je[p] = Fe.determinant();
   }
+  // save_data.cpp:44-164: x, v, p, q, Je, then the plastic fields the model has
   std::vector<std::pair<std::string, const double*>> cols;
   const char* xs[3] = {"x", "y", "z"};
   const char* vs[3] = {"vx", "vy", "vz"};
   for (int a = 0; a < DIMENSION; ++a) cols.push_back({xs[a], X[a].data()});
   for (int a = 0; a < DIMENSION; ++a) cols.push_back({vs[a], V[a].data()});
-  cols.push_back({"pressure", pres.data()});
-  cols.push_back({"devstress", dev.data()});
+  cols.push_back({"p", pres.data()});
+  cols.push_back({"q", dev.data()});
   cols.push_back({"Je", Je.data()});
-  cols.push_back({"eps_pl_dev", particles.eps_pl_dev.data()});
-  cols.push_back({"eps_pl_vol", particles.eps_pl_vol.data()});
-  cols.push_back({"eps_pl_vol_pradhana", particles.eps_pl_vol_pradhana.data()});
-  cols.push_back({"delta_gamma", particles.delta_gamma.data()});
-  cols.push_back({"viscosity", particles.viscosity.data()});
-  cols.push_back({"muI", particles.muI.data()});
+  if (plastic_model != PlasticModel::NoPlasticity) {
+    cols.push_back({"eps_pl_vol", particles.eps_pl_vol.data()});
+    cols.push_back({"eps_pl_dev", particles.eps_pl_dev.data()});
+    cols.push_back({"delta_gamma", particles.delta_gamma.data()});
+    const bool mui_model = plastic_model == PlasticModel::DPMui || plastic_model == PlasticModel::MCCMui;
+    if (((plastic_model == PlasticModel::DPVisc || plastic_model == PlasticModel::MCCVisc) && use_mibf) || mui_model)
+      cols.push_back({"muI", particles.muI.data()});
+    if (mui_model) cols.push_back({"viscosity", particles.viscosity.data()});
+  }
   write_ply(directory + sim_name + "/particles_f" + extra + std::to_string(frame) + ".ply", n, cols);
   std::ofstream(directory + sim_name + "/last_written.txt") << frame << "\n";
 }
@@ -604,6 +657,11 @@ void Simulation::saveGridData(std::string extra) {
   for (int a = 0; a < DIMENSION; ++a) cols.push_back({xs[a], X[a].data()});
   for (int a = 0; a < DIMENSION; ++a) cols.push_back({vs[a], V[a].data()});
   cols.push_back({"mass", m.data()});
+  std::vector<double> fric;
+  if (use_mibf) {  // save_data.cpp:247-255
+    fric.resize(G);
+    if (mtr_get_grid_friction(ctx_, fric.data()) == MTR_OK) cols.push_back({"friction", fric.data()});
+  }
   write_ply(directory + sim_name + "/grid_f" + extra + std::to_string(frame) + ".ply", G, cols);
 }
 

@@ -13,6 +13,7 @@
 #include <chrono>
 #include <cmath>
 #include <memory>
+#include <thread>
 #include <utility>
 
 #include "../data_structures.hpp"
@@ -187,6 +188,11 @@ class Simulation {
 
   // GPU context of the running simulation
   mtr_ctx* ctx_ = nullptr;
+  // writes the particle file of the last snapshot (mtr_frame_begin) while the
+  // next frame steps on the GPU
+  std::thread frame_writer_;
+  void save_frame_async();
+  void finish_frame_output();
   bool prepare_device();
   void derive_constants();
   void download_state();

@@ -10,6 +10,11 @@ worker, and the memory it frees admits the next waiting request.  A tick
 advances every member by `tick_steps` steps; each member has a step limit,
 so it stops exactly after the steps it asked for.
 
+Block shapes of the tile kernels: the first batch that holds a group key
+(dimension, spline, precision, USL/MUSL, return-mapping kernel) is tuned
+(mtr_batch_autotune, trial steps that leave the scenes as they were); later
+batches take the shapes cached for their keys.
+
 No counterpart in the reference, which runs one Simulation per process.
 """
 import collections
@@ -43,7 +48,11 @@ class Server:
     admitted scenes together.  `precision` overrides each scene's precision
     (None keeps it)."""
 
-    def __init__(self, budget_bytes, device=0, tick_steps=8, precision=PREC_MIXED, keep_result=("x", "v")):
+    def __init__(self, budget_bytes, device=0, tick_steps=8, precision=PREC_MIXED, keep_result=("x", "v"),
+                 autotune=True, tune_reps=2):
+        self.autotune = autotune
+        self.tune_reps = int(tune_reps)
+        self.shapes = {}         # group key -> tile-kernel block shapes
         self.budget = int(budget_bytes)
         self.device = device
         self.tick_steps = int(tick_steps)
@@ -126,6 +135,8 @@ class Server:
                         batch.close()
                     batch = GpuBatch([r.sim for r in active])
                     members_key = key
+                    if self.autotune:
+                        self._shape(batch)
                 ts = now()
                 for r in active:
                     if r.started is None:
@@ -157,6 +168,22 @@ class Server:
         self.wall_s = now()
         return done
 
+    @staticmethod
+    def _key(gr):
+        return (gr["dim"], gr["spline_deg"], gr["fp32"], gr["musl"], gr["plastic_model_kernel"])
+
+    def _shape(self, batch):
+        """Applies the cached block shapes of the batch's groups; tunes the
+        batch when a group key is new."""
+        groups = batch.groups()
+        if any(self._key(gr) not in self.shapes for gr in groups):
+            groups = batch.autotune(self.tune_reps)
+            for gr in groups:
+                self.shapes.setdefault(self._key(gr), gr["tile_threads"])
+        for i, gr in enumerate(groups):
+            if gr["tile_threads"] != self.shapes[self._key(gr)]:
+                batch.set_tile_threads(i, self.shapes[self._key(gr)])
+
     # -- report ---------------------------------------------------------------
     def report(self, done):
         lat = np.array([r.done - r.arrival for r in done])
@@ -178,6 +205,7 @@ class Server:
             "mean_members": float(np.mean(self.tick_members)) if self.tick_members else 0.0,
             "peak_bytes": self.peak_bytes,
             "budget_bytes": self.budget,
+            "tile_threads": {"/".join(str(int(v)) for v in k): sh for k, sh in self.shapes.items()},
         }
 
 

@@ -5,6 +5,8 @@
 //
 //   host_parity steps  N  OUTDIR   -> N calls of advanceStep()
 //   host_parity frames N  OUTDIR   -> simulate() with end_frame = N
+//   host_parity saved  N  OUTDIR   -> the same with save_sim and save_grid:
+//                                     frame files under OUTDIR/run/
 //
 // OUTDIR/init.bin and OUTDIR/final.bin hold Np, then x, v, F, B (AoS, column-
 // major matrices) and the six plastic scalars per particle, as doubles;
@@ -51,9 +53,14 @@ int main(int argc, char** argv) {
   const int n = std::atoi(argv[2]);
 
   Simulation sim;
-  sim.initialize(false);
+  if (mode == "saved") {
+    sim.initialize(true, out + "/", "run");
+    sim.save_grid = true;
+  } else {
+    sim.initialize(false);
+  }
   sim.reduce_verbose = true;
-  sim.end_frame = mode == "frames" ? n : 1000;
+  sim.end_frame = mode == "steps" ? 1000 : n;
   sim.fps = 400;
   sim.cfl = 0.5;
   sim.flip_ratio = -0.95;

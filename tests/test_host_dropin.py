@@ -196,6 +196,59 @@ def test_host_simulation_matches_the_oracle(tmp_path, mode, n, dim, deg):
     compare_states(gpu, o, 1e-9, fields=("x", "v", "F", "B"), grid=False, sens=sens)
 
 
+def read_ply(path):
+    """(property names, rows) of a binary little-endian PLY file of doubles."""
+    with open(path, "rb") as f:
+        names, n = [], 0
+        assert f.readline() == b"ply\n"
+        assert f.readline() == b"format binary_little_endian 1.0\n"
+        for line in iter(f.readline, b"end_header\n"):
+            t = line.decode().split()
+            if t[0] == "element":
+                assert t[1] == "vertex"
+                n = int(t[2])
+            elif t[0] == "property":
+                assert t[1] == "double"
+                names.append(t[2])
+        rows = np.frombuffer(f.read(), dtype="<f8")
+    return names, rows.reshape(n, len(names))
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")
+@pytest.mark.parametrize("dim,deg", [(3, 2), (2, 3)])
+def test_saved_frames_have_the_reference_columns_and_the_run_state(tmp_path, dim, deg):
+    """simulate() with save_sim: the particle file of every frame (written from
+    a GPU snapshot while the next frame steps) and the grid file carry the
+    reference's properties in its order (save_data.cpp:7-255); the first file
+    holds the initial state and the last one the final state."""
+    exe = build_setup(os.path.join(SETUPS, "host_parity.cpp"), tmp_path, dim, deg)
+    n = 3
+    r = subprocess.run([exe, "saved", str(n), str(tmp_path)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    init = read_state(tmp_path / "init.bin", dim, False)
+    fin = read_state(tmp_path / "final.bin", dim, True)
+    run = tmp_path / "run"
+    xyz, vel = ["x", "y", "z"][:dim], ["vx", "vy", "vz"][:dim]
+    want = xyz + vel + ["p", "q", "Je", "eps_pl_vol", "eps_pl_dev", "delta_gamma"]  # DPVisc without MIBF
+    for f in range(n + 1):
+        names, rows = read_ply(run / f"particles_f{f}.ply")
+        assert names == want, names
+        assert rows.shape[0] == init["x"].shape[0]
+    _, first = read_ply(run / "particles_f0.ply")
+    assert np.array_equal(first[:, :dim], init["x"]) and np.array_equal(first[:, dim:2 * dim], init["v"])
+    _, last = read_ply(run / f"particles_f{n}.ply")
+    assert np.array_equal(last[:, :dim], fin["x"]) and np.array_equal(last[:, dim:2 * dim], fin["v"])
+    assert np.array_equal(last[:, 2 * dim + 3], fin["scalars"][:, 1])  # eps_pl_vol
+    assert np.array_equal(last[:, 2 * dim + 4], fin["scalars"][:, 0])  # eps_pl_dev
+    je = np.linalg.det(fin["F"])
+    assert np.abs(last[:, 2 * dim + 2] - je).max() <= 1e-12
+    gnames, grows = read_ply(run / f"grid_f{n}.ply")
+    assert gnames == xyz + vel + ["mass"]
+    assert grows[:, 2 * dim].sum() > 0
+    assert (run / "last_written.txt").read_text().strip() == str(n)
+
+
 KATS = ["BoundaryTest.AnalyticSlipFree", "BoundaryTest.AnalyticSlipStick", "CoulombFrictionTest.PlateSlipFree",
         "CoulombFrictionTest.PlateSlipStick", "CoulombFrictionTest.GeneralSlipFree",
         "CoulombFrictionTest.GeneralSlipStick", "BoundaryTest.MIBF", "ElasticityTest.BulkModulus",
