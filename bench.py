@@ -366,7 +366,9 @@ def measure(args, world, rank, local, sc, precision, sampler=None):
     ms_max = max_over_ranks(world, ms, local)
     value = sc.Np * args.steps * world / (ms_max / 1e3)
 
-    # per-kernel profile of the same state (CUDA events between launches)
+    # per-kernel profile of the same state (CUDA events between launches),
+    # after one untimed profiled step
+    g.profile(1)
     slots = g.profile(args.profile_steps)
     Ga, G = g.active_nodes()
     peak, peak_kind = hbm_peak()
