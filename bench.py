@@ -491,16 +491,25 @@ def ensemble_measure(args, local):
     sims = [make(sc) for sc in scs]
     batch = GpuBatch(sims)
     batch.step(W)
-    default_shapes = None
+    default = [gr["tile_threads"] for gr in batch.groups()]
     if not args.no_autotune:
-        # the default shapes first, on K/4 steps, then the tuned shapes
-        kd = max(8, K // 4)
-        default_shapes = {"value": ntot * kd / (timed(batch, kd) / 1e3), "steps": kd,
-                          "groups": batch.groups()}
-        batch.autotune(args.tune_reps)
+        batch.autotune(args.tune_reps)  # setup, untimed: trial steps leave the scenes as they are
     groups = batch.groups()
     ms = timed(batch, K)
     launches = batch.launch_count()
+    # tuned against default shapes on the same batch, interleaved in rounds of
+    # 16 steps so that both see the same states
+    ab = None
+    if not args.no_autotune:
+        tuned = [gr["tile_threads"] for gr in groups]
+        t_ms = {"tuned": 0.0, "default": 0.0}
+        for _ in range(4):
+            for name, shapes in (("default", default), ("tuned", tuned)):
+                for gi, sh in enumerate(shapes):
+                    batch.set_tile_threads(gi, sh)
+                t_ms[name] += timed(batch, 16)
+        ab = {"tuned_over_default": t_ms["default"] / t_ms["tuned"], "steps_each": 64,
+              "timed": "4 interleaved rounds of 16 batched steps per shape set, CUDA events"}
     lat = []
     for _ in range(max(8, K // 8)):
         t0 = time.perf_counter()
@@ -535,7 +544,7 @@ def ensemble_measure(args, local):
             "serial": {"value": serial, "ms_total": serial_ms,
                        "timed": "each scene alone through its own context and graphs, CUDA events"},
             "batched_over_serial": value / serial, "gpu_launches": launches, "dtype": "f32+f64",
-            "groups": groups, "default_shapes": default_shapes,
+            "groups": groups, "shapes_ab": ab,
             "config": "seeded DP column collapses: Np log-uniform 5k-300k, P(3D) 0.5, aspect U(0.5,4), "
                       "friction angle U(20,40) deg, E log-uniform 1e5-1e7 Pa, APIC USL, quadratic",
             "all_scenes_advanced": bool(min(steps_done) >= W + K)}

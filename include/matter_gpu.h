@@ -69,10 +69,16 @@ enum mtr_object_kind {
   MTR_OBJ_SILO = 5,        /* object_silo.hpp:16-54     prm[0] = cut (3D only)                */
   MTR_OBJ_BOX_ROTATED = 6, /* object_box.hpp:18-43       prm[0..2] center, prm[3..5] half
                               extents, prm[6..14] rotation, column-major (dim-sized in 2D)    */
-  MTR_OBJ_TERRAIN_GAUSS = 7 /* no reference counterpart: surface y = prm[0] + sum_k h_k *
+  MTR_OBJ_TERRAIN_GAUSS = 7, /* no reference counterpart: surface y = prm[0] + sum_k h_k *
                               exp(-r_k^2 / (2 sigma_k^2)), prm[1] = nbumps (<= 4), bump k at
                               prm[2+4k..5+4k] = (x_k, z_k, h_k, sigma_k); 2D ignores z_k      */
+  MTR_OBJ_LEVELSET = 8      /* object_vdb.hpp:17-94 on a dense lattice: prm[0] = level-set
+                              slot (mtr_set_levelset).  Inside where the trilinear sample of
+                              the signed distance phi is <= 0; normal = the trilinear sample
+                              of its gradient (second-order central differences, or the
+                              normals given at upload), normalised, zero where that is zero */
 };
+#define MTR_MAX_LEVELSETS 4
 
 /* scalar slots per particle (data_structures.hpp:16-21) */
 enum { MTR_SCALAR_EPS_PL_DEV = 0, MTR_SCALAR_EPS_PL_VOL, MTR_SCALAR_EPS_PL_VOL_PRADHANA,
@@ -159,6 +165,18 @@ int mtr_upload(mtr_ctx* ctx, const double* x, const double* v, const double* F, 
 /* Replaces the plate and object lists (simulation.hpp:109-110). */
 int mtr_set_objects(mtr_ctx* ctx, const mtr_plate* plates, int n_plates,
                     const mtr_object* objects, int n_objects);
+
+/* Dense level set for MTR_OBJ_LEVELSET objects (the grid an ObjectVdb samples,
+ * object_vdb.hpp:17-94, baked to a dense lattice; OpenVDB itself is not
+ * used).  phi: signed distance (negative inside) at origin + (i, j, k) *
+ * spacing, dims[0] x dims[1] x dims[2] samples (dims[2] = 1 in 2D), stored
+ * like grid nodes: index (i * dims[1] + j) * dims[2] + k.  normals: NULL to
+ * use the central-difference gradient of phi, or 3 floats per sample (a
+ * baked normal field).  Samples outside the lattice read phi = 3 * spacing
+ * (an OpenVDB narrow-band background) and a zero gradient.  Slots
+ * 0..MTR_MAX_LEVELSETS-1; a slot may be replaced at any time between steps. */
+int mtr_set_levelset(mtr_ctx* ctx, int slot, const float* phi, const float* normals, const uint32_t dims[3],
+                     const double origin[3], double spacing);
 
 /* Advances up to nsteps calls of Simulation::advanceStep (simulation.cpp:219-273)
  * including the time/frame bookkeeping of simulate() (simulation.cpp:176-200);

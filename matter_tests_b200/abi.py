@@ -55,7 +55,10 @@ class BC:  # tools.hpp:57
 
 
 class ObjectKind:
-    Bump, Ground, Ramp, Curve, Gate, Silo, BoxRotated, TerrainGauss = range(8)
+    Bump, Ground, Ramp, Curve, Gate, Silo, BoxRotated, TerrainGauss, LevelSet = range(9)
+
+
+MAX_LEVELSETS = 4
 
 
 PREC_FP64 = 0

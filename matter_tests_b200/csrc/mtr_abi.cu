@@ -176,6 +176,9 @@ struct mtr_ctx {
   bool frame_pending = false;
   uint32_t frame_n = 0;
   int frame_ncols = 0;
+  // dense level sets (mtr_set_levelset)
+  float* ls_phi[MTR_MAX_LEVELSETS] = {};
+  float* ls_grad[MTR_MAX_LEVELSETS] = {};
 };
 
 namespace {
@@ -475,6 +478,13 @@ void build_graphs(mtr_ctx* c) {
     if (e != cudaSuccess) throw MtrError{MTR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)};
     c->launches_per_step = n / kGraphSteps;
   }
+}
+
+// Every MTR_OBJ_LEVELSET object must name a loaded slot before a step.
+void check_levelsets(const mtr_ctx* c) {
+  for (const mtr_object& o : c->objects)
+    if (o.kind == MTR_OBJ_LEVELSET && !c->ls_phi[(int)o.prm[0]])
+      throw MtrError{MTR_ERR_STATE, "level-set object whose slot has no mtr_set_levelset data"};
 }
 
 // Columns of the particle frame file (save_data.cpp:7-171) for these parameters.
@@ -1115,9 +1125,15 @@ int mtr_set_objects(mtr_ctx* c, const mtr_plate* plates, int n_plates, const mtr
     for (int i = 0; i < n_plates; ++i)
       if (plates[i].bc < 0 || plates[i].bc > 2 || plates[i].plate_type < 0 || plates[i].plate_type > 5)
         throw MtrError{MTR_ERR_INVALID, "invalid plate type or BC"};
-    for (int i = 0; i < n_objects; ++i)
-      if (objects[i].bc < 0 || objects[i].bc > 2 || objects[i].kind < 0 || objects[i].kind > MTR_OBJ_TERRAIN_GAUSS)
+    for (int i = 0; i < n_objects; ++i) {
+      if (objects[i].bc < 0 || objects[i].bc > 2 || objects[i].kind < 0 || objects[i].kind > MTR_OBJ_LEVELSET)
         throw MtrError{MTR_ERR_INVALID, "invalid object kind or BC"};
+      if (objects[i].kind == MTR_OBJ_LEVELSET) {
+        const double sl = objects[i].prm[0];
+        if (!(sl >= 0 && sl < MTR_MAX_LEVELSETS) || sl != std::floor(sl))
+          throw MtrError{MTR_ERR_INVALID, "level-set object: prm[0] must be a slot 0..MTR_MAX_LEVELSETS-1"};
+      }
+    }
     CK(cudaSetDevice(c->device));
     c->plates.assign(plates, plates + n_plates);
     c->objects.assign(objects, objects + n_objects);
@@ -1138,6 +1154,7 @@ int mtr_step(mtr_ctx* c, int nsteps) {
   return guarded([&]() -> int {
     if (!c) throw MtrError{MTR_ERR_INVALID, "null context"};
     if (!c->uploaded) throw MtrError{MTR_ERR_STATE, "mtr_step before mtr_upload"};
+    check_levelsets(c);
     if (nsteps <= 0) return MTR_OK;
     CK(cudaSetDevice(c->device));
     read_header(c);
@@ -1460,6 +1477,51 @@ int mtr_profile(mtr_ctx* c, int nsteps, double* slot_ms, const char** slot_names
   });
 }
 
+int mtr_set_levelset(mtr_ctx* c, int slot, const float* phi, const float* normals, const uint32_t dims[3],
+                     const double origin[3], double spacing) {
+  return guarded([&]() -> int {
+    if (!c || !phi || !dims || !origin) throw MtrError{MTR_ERR_INVALID, "null argument"};
+    if (slot < 0 || slot >= MTR_MAX_LEVELSETS) throw MtrError{MTR_ERR_INVALID, "slot out of range"};
+    if (!(spacing > 0) || !std::isfinite(spacing)) throw MtrError{MTR_ERR_INVALID, "spacing must be positive"};
+    if (dims[0] < 2 || dims[1] < 2 || (c->dim == 3 ? dims[2] < 2 : dims[2] != 1))
+      throw MtrError{MTR_ERR_INVALID, "dims: at least 2 samples per axis (dims[2] = 1 in 2D)"};
+    const uint64_t n = (uint64_t)dims[0] * dims[1] * dims[2];
+    if (n > (1ull << 34)) throw MtrError{MTR_ERR_TOO_LARGE, "level set larger than 2^34 samples"};
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));  // no step may still read the old arrays
+    dfree(c->ls_phi[slot]);
+    dfree(c->ls_grad[slot]);
+    c->ls_phi[slot] = c->ls_grad[slot] = nullptr;
+    c->hp.ls[slot] = DevParams::LevelSet{};
+    float* dphi = dalloc<float>(n);
+    c->ls_phi[slot] = dphi;
+    float* dgrad = dalloc<float>(3 * n);
+    c->ls_grad[slot] = dgrad;
+    CK(cudaMemcpyAsync(dphi, phi, sizeof(float) * n, cudaMemcpyHostToDevice, c->stream));
+    const float background = (float)(3.0 * spacing);
+    if (normals) {
+      CK(cudaMemcpyAsync(dgrad, normals, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+    } else {
+      k_levelset_grad<<<cap_blocks(n, 256, 148 * 16), 256, 0, c->stream>>>(dphi, dgrad, dims[0], dims[1], dims[2],
+                                                                        c->dim, background, 0.5 / spacing);
+      CK(cudaGetLastError());
+    }
+    DevParams::LevelSet& L = c->hp.ls[slot];
+    L.phi = dphi;
+    L.grad = dgrad;
+    for (int a = 0; a < 3; ++a) {
+      L.n[a] = dims[a];
+      L.org[a] = a < c->dim ? origin[a] : 0.0;
+    }
+    L.h = spacing;
+    L.inv_h = 1.0 / spacing;
+    L.background = (double)background;
+    upload_params(c);
+    CK(cudaStreamSynchronize(c->stream));
+    return MTR_OK;
+  });
+}
+
 int mtr_frame_columns(mtr_ctx* c, const char** names, int max_names) {
   if (!c) return MTR_ERR_INVALID;
   std::vector<const char*> n;
@@ -1706,6 +1768,7 @@ int mtr_batch_create(mtr_ctx* const* ctxs, int n, mtr_batch** out) {
     *out = nullptr;
     for (int i = 0; i < n; ++i) {
       if (!ctxs[i] || !ctxs[i]->uploaded) throw MtrError{MTR_ERR_STATE, "every member needs mtr_upload first"};
+      check_levelsets(ctxs[i]);
       if (ctxs[i]->device != ctxs[0]->device) throw MtrError{MTR_ERR_INVALID, "members must share one device"};
       if (ctxs[i]->prm.pbc) throw MtrError{MTR_ERR_INVALID, "periodic scenes step on their own, not in a batch"};
       for (int j = 0; j < i; ++j)
@@ -1915,6 +1978,10 @@ void mtr_ctx_destroy(mtr_ctx* c) {
   }
   dfree(c->frame_dev);
   if (c->frame_host) cudaFreeHost(c->frame_host);
+  for (int i = 0; i < MTR_MAX_LEVELSETS; ++i) {
+    dfree(c->ls_phi[i]);
+    dfree(c->ls_grad[i]);
+  }
   free_graphs(c);
   free_grid(c);
   for (void* p : c->pallocs) dfree(p);

@@ -21,10 +21,50 @@ __device__ __forceinline__ void normalize(double (&n)[3]) {
   }
 }
 
+// Trilinear (2D: bilinear) sample of component `comp` of a dense level-set
+// lattice field with `stride` floats per sample; lattice points outside read
+// `outside`.  The sample is the OpenVDB BoxSampler's: index coordinates
+// u = (X - org) / h, weights from u - floor(u), and lerp(a, b, w) = a + w (b - a)
+// applied along x, then y, then z, each operation rounded on its own.
 template <int D>
-__device__ bool obj_inside(const mtr_object& o, const double (&X)[3]) {
+__device__ double ls_sample(const DevParams::LevelSet& L, const float* f, int stride, int comp,
+                            const double (&X)[3], double outside) {
+  int i0[3] = {0, 0, 0};
+  double w[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    const double u = __dmul_rn(__dsub_rn(X[a], L.org[a]), L.inv_h);
+    const double fl = floor(u);
+    i0[a] = fl < -2.0 ? -2 : (fl > 2.0e9 ? 2000000000 : (int)fl);
+    w[a] = __dsub_rn(u, fl);
+  }
+  auto at = [&](int i, int j, int k) -> double {
+    if (i < 0 || j < 0 || k < 0 || i >= (int)L.n[0] || j >= (int)L.n[1] || k >= (int)L.n[2]) return outside;
+    return (double)f[((size_t)((size_t)i * L.n[1] + j) * L.n[2] + k) * stride + comp];
+  };
+  auto lerp = [](double a, double b, double t) { return __dadd_rn(a, __dmul_rn(t, __dsub_rn(b, a))); };
+  const int i = i0[0], j = i0[1], k = i0[2];
+  if constexpr (D == 3) {
+    const double c00 = lerp(at(i, j, k), at(i + 1, j, k), w[0]);
+    const double c10 = lerp(at(i, j + 1, k), at(i + 1, j + 1, k), w[0]);
+    const double c01 = lerp(at(i, j, k + 1), at(i + 1, j, k + 1), w[0]);
+    const double c11 = lerp(at(i, j + 1, k + 1), at(i + 1, j + 1, k + 1), w[0]);
+    return lerp(lerp(c00, c10, w[1]), lerp(c01, c11, w[1]), w[2]);
+  } else {
+    const double c0 = lerp(at(i, j, 0), at(i + 1, j, 0), w[0]);
+    const double c1 = lerp(at(i, j + 1, 0), at(i + 1, j + 1, 0), w[0]);
+    return lerp(c0, c1, w[1]);
+  }
+}
+
+template <int D>
+__device__ bool obj_inside(const DevParams& P, const mtr_object& o, const double (&X)[3]) {
   const double x = X[0], y = X[1];
   switch (o.kind) {
+    case MTR_OBJ_LEVELSET: {  // object_vdb.hpp:45-57: phi <= 0
+      const DevParams::LevelSet& L = P.ls[(int)o.prm[0]];
+      return ls_sample<D>(L, L.phi, 1, 0, X, L.background) <= 0.0;
+    }
     case MTR_OBJ_BUMP: return y < 0.0475 / cosh(25 * (x - 0.43));  // object_bump.hpp:15-27
     case MTR_OBJ_GROUND: return !(y > o.prm[0]);                  // object_ground.hpp:16-25
     case MTR_OBJ_RAMP: return y < 0.1 * tanh(-100 * x);           // object_ramp.hpp:15-26
@@ -73,7 +113,7 @@ __device__ bool obj_inside(const mtr_object& o, const double (&X)[3]) {
 }
 
 template <int D>
-__device__ void obj_normal(const mtr_object& o, const double (&X)[3], double (&n)[3]) {
+__device__ void obj_normal(const DevParams& P, const mtr_object& o, const double (&X)[3], double (&n)[3]) {
   const double x = X[0], y = X[1];
   n[0] = n[1] = n[2] = 0.0;
   switch (o.kind) {
@@ -171,6 +211,13 @@ __device__ void obj_normal(const mtr_object& o, const double (&X)[3], double (&n
       normalize<D>(n);
       break;
     }
+    case MTR_OBJ_LEVELSET: {  // object_vdb.hpp:59-78: sampled gradient, normalised (zero stays zero)
+      const DevParams::LevelSet& L = P.ls[(int)o.prm[0]];
+#pragma unroll
+      for (int a = 0; a < D; ++a) n[a] = ls_sample<D>(L, L.grad, 3, a, X, 0.0);
+      normalize<D>(n);
+      break;
+    }
   }
 }
 
@@ -223,13 +270,13 @@ __device__ bool boundary_collision(const DevParams& P, const mtr_plate* plates, 
   double X[3] = {Xi[0] + dt * vi[0], Xi[1] + dt * vi[1], D == 3 ? Xi[2] + dt * vi[2] : 0.0};
   for (int oi = 0; oi < P.nobjects; ++oi) {  // boundary_collision.cpp:13-79
     const mtr_object& o = P.objects[oi];
-    if (!obj_inside<D>(o, X)) continue;
+    if (!obj_inside<D>(P, o, X)) continue;
     double vr[3] = {vo[0], vo[1], vo[2]};
     if (o.bc == MTR_BC_NOSLIP) {
       vr[0] = vr[1] = vr[2] = 0.0;
     } else if (o.bc == MTR_BC_SLIPFREE) {
       double n[3];
-      obj_normal<D>(o, X, n);
+      obj_normal<D>(P, o, X, n);
       double dot = vr[0] * n[0] + vr[1] * n[1];
       if constexpr (D == 3) dot += vr[2] * n[2];
       if (dot < 0) {
@@ -254,7 +301,7 @@ __device__ bool boundary_collision(const DevParams& P, const mtr_plate* plates, 
       }
     } else if (o.bc == MTR_BC_SLIPSTICK) {
       double n[3];
-      obj_normal<D>(o, X, n);
+      obj_normal<D>(P, o, X, n);
       double dot = vr[0] * n[0] + vr[1] * n[1];
       if constexpr (D == 3) dot += vr[2] * n[2];
 #pragma unroll

@@ -44,6 +44,13 @@ struct DevParams {
   // 1e-9 on the mixed path, whose FP32 strains carry about that much
   double dgamma_tol;
   mtr_object objects[MTR_MAXO];
+  // dense level sets of MTR_OBJ_LEVELSET objects (mtr_set_levelset)
+  struct LevelSet {
+    const float* phi;   // n[0] * n[1] * n[2] samples
+    const float* grad;  // 3 per sample
+    uint32_t n[3];
+    double org[3], h, inv_h, background;
+  } ls[MTR_MAX_LEVELSETS];
 };
 
 // Per-step state that lives on the device so a whole step (and many steps in

@@ -2051,6 +2051,31 @@ __global__ void __launch_bounds__(256) k_frame_rows(PBufT<R> b0, PBufT<R> b1, co
   if (cols & kFrameViscosity) row[c++] = p.s.viscosity;
 }
 
+// Gradient of a dense level set by second-order central differences,
+// 0.5 (phi[i+1] - phi[i-1]) / h per axis, neighbours outside the lattice
+// reading `background` (OpenVDB's Gradient with CD_2ND, tools/GridOperators.h,
+// on a fully active grid).  Three floats per sample; unused axes are zero.
+static __global__ void __launch_bounds__(256) k_levelset_grad(const float* __restrict__ phi, float* __restrict__ grad,
+                                                       uint32_t n0, uint32_t n1, uint32_t n2, int dim,
+                                                       float background, double half_inv_h) {
+  const uint64_t total = (uint64_t)n0 * n1 * n2;
+  for (uint64_t l = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; l < total; l += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t k = (uint32_t)(l % n2), j = (uint32_t)((l / n2) % n1), i = (uint32_t)(l / ((uint64_t)n1 * n2));
+    const uint32_t n[3] = {n0, n1, n2}, c[3] = {i, j, k};
+    const uint64_t step[3] = {(uint64_t)n1 * n2, n2, 1};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float g = 0.0f;
+      if (a < dim) {
+        const float plus = c[a] + 1 < n[a] ? phi[l + step[a]] : background;
+        const float minus = c[a] >= 1 ? phi[l - step[a]] : background;
+        g = (float)((double)__fsub_rn(plus, minus) * half_inv_h);
+      }
+      grad[l * 3 + a] = g;
+    }
+  }
+}
+
 // node array of type R -> FP64 (grid read-back of the FP32 path)
 template <typename R>
 __global__ void k_to_f64(uint64_t n, const R* __restrict__ src, double* dst) {

@@ -26,7 +26,7 @@ EXPORTS = (
     "mtr_footprint", "mtr_ctx_destroy", "mtr_last_error", "mtr_p2g_noalloc",
     "mtr_autotune", "mtr_set_tile_threads", "mtr_get_tile_threads", "mtr_batch_autotune", "mtr_batch_groups",
     "mtr_batch_get_group", "mtr_batch_set_tile_threads", "mtr_frame_columns", "mtr_frame_begin",
-    "mtr_frame_wait", "mtr_get_grid_friction",
+    "mtr_frame_wait", "mtr_get_grid_friction", "mtr_set_levelset",
 )
 
 _lib = None
@@ -96,6 +96,8 @@ def load_library(path=LIB_PATH):
     lib.mtr_frame_wait.argtypes = [C.c_void_p, C.c_double, C.POINTER(_P), C.POINTER(C.c_uint32),
                                    C.POINTER(C.c_int), C.POINTER(MtrClock)]
     lib.mtr_get_grid_friction.argtypes = [C.c_void_p, _P]
+    _F = C.POINTER(C.c_float)
+    lib.mtr_set_levelset.argtypes = [C.c_void_p, C.c_int, _F, _F, _U, _P, C.c_double]
     lib.mtr_ctx_destroy.argtypes = [C.c_void_p]
     lib.mtr_ctx_destroy.restype = None
     lib.mtr_last_error.restype = C.c_char_p
@@ -105,6 +107,18 @@ def load_library(path=LIB_PATH):
 
 def _ptr(a):
     return None if a is None else a.ctypes.data_as(_P)
+
+
+def _set_levelset(fn, h, ls):
+    """Calls an mtr_set_levelset-shaped entry point with a scenes.LevelSetData."""
+    phi = np.ascontiguousarray(ls.phi, dtype=np.float32).reshape(-1)
+    nrm = None if ls.normals is None else np.ascontiguousarray(ls.normals, dtype=np.float32).reshape(-1)
+    dims = (C.c_uint32 * 3)(*(list(ls.dims) + [1] * (3 - len(ls.dims))))
+    org = np.zeros(3)
+    org[:len(ls.origin)] = ls.origin
+    F = C.POINTER(C.c_float)
+    return fn(h, int(ls.slot), phi.ctypes.data_as(F), None if nrm is None else nrm.ctypes.data_as(F), dims,
+              _ptr(org), float(ls.spacing))
 
 
 def _check(lib, fn, rc):
@@ -147,6 +161,16 @@ class GpuSim:
         pa = (MtrPlate * max(1, len(plates)))(*plates)
         oa = (MtrObject * max(1, len(objects)))(*objects)
         _check(self.lib, "mtr_set_objects", self.lib.mtr_set_objects(self.h, pa, len(plates), oa, len(objects)))
+
+    def set_levelset(self, ls):
+        """Uploads a scenes.LevelSetData to its slot (mtr_set_levelset)."""
+        _check(self.lib, "mtr_set_levelset", _set_levelset(self.lib.mtr_set_levelset, self.h, ls))
+
+    def set_scene_objects(self, scene):
+        """The scene's level sets, plates and objects."""
+        for ls in getattr(scene, "levelsets", ()):
+            self.set_levelset(ls)
+        self.set_objects(scene.plates, scene.objects)
 
     def set_step_limit(self, last_step):
         """No step past step number last_step (mtr_set_step_limit)."""

@@ -3,7 +3,8 @@
 // normal), plus describe(): the B200 step evaluates objects on the GPU, so an
 // object must be able to describe itself as an mtr_object (kind + parameters).
 // The built-in objects do; a user subclass that does not override describe()
-// is reported by Simulation::simulate as not representable on the GPU.
+// is baked by Simulation::simulate into a dense level set (object_levelset.hpp)
+// over the box the flow can reach.
 #ifndef OBJECTGENERAL_HPP
 #define OBJECTGENERAL_HPP
 
@@ -11,6 +12,8 @@
 
 #include "../tools.hpp"
 #include "matter_gpu.h"
+
+class ObjectLevelSet;
 
 class ObjectGeneral {
  public:
@@ -23,8 +26,11 @@ class ObjectGeneral {
   virtual bool inside(const TV& X_in) const = 0;
   virtual TV normal(const TV& X_in) const = 0;
 
-  // Fills `out` with this object's GPU descriptor; false if there is none.
+  // Fills `out` with this object's GPU descriptor; false if there is none
+  // (Simulation then bakes the object into a dense level set).
   virtual bool describe(mtr_object& out) const { return false; }
+  // The dense level set of an ObjectLevelSet (objects/object_levelset.hpp).
+  virtual const ObjectLevelSet* levelset() const { return nullptr; }
 
  protected:
   mtr_object base_descriptor(int kind) const {

@@ -10,6 +10,7 @@
 
 #include <sys/stat.h>
 
+#include <algorithm>
 #include <cerrno>
 #include <cstdlib>
 #include <cstring>
@@ -259,12 +260,59 @@ bool Simulation::prepare_device() {
     pl.push_back(m);
   }
   std::vector<mtr_object> ob;
+  std::vector<std::unique_ptr<ObjectLevelSet>> baked;
+  int slot = 0;
   for (const auto& o : objects) {
     mtr_object m;
-    if (!o->describe(m)) {
-      debug("Object '", o->name, "' has no GPU description (a user subclass of ObjectGeneral without describe()).");
-      exit = 1;
-      return false;
+    const ObjectLevelSet* ls = o->levelset();
+    if (!ls && !o->describe(m)) {
+      TV lo = bake_min, hi = bake_max;
+      if (!(hi - lo).norm()) {  // the initial particle box, grown
+        lo = particles.x[0];
+        hi = particles.x[0];
+        for (unsigned int q = 1; q < Np; ++q)
+          for (int a = 0; a < DIMENSION; ++a) {
+            lo(a) = std::min(lo(a), particles.x[q](a));
+            hi(a) = std::max(hi(a), particles.x[q](a));
+          }
+        T ext = 0;
+        for (int a = 0; a < DIMENSION; ++a) ext = std::max(ext, hi(a) - lo(a));
+        for (int a = 0; a < DIMENSION; ++a) {
+          lo(a) -= 0.5 * ext + 8 * dx;
+          hi(a) += 0.5 * ext + 8 * dx;
+        }
+      }
+      const T h = bake_spacing > 0 ? bake_spacing : 0.5 * dx;
+      double samples = 1;
+      for (int a = 0; a < DIMENSION; ++a) samples *= std::ceil((hi(a) - lo(a)) / h) + 1;
+      if (samples > 4.0e8) {
+        debug("Object '", o->name, "': baking it at spacing ", h, " needs ", samples,
+              " samples; set bake_spacing or bake_min/bake_max.");
+        exit = 1;
+        return false;
+      }
+      if (!reduce_verbose)
+        debug("Object '", o->name, "' has no GPU description: baking it into a level set (", samples,
+              " samples, spacing ", h, ").");
+      baked.push_back(ObjectLevelSet::bake(*o, lo, hi, h));
+      ls = baked.back().get();
+    }
+    if (ls) {
+      if (slot >= MTR_MAX_LEVELSETS) {
+        debug("At most ", MTR_MAX_LEVELSETS, " level-set objects (baked or given) per simulation.");
+        exit = 1;
+        return false;
+      }
+      const uint32_t dims[3] = {ls->dims[0], ls->dims[1], ls->dims[2]};
+      double org[3] = {0.0, 0.0, 0.0};
+      for (int a = 0; a < DIMENSION; ++a) org[a] = ls->origin(a);
+      rc = mtr_set_levelset(ctx_, slot, ls->phi.data(), ls->normals.empty() ? nullptr : ls->normals.data(), dims,
+                            org, ls->spacing);
+      if (rc != MTR_OK) {
+        report_device_error(rc, "mtr_set_levelset");
+        return false;
+      }
+      m = ls->descriptor(slot++);
     }
     ob.push_back(m);
   }

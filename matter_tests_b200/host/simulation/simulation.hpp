@@ -18,6 +18,7 @@
 
 #include "../data_structures.hpp"
 #include "../objects/object_general.hpp"
+#include "../objects/object_levelset.hpp"
 #include "../objects/object_plate.hpp"
 #include "../timer.hpp"
 #include "../tools.hpp"
@@ -109,6 +110,12 @@ class Simulation {
   // (MTR_PREC_FP64 is the reference's double precision)
   int device = 0;
   int precision = MTR_PREC_FP64;
+  // Objects without a GPU description (user subclasses of ObjectGeneral) are
+  // baked into dense level sets (objects/object_levelset.hpp) at this lattice
+  // spacing (0: dx / 2) over [bake_min, bake_max] (equal corners: the initial
+  // particle box grown on every side by half its largest extent plus 8 dx).
+  T bake_spacing = 0;
+  TV bake_min = TV::Zero(), bake_max = TV::Zero();
   // simulated time and step count reached (the reference keeps them private)
   T elapsed_time() const { return time; }
   unsigned int elapsed_steps() const { return current_time_step; }

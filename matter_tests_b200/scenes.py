@@ -31,6 +31,7 @@ class Scene:
     scalars: np.ndarray = None
     plates: list = field(default_factory=list)
     objects: list = field(default_factory=list)
+    levelsets: list = field(default_factory=list)  # LevelSetData for ObjectKind.LevelSet objects
 
     @property
     def Np(self):
@@ -39,6 +40,47 @@ class Scene:
     @property
     def dim(self):
         return self.params.dim
+
+
+@dataclass
+class LevelSetData:
+    """A dense level set (mtr_set_levelset): phi[i, j, k] at origin + (i, j, k) * spacing."""
+    slot: int
+    phi: np.ndarray          # float32, shape dims (dims[2] = 1 in 2D)
+    origin: tuple
+    spacing: float
+    normals: np.ndarray = None  # float32 (*dims, 3) or None for the gradient of phi
+
+    @property
+    def dims(self):
+        return tuple(int(n) for n in self.phi.shape)
+
+
+def sample_levelset(fn, lo, hi, spacing, dim, slot=0):
+    """Samples a signed-distance-like function fn(X) (X: (n, dim) array, negative
+    inside) on the lattice covering [lo, hi] at `spacing`."""
+    n = [int(math.ceil((hi[a] - lo[a]) / spacing)) + 1 for a in range(dim)]
+    axes = [lo[a] + spacing * np.arange(n[a]) for a in range(dim)]
+    grid = np.stack(np.meshgrid(*axes, indexing="ij"), axis=-1).reshape(-1, dim)
+    phi = np.asarray(fn(grid), dtype=np.float64).astype(np.float32)
+    shape = tuple(n) + ((1,) if dim == 2 else ())
+    return LevelSetData(slot, phi.reshape(shape), tuple(lo[:dim]) + ((0.0,) if dim == 2 else ()), float(spacing))
+
+
+def terrain_levelset(obj, dim, lo, hi, spacing, slot=0):
+    """phi = y - s(x, z) of a TerrainGauss object: its gradient (-s_x, 1, -s_z)
+    points along the analytic terrain normal."""
+    prm = list(obj.prm)
+
+    def surf(X):
+        ys = np.full(X.shape[0], prm[0])
+        for b in range(int(prm[1])):
+            xb, zb, hb, sb = prm[2 + 4 * b:6 + 4 * b]
+            r2 = (X[:, 0] - xb) ** 2 + ((X[:, 2] - zb) ** 2 if dim == 3 else 0.0)
+            ys = ys + hb * np.exp(-r2 / (2 * sb * sb))
+        return X[:, 1] - ys
+
+    return sample_levelset(surf, lo, hi, spacing, dim, slot)
 
 
 def lattice(lo, hi, dx, ppc_axis, rng, jitter=0.25):

@@ -162,6 +162,14 @@ class Oracle(_Checker):
         if not self.h:
             raise ValueError("oracle rejected the parameters")
 
+    def set_levelset(self, ls):
+        """A scenes.LevelSetData into its slot (orc_set_levelset)."""
+        from matter_tests_b200.gpu import _set_levelset
+        self.lib.orc_set_levelset.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                              _U, _P, C.c_double]
+        self._ls_keep = getattr(self, "_ls_keep", []) + [ls]
+        assert _set_levelset(self.lib.orc_set_levelset, self.h, ls) == 0
+
     def keys(self):
         k = np.zeros(self.Np, dtype=np.uint32)
         self.lib.orc_get_keys(self.h, k.ctypes.data_as(_U))

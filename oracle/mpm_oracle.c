@@ -54,6 +54,12 @@ typedef struct orc {
   int nplates, nobjects;
   mtr_plate plates[MAXP];
   mtr_object objects[MAXO];
+  /* dense level sets of MTR_OBJ_LEVELSET objects (orc_set_levelset) */
+  struct {
+    float *phi, *grad;
+    uint32_t n[3];
+    double org[3], h, inv_h, background;
+  } ls[MTR_MAX_LEVELSETS];
   /* constants derived in simulate(), simulation.cpp:94-136 */
   double lambda, mu, K, wave_speed, dt_max, frame_dt, final_time;
   double one_over_dx, one_over_dx_square, apicDinverse;
@@ -615,9 +621,50 @@ static void neohookean_piola(orc* s, M3 Fe, M3 P) {
 /* ------------------------------------------------------------------------ */
 /* boundary collision, boundary_collision.cpp:5-394 and object_*.hpp         */
 /* ------------------------------------------------------------------------ */
+/* Dense level set: the signed distance an ObjectVdb samples (object_vdb.hpp:
+ * 17-94) on a uniform lattice.  Trilinear (2D: bilinear) sample in index
+ * coordinates u = (X - org) / h with weights u - floor(u) and
+ * lerp(a, b, w) = a + w (b - a) along x, then y, then z (OpenVDB's
+ * BoxSampler); lattice points outside read `outside`. */
+static double ls_sample(const orc* s, int slot, const float* f, int stride, int comp, const double* X,
+                        double outside) {
+  int d = s->dim;
+  int i0[3] = {0, 0, 0};
+  double w[3] = {0.0, 0.0, 0.0};
+  for (int a = 0; a < d; ++a) {
+    double u = (X[a] - s->ls[slot].org[a]) * s->ls[slot].inv_h;
+    double fl = floor(u);
+    i0[a] = fl < -2.0 ? -2 : (fl > 2.0e9 ? 2000000000 : (int)fl);
+    w[a] = u - fl;
+  }
+  double c[8];
+  for (int q = 0; q < 8; ++q) {
+    int i = i0[0] + (q & 1), j = i0[1] + ((q >> 1) & 1), k = i0[2] + ((q >> 2) & 1);
+    if (d == 2 && (q >> 2)) {
+      c[q] = 0.0;
+      continue;
+    }
+    const uint32_t* n = s->ls[slot].n;
+    if (i < 0 || j < 0 || k < 0 || i >= (int)n[0] || j >= (int)n[1] || k >= (int)n[2])
+      c[q] = outside;
+    else
+      c[q] = (double)f[(((size_t)i * n[1] + j) * n[2] + k) * stride + comp];
+  }
+#define LERP(a, b, t) ((a) + (t) * ((b) - (a)))
+  double c0 = LERP(c[0], c[1], w[0]), c1 = LERP(c[2], c[3], w[0]);
+  if (d == 2) return LERP(c0, c1, w[1]);
+  double c2 = LERP(c[4], c[5], w[0]), c3 = LERP(c[6], c[7], w[0]);
+  return LERP(LERP(c0, c1, w[1]), LERP(c2, c3, w[1]), w[2]);
+#undef LERP
+}
+
 static int obj_inside(const orc* s, const mtr_object* o, const double* X) {
   double x = X[0], y = X[1];
   switch (o->kind) {
+    case MTR_OBJ_LEVELSET: { /* object_vdb.hpp:45-57: phi <= 0 */
+      int sl = (int)o->prm[0];
+      return ls_sample(s, sl, s->ls[sl].phi, 1, 0, X, s->ls[sl].background) <= 0.0;
+    }
     case MTR_OBJ_BUMP: return y < 0.0475 / cosh(25 * (x - 0.43)); /* object_bump.hpp:15-27 */
     case MTR_OBJ_GROUND: return !(y > o->prm[0]);                 /* object_ground.hpp:16-25 */
     case MTR_OBJ_RAMP: return y < 0.1 * tanh(-100 * x);           /* object_ramp.hpp:15-26 */
@@ -676,6 +723,12 @@ static void obj_normal(const orc* s, const mtr_object* o, const double* X, doubl
   double x = X[0], y = X[1];
   n[0] = n[1] = n[2] = 0.0;
   switch (o->kind) {
+    case MTR_OBJ_LEVELSET: { /* object_vdb.hpp:59-78: sampled gradient, normalised */
+      int sl = (int)o->prm[0];
+      for (int a = 0; a < d; ++a) n[a] = ls_sample(s, sl, s->ls[sl].grad, 3, a, X, 0.0);
+      normalize(d, n);
+      break;
+    }
     case MTR_OBJ_BUMP: { /* object_bump.hpp:29-41 */
       double arg = 25 * (x - 0.43);
       double b_der = -25 * 0.0475 * tanh(arg) / cosh(arg);
@@ -1973,6 +2026,51 @@ int orc_set_objects(orc* s, const mtr_plate* plates, int np, const mtr_object* o
   return 0;
 }
 
+/* A dense level set for MTR_OBJ_LEVELSET objects; normals NULL = the
+ * second-order central-difference gradient 0.5 (phi[i+1] - phi[i-1]) / h
+ * (OpenVDB's Gradient with CD_2ND), neighbours outside the lattice reading
+ * the background 3 h. */
+int orc_set_levelset(orc* s, int slot, const float* phi, const float* normals, const uint32_t* dims,
+                     const double* origin, double spacing) {
+  if (slot < 0 || slot >= MTR_MAX_LEVELSETS || !(spacing > 0)) return -1;
+  size_t n = (size_t)dims[0] * dims[1] * dims[2];
+  free(s->ls[slot].phi);
+  free(s->ls[slot].grad);
+  s->ls[slot].phi = (float*)malloc(sizeof(float) * n);
+  s->ls[slot].grad = (float*)malloc(sizeof(float) * 3 * n);
+  memcpy(s->ls[slot].phi, phi, sizeof(float) * n);
+  float bg = (float)(3.0 * spacing);
+  if (normals) {
+    memcpy(s->ls[slot].grad, normals, sizeof(float) * 3 * n);
+  } else {
+    double half_inv_h = 0.5 / spacing;
+    for (size_t l = 0; l < n; ++l) {
+      uint32_t k = (uint32_t)(l % dims[2]), j = (uint32_t)((l / dims[2]) % dims[1]);
+      uint32_t i = (uint32_t)(l / ((size_t)dims[1] * dims[2]));
+      uint32_t c[3] = {i, j, k};
+      size_t step[3] = {(size_t)dims[1] * dims[2], dims[2], 1};
+      for (int a = 0; a < 3; ++a) {
+        float g = 0.0f;
+        if (a < s->dim) {
+          float plus = c[a] + 1 < dims[a] ? phi[l + step[a]] : bg;
+          float minus = c[a] >= 1 ? phi[l - step[a]] : bg;
+          float diff = plus - minus;
+          g = (float)((double)diff * half_inv_h);
+        }
+        s->ls[slot].grad[l * 3 + a] = g;
+      }
+    }
+  }
+  for (int a = 0; a < 3; ++a) {
+    s->ls[slot].n[a] = dims[a];
+    s->ls[slot].org[a] = a < s->dim ? origin[a] : 0.0;
+  }
+  s->ls[slot].h = spacing;
+  s->ls[slot].inv_h = 1.0 / spacing;
+  s->ls[slot].background = (double)bg;
+  return 0;
+}
+
 /* advanceStep, simulation.cpp:219-273, plus the loop body of simulate(),
  * simulation.cpp:175-200.  Returns the number of steps executed. */
 int orc_step(orc* s, int nsteps) {
@@ -2076,6 +2174,10 @@ void orc_destroy(orc* s) {
   free(s->Fe); free(s->eps_pl_dev); free(s->eps_pl_vol); free(s->eps_pl_vol_pradhana);
   free(s->delta_gamma); free(s->viscosity); free(s->muI); free(s->keys); free(s->gsrc); free(s->gpos);
   free(s->gx); free(s->gy); free(s->gz); free(s->gmass); free(s->gv); free(s->gflip); free(s->gfric);
+  for (int i = 0; i < MTR_MAX_LEVELSETS; ++i) {
+    free(s->ls[i].phi);
+    free(s->ls[i].grad);
+  }
   free(s);
 }
 

@@ -164,3 +164,40 @@ def max_rel(a, b):
     b = np.asarray(b, dtype=np.float64)
     s = max(np.abs(b).max(initial=0.0), 1e-300)
     return float(np.abs(a - b).max(initial=0.0) / s)
+
+
+def levelset_cases(dim):
+    """Dense level-set objects (ObjectKind.LevelSet) intersecting a block at the
+    origin: name -> (objects, levelsets)."""
+    lo, hi = [-0.05] * dim, [0.1] * dim
+    h = 0.004
+    c = np.array([0.025, -0.004, 0.025][:dim])
+
+    def sphere(X):
+        return np.linalg.norm(X - c, axis=1) - 0.02
+
+    def sphere_normals(ls):
+        n = [ls.phi.shape[a] for a in range(dim)]
+        axes = [ls.origin[a] + ls.spacing * np.arange(n[a]) for a in range(dim)]
+        X = np.stack(np.meshgrid(*axes, indexing="ij"), axis=-1).reshape(-1, dim)
+        d = X - c
+        d /= np.maximum(np.linalg.norm(d, axis=1, keepdims=True), 1e-30)
+        out = np.zeros((X.shape[0], 3), dtype=np.float32)
+        out[:, :dim] = d
+        return out.reshape(ls.phi.shape + (3,))
+
+    terrain = make_object(ObjectKind.TerrainGauss, BC.SlipFree, 0.45,
+                          [0.005, 2, 0.03, 0.03, 0.01, 0.02, 0.05, 0.01, 0.015, 0.015])
+    out = {}
+    s0 = scenes.sample_levelset(sphere, lo, hi, h, dim, slot=0)
+    out["sphere_slipstick"] = ([make_object(ObjectKind.LevelSet, BC.SlipStick, 0.4, [0])], [s0])
+    s1 = scenes.sample_levelset(sphere, lo, hi, h, dim, slot=2)
+    s1.normals = sphere_normals(s1)
+    out["sphere_normals_slipfree"] = ([make_object(ObjectKind.LevelSet, BC.SlipFree, 0.3, [2])], [s1])
+    t = scenes.terrain_levelset(terrain, dim, lo, hi, h, slot=1)
+    out["terrain_slipfree"] = ([make_object(ObjectKind.LevelSet, BC.SlipFree, 0.45, [1])], [t])
+    small = scenes.sample_levelset(sphere, [0.0] * dim, [0.03] * dim, h, dim, slot=3)  # ends inside the block
+    out["partial_lattice_noslip_and_ground"] = (
+        [make_object(ObjectKind.LevelSet, BC.NoSlip, 0.0, [3]),
+         make_object(ObjectKind.Ground, BC.SlipFree, 0.2, [0.008])], [small])
+    return out

@@ -20,7 +20,7 @@ def run_gpu(scene, nsteps, keep_pic_flip=True, graphs=True):
     from matter_tests_b200.gpu import GpuSim
     g = GpuSim(scene.params)
     g.upload(scene.x, scene.v, scene.F, scene.B, scene.scalars)
-    g.set_objects(scene.plates, scene.objects)
+    g.set_scene_objects(scene)
     if keep_pic_flip:
         g.keep_pic_flip(True)
     if not graphs:
@@ -35,6 +35,8 @@ def run_gpu(scene, nsteps, keep_pic_flip=True, graphs=True):
 def run_oracle(scene, nsteps):
     o = Oracle(scene.params)
     o.set_particles(scene.x, scene.v, scene.F, scene.B, scene.scalars)
+    for ls in getattr(scene, "levelsets", ()):
+        o.set_levelset(ls)
     o.set_objects(scene.plates, scene.objects)
     n = o.step(nsteps)
     out = dict(n=n, p=o.particles(), g=o.grid(), c=o.clock(), keys=o.keys(), plates=o.plates())

@@ -249,6 +249,31 @@ def test_saved_frames_have_the_reference_columns_and_the_run_state(tmp_path, dim
     assert (run / "last_written.txt").read_text().strip() == str(n)
 
 
+@pytest.mark.parametrize("dim", [3, 2])
+def test_user_object_setup_builds(tmp_path, dim):
+    assert os.path.exists(build_setup(os.path.join(SETUPS, "host_baked.cpp"), tmp_path, dim, 2))
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")
+@pytest.mark.parametrize("dim", [3, 2])
+def test_user_object_is_baked_and_steers_like_the_builtin(tmp_path, dim):
+    """A user subclass of ObjectGeneral (inside()/normal() only) is baked into a
+    dense level set at dx/4 and steers a falling block like the built-in
+    analytic object it delegates to: final positions within 2% of dx on
+    average and 0.5 dx at most."""
+    exe = build_setup(os.path.join(SETUPS, "host_baked.cpp"), tmp_path, dim, 2)
+    out = {}
+    for mode in ("builtin", "user"):
+        path = tmp_path / f"{mode}.bin"
+        r = subprocess.run([exe, mode, str(path)], capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+        raw = np.fromfile(path)
+        out[mode] = raw[1:].reshape(int(raw[0]), dim)
+    err = np.abs(out["user"] - out["builtin"])
+    assert err.mean() <= 0.02 * 0.01 and err.max() <= 0.5 * 0.01, (err.mean(), err.max())
+
+
 KATS = ["BoundaryTest.AnalyticSlipFree", "BoundaryTest.AnalyticSlipStick", "CoulombFrictionTest.PlateSlipFree",
         "CoulombFrictionTest.PlateSlipStick", "CoulombFrictionTest.GeneralSlipFree",
         "CoulombFrictionTest.GeneralSlipStick", "BoundaryTest.MIBF", "ElasticityTest.BulkModulus",
