@@ -347,7 +347,9 @@ def measure(args, world, rank, local, sc, precision, sampler=None):
     g.set_objects(sc.plates, sc.objects)
     g.step(args.warmup)
     # block shapes of the tile kernels, tuned on the warmed-up scene (setup, untimed)
-    shapes = g.tile_threads if args.no_autotune else g.autotune(args.tune_reps)
+    if not args.no_autotune:
+        g.autotune(args.tune_reps)
+    shapes = {"threads": g.tile_threads, "lanes_per_particle": g.tile_lanes}
     stream = torch.cuda.ExternalStream(g.stream, device=torch.device("cuda", local))
     barrier(world)
     torch.cuda.synchronize(local)
@@ -491,7 +493,7 @@ def ensemble_measure(args, local):
     sims = [make(sc) for sc in scs]
     batch = GpuBatch(sims)
     batch.step(W)
-    default = [gr["tile_threads"] for gr in batch.groups()]
+    default = [(gr["tile_threads"], gr["tile_lanes"]) for gr in batch.groups()]
     if not args.no_autotune:
         batch.autotune(args.tune_reps)  # setup, untimed: trial steps leave the scenes as they are
     groups = batch.groups()
@@ -501,12 +503,13 @@ def ensemble_measure(args, local):
     # 16 steps so that both see the same states
     ab = None
     if not args.no_autotune:
-        tuned = [gr["tile_threads"] for gr in groups]
+        tuned = [(gr["tile_threads"], gr["tile_lanes"]) for gr in groups]
         t_ms = {"tuned": 0.0, "default": 0.0}
         for _ in range(4):
             for name, shapes in (("default", default), ("tuned", tuned)):
-                for gi, sh in enumerate(shapes):
-                    batch.set_tile_threads(gi, sh)
+                for gi, (th, ln) in enumerate(shapes):
+                    batch.set_tile_threads(gi, th)
+                    batch.set_tile_lanes(gi, ln)
                 t_ms[name] += timed(batch, 16)
         ab = {"tuned_over_default": t_ms["default"] / t_ms["tuned"], "steps_each": 64,
               "timed": "4 interleaved rounds of 16 batched steps per shape set, CUDA events"}

@@ -327,11 +327,23 @@ typedef struct mtr_group_info {
   int32_t plastic_model_kernel; /* model the return mapping is compiled for, -1: any */
   int32_t members;
   int32_t tile_threads[4];
+  int32_t tile_lanes[2];        /* lanes per particle of the P2G and MUSL scatters */
 } mtr_group_info;
 int mtr_autotune(mtr_ctx* ctx, int reps, int* threads /* [4] out, may be NULL */);
 int mtr_set_tile_threads(mtr_ctx* ctx, const int* threads /* [4] */);
 int mtr_get_tile_threads(mtr_ctx* ctx, int* threads /* [4] */);
+/* Lanes per particle of the two scatters, lanes[0] P2G and lanes[1] MUSL: the
+ * warp lanes that share one particle's stencil (3D: 16, each lane one (y, z)
+ * column of 4 x nodes, or 32, each lane 2 of a column's x nodes; 2D: 4 or 8).
+ * A warp scatters 32 / lanes particles at a time.  mtr_autotune tunes them
+ * with the block sizes (candidates 64/128/256 threads x both lane counts). */
+int mtr_set_tile_lanes(mtr_ctx* ctx, const int* lanes /* [2] */);
+int mtr_get_tile_lanes(mtr_ctx* ctx, int* lanes /* [2] */);
+int mtr_batch_set_tile_lanes(mtr_batch* batch, int group, const int* lanes /* [2] */);
 int mtr_batch_autotune(mtr_batch* batch, int reps);
+/* The clocks of the members (in mtr_batch_create order) as of the end of the
+ * last mtr_batch_step, without a device round trip; returns the member count. */
+int mtr_batch_clocks(mtr_batch* batch, mtr_clock* clocks, int n);
 int mtr_batch_groups(mtr_batch* batch);
 int mtr_batch_get_group(mtr_batch* batch, int group, mtr_group_info* info);
 int mtr_batch_set_tile_threads(mtr_batch* batch, int group, const int* threads /* [4] */);

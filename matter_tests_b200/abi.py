@@ -110,11 +110,14 @@ class MtrClock(C.Structure):
 
 class MtrGroupInfo(C.Structure):
     _fields_ = [("dim", C.c_int32), ("spline_deg", C.c_int32), ("fp32", C.c_int32), ("musl", C.c_int32),
-                ("plastic_model_kernel", C.c_int32), ("members", C.c_int32), ("tile_threads", C.c_int32 * 4)]
+                ("plastic_model_kernel", C.c_int32), ("members", C.c_int32), ("tile_threads", C.c_int32 * 4),
+                ("tile_lanes", C.c_int32 * 2)]
 
 
-# slots of the tile-kernel block shapes (MTR_TILE_*)
+# slots of the tile-kernel block shapes (MTR_TILE_*); the first two are the
+# scatters, which also have a lanes-per-particle choice
 TILE_SLOTS = ("p2g", "musl", "g2p", "defgrad")
+SCATTER_SLOTS = TILE_SLOTS[:2]
 
 
 def default_params(dim=3, spline_deg=2):

@@ -115,6 +115,17 @@ bool valid_tile_threads(const int* t) {
   return true;
 }
 
+// Lanes per particle of the two scatters (P2G, MUSL): the stencil columns of
+// a particle's cell (16 in 3D, 4 in 2D) times the split of each column's 4 x
+// nodes over 1 or 2 lanes; a warp then takes 32 / lanes particles at a time.
+constexpr int kScatterSlots = 2;
+int scatter_columns(int dim) { return dim == 3 ? 16 : 4; }
+bool valid_tile_lanes(int dim, const int* lanes) {
+  for (int i = 0; i < kScatterSlots; ++i)
+    if (lanes[i] != scatter_columns(dim) && lanes[i] != 2 * scatter_columns(dim)) return false;
+  return true;
+}
+
 }  // namespace
 
 struct mtr_ctx {
@@ -160,6 +171,7 @@ struct mtr_ctx {
   bool use_graphs = true;
   uint32_t step_limit = 0xffffffffu;  // mtr_set_step_limit: no step beyond this step count
   int tile_threads[kTileSlots] = {kChunk, kChunk, kChunk, kChunk};
+  int tile_split[kScatterSlots] = {1, 1};  // x-node split of the P2G and MUSL scatters (1 or 2)
   // a trial step runs every kernel of a step but the commit (k_tail): the
   // particle buffer it reads and the clock stay as they were
   bool trial = false;
@@ -262,9 +274,13 @@ void mark(mtr_ctx* c, const char* name) { c->marks.record(name, c->stream); }
 
 template <int D, int DEG, typename R>
 void set_kernel_attributes_t() {
-  CK(cudaFuncSetAttribute(k_p2g_w<D, DEG, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  CK(cudaFuncSetAttribute(k_p2g_w<D, DEG, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)p2g_smem_bytes<D, R>(kMaxTileThreads)));
-  CK(cudaFuncSetAttribute(k_g2p_musl_w<D, DEG, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  CK(cudaFuncSetAttribute(k_p2g_w<D, DEG, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)p2g_smem_bytes<D, R>(kMaxTileThreads)));
+  CK(cudaFuncSetAttribute(k_g2p_musl_w<D, DEG, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)musl_smem_bytes<D, R>(kMaxTileThreads)));
+  CK(cudaFuncSetAttribute(k_g2p_musl_w<D, DEG, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)musl_smem_bytes<D, R>(kMaxTileThreads)));
 }
 
@@ -410,7 +426,13 @@ int enqueue_step_t(mtr_ctx* c, int parity) {
   ++n;
   mark(c, "k_tile_ranges");
   const int* tt = c->tile_threads;
-  k_p2g_w<D, DEG, R><<<c->cap_tiles, tt[kSlotP2G], p2g_smem_bytes<D, R>(tt[kSlotP2G]), st>>>(A, perm);
+  {
+    const size_t sm = p2g_smem_bytes<D, R>(tt[kSlotP2G]);
+    if (c->tile_split[kSlotP2G] == 2)
+      k_p2g_w<D, DEG, R, 2><<<c->cap_tiles, tt[kSlotP2G], sm, st>>>(A, perm);
+    else
+      k_p2g_w<D, DEG, R, 1><<<c->cap_tiles, tt[kSlotP2G], sm, st>>>(A, perm);
+  }
   ++n;
   mark(c, "k_p2g");
   if (c->prm.pbc) {
@@ -425,7 +447,11 @@ int enqueue_step_t(mtr_ctx* c, int parity) {
   if (c->prm.use_musl) {
     CK(cudaMemsetAsync(c->v2, 0, sizeof(double) * D * c->cap_nodes, st));
     mark(c, "memset(v2)");
-    k_g2p_musl_w<D, DEG, R><<<c->cap_tiles, tt[kSlotMUSL], musl_smem_bytes<D, R>(tt[kSlotMUSL]), st>>>(A, perm);
+    const size_t sm = musl_smem_bytes<D, R>(tt[kSlotMUSL]);
+    if (c->tile_split[kSlotMUSL] == 2)
+      k_g2p_musl_w<D, DEG, R, 2><<<c->cap_tiles, tt[kSlotMUSL], sm, st>>>(A, perm);
+    else
+      k_g2p_musl_w<D, DEG, R, 1><<<c->cap_tiles, tt[kSlotMUSL], sm, st>>>(A, perm);
     mark(c, "k_g2p_musl");
     k_musl_norm<D, R><<<gblocks, 256, 0, st>>>(A);
     mark(c, "k_musl_norm");
@@ -688,6 +714,7 @@ struct mtr_batch_group {
   uint32_t* doff = nullptr;   // [kBK_KINDS][n + 1]
   uint32_t total[kBK_KINDS] = {};
   int tile_threads[kTileSlots] = {kChunk, kChunk, kChunk, kChunk};
+  int tile_split[kScatterSlots] = {1, 1};
 };
 
 struct mtr_batch {
@@ -701,6 +728,7 @@ struct mtr_batch {
   int launches_per_step = 0;
   bool trial = false;  // trial steps: no kb_tail (see mtr_ctx::trial)
   EventMarks marks;    // tagged with the group index
+  int sms = 148;       // multiprocessors of the device (persistent tile-kernel grids)
 };
 
 namespace {
@@ -749,6 +777,18 @@ void build_group_tables(mtr_batch* b, mtr_batch_group& g) {
   CK(cudaStreamSynchronize(b->stream));
 }
 
+// Launches a persistent batched tile kernel (batch_tiles): as many blocks as
+// the GPU holds at once for this kernel and shape, at most one per tile block.
+template <typename R>
+void launch_tiles(const mtr_batch* b, void (*kernel)(BatchView<R>), uint32_t total, int threads, size_t smem,
+                  cudaStream_t st, const BatchView<R>& B) {
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+  const uint64_t cap = (uint64_t)std::max(per_sm, 1) * (uint64_t)b->sms;
+  const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(total, cap));
+  kernel<<<grid, threads, smem, st>>>(B);
+}
+
 template <int D, int DEG, typename R>
 int enqueue_group_step_t(mtr_batch* b, mtr_batch_group& g, int gi) {
   cudaStream_t st = b->stream;
@@ -767,39 +807,33 @@ int enqueue_group_step_t(mtr_batch* b, mtr_batch_group& g, int gi) {
   }
   kb_tile_ranges<R><<<g.total[kBK_TILES], 256, 0, st>>>(B);
   b->marks.record("kb_tile_ranges", st, gi);
-  kb_p2g_w<D, DEG, R><<<g.total[kBK_TILEK], tt[kSlotP2G], p2g_smem_bytes<D, R>(tt[kSlotP2G]), st>>>(B);
+  const uint32_t tiles = g.total[kBK_TILEK];
+  launch_tiles<R>(b, g.tile_split[kSlotP2G] == 2 ? kb_p2g_w<D, DEG, R, 2> : kb_p2g_w<D, DEG, R, 1>, tiles,
+                  tt[kSlotP2G], p2g_smem_bytes<D, R>(tt[kSlotP2G]), st, B);
   b->marks.record(kSlotMark[kSlotP2G], st, gi);
   kb_grid<D, R><<<g.total[kBK_NODES], 256, 0, st>>>(B);
   b->marks.record("kb_grid", st, gi);
   n += 3;
   if (g.musl) {
-    kb_g2p_musl_w<D, DEG, R><<<g.total[kBK_TILEK], tt[kSlotMUSL], musl_smem_bytes<D, R>(tt[kSlotMUSL]), st>>>(B);
+    launch_tiles<R>(b, g.tile_split[kSlotMUSL] == 2 ? kb_g2p_musl_w<D, DEG, R, 2> : kb_g2p_musl_w<D, DEG, R, 1>,
+                    tiles, tt[kSlotMUSL], musl_smem_bytes<D, R>(tt[kSlotMUSL]), st, B);
     b->marks.record(kSlotMark[kSlotMUSL], st, gi);
     kb_musl_norm<D, R><<<g.total[kBK_NODES], 256, 0, st>>>(B);
     b->marks.record("kb_musl_norm", st, gi);
-    const int td = tt[kSlotDefgrad];
+    void (*kd)(BatchView<R>) = kb_defgrad_t<D, DEG, R>;
     if constexpr (D == 3) {
-      if (g.spm == MTR_PM_DPMUI)
-        kb_defgrad_t<D, DEG, R, MTR_PM_DPMUI><<<g.total[kBK_TILEK], td, 0, st>>>(B);
-      else
-        kb_defgrad_t<D, DEG, R><<<g.total[kBK_TILEK], td, 0, st>>>(B);
-    } else {
-      kb_defgrad_t<D, DEG, R><<<g.total[kBK_TILEK], td, 0, st>>>(B);
+      if (g.spm == MTR_PM_DPMUI) kd = kb_defgrad_t<D, DEG, R, MTR_PM_DPMUI>;
     }
+    launch_tiles<R>(b, kd, tiles, tt[kSlotDefgrad], 0, st, B);
     b->marks.record(kSlotMark[kSlotDefgrad], st, gi);
     n += 3;
   } else {
-    const int tg = tt[kSlotG2P];
+    void (*kg)(BatchView<R>) = kb_g2p_t<D, DEG, R>;
     if constexpr (D == 3) {
-      if (g.spm == MTR_PM_DP)
-        kb_g2p_t<D, DEG, R, MTR_PM_DP><<<g.total[kBK_TILEK], tg, 0, st>>>(B);
-      else if (g.spm == MTR_PM_MCCVISC)
-        kb_g2p_t<D, DEG, R, MTR_PM_MCCVISC><<<g.total[kBK_TILEK], tg, 0, st>>>(B);
-      else
-        kb_g2p_t<D, DEG, R><<<g.total[kBK_TILEK], tg, 0, st>>>(B);
-    } else {
-      kb_g2p_t<D, DEG, R><<<g.total[kBK_TILEK], tg, 0, st>>>(B);
+      if (g.spm == MTR_PM_DP) kg = kb_g2p_t<D, DEG, R, MTR_PM_DP>;
+      if (g.spm == MTR_PM_MCCVISC) kg = kb_g2p_t<D, DEG, R, MTR_PM_MCCVISC>;
     }
+    launch_tiles<R>(b, kg, tiles, tt[kSlotG2P], 0, st, B);
     b->marks.record(kSlotMark[kSlotG2P], st, gi);
     ++n;
   }
@@ -829,9 +863,13 @@ int enqueue_batch_step(mtr_batch* b) {
 
 template <int D, int DEG, typename R>
 void set_batch_attributes_t() {
-  CK(cudaFuncSetAttribute(kb_p2g_w<D, DEG, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  CK(cudaFuncSetAttribute(kb_p2g_w<D, DEG, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)p2g_smem_bytes<D, R>(kMaxTileThreads)));
-  CK(cudaFuncSetAttribute(kb_g2p_musl_w<D, DEG, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  CK(cudaFuncSetAttribute(kb_p2g_w<D, DEG, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)p2g_smem_bytes<D, R>(kMaxTileThreads)));
+  CK(cudaFuncSetAttribute(kb_g2p_musl_w<D, DEG, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)musl_smem_bytes<D, R>(kMaxTileThreads)));
+  CK(cudaFuncSetAttribute(kb_g2p_musl_w<D, DEG, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)musl_smem_bytes<D, R>(kMaxTileThreads)));
 }
 
@@ -888,12 +926,18 @@ void write_batch_headers(mtr_batch* b) {
   CK(cudaStreamSynchronize(b->stream));
 }
 
-// Block-shape tuning.  best[slot][k] is the shortest time seen for the slot's
-// kernel with candidate k (infinity: not measured).  A slot keeps `current`
-// unless another candidate was more than 2% faster, so timing noise does not
-// flip an equal choice.
+// Block-shape tuning over kTuneRounds candidates: candidate k runs every tile
+// kernel with kTileCandidates[k % 3] threads (capped at the slot's maximum)
+// and the scatters with x split 1 + k / 3 (16 or 32 lanes per particle in 3D,
+// 4 or 8 in 2D).  best[slot][k] is the shortest time seen for the slot's
+// kernel with candidate k (infinity: not measured); for the gathers, whose
+// shape is the thread count alone, rounds k and k + 3 are the same candidate.
+// A slot keeps its current shape unless another candidate was more than 2%
+// faster, so timing noise does not flip an equal choice.
+constexpr int kTuneRounds = 6;
+
 struct TuneTimes {
-  double best[kTileSlots][3];
+  double best[kTileSlots][kTuneRounds];
   TuneTimes() {
     for (auto& r : best)
       for (double& v : r) v = 1e300;
@@ -902,24 +946,29 @@ struct TuneTimes {
     for (int sl = 0; sl < kTileSlots; ++sl)
       if (std::strcmp(name, kSlotMark[sl]) == 0) best[sl][k] = std::min(best[sl][k], (double)ms);
   }
-  void choose(int* threads) const {
+  void choose(int* threads, int* split) const {
     for (int sl = 0; sl < kTileSlots; ++sl) {
+      const bool scatter = sl < kScatterSlots;
+      const int nk = scatter ? kTuneRounds : 3;
+      auto time_of = [&](int k) { return scatter ? best[sl][k] : std::min(best[sl][k], best[sl][k + 3]); };
       int cur = -1, arg = -1;
-      for (int k = 0; k < 3; ++k) {
-        if (kTileCandidates[k] > kSlotMax[sl] || best[sl][k] >= 1e300) continue;
-        if (kTileCandidates[k] == threads[sl]) cur = k;
-        if (arg < 0 || best[sl][k] < best[sl][arg]) arg = k;
+      for (int k = 0; k < nk; ++k) {
+        if (kTileCandidates[k % 3] > kSlotMax[sl] || time_of(k) >= 1e300) continue;
+        if (kTileCandidates[k % 3] == threads[sl] && (!scatter || 1 + k / 3 == split[sl])) cur = k;
+        if (arg < 0 || time_of(k) < time_of(arg)) arg = k;
       }
       if (arg < 0) continue;  // the slot's kernel does not run in this step
-      if (cur >= 0 && best[sl][cur] <= 1.02 * best[sl][arg]) continue;
-      threads[sl] = kTileCandidates[arg];
+      if (cur >= 0 && time_of(cur) <= 1.02 * time_of(arg)) continue;
+      threads[sl] = kTileCandidates[arg % 3];
+      if (scatter) split[sl] = 1 + arg / 3;
     }
   }
 };
 
-// the candidate shapes of round k for every slot
-void set_candidate(int* threads, int k) {
-  for (int sl = 0; sl < kTileSlots; ++sl) threads[sl] = std::min(kTileCandidates[k], kSlotMax[sl]);
+// the shapes of candidate k for every slot
+void set_candidate(int* threads, int* split, int k) {
+  for (int sl = 0; sl < kTileSlots; ++sl) threads[sl] = std::min(kTileCandidates[k % 3], kSlotMax[sl]);
+  for (int sl = 0; sl < kScatterSlots; ++sl) split[sl] = 1 + k / 3;
 }
 
 // Restores flags changed for trial steps even when a step throws.
@@ -1649,6 +1698,23 @@ int mtr_get_tile_threads(mtr_ctx* c, int* threads) {
   return MTR_OK;
 }
 
+int mtr_set_tile_lanes(mtr_ctx* c, const int* lanes) {
+  return guarded([&]() -> int {
+    if (!c || !lanes) throw MtrError{MTR_ERR_INVALID, "null argument"};
+    if (!valid_tile_lanes(c->dim, lanes)) throw MtrError{MTR_ERR_INVALID, "lanes per particle: 16 or 32 (3D), 4 or 8 (2D)"};
+    CK(cudaSetDevice(c->device));
+    for (int i = 0; i < kScatterSlots; ++i) c->tile_split[i] = lanes[i] / scatter_columns(c->dim);
+    free_graphs(c);
+    return MTR_OK;
+  });
+}
+
+int mtr_get_tile_lanes(mtr_ctx* c, int* lanes) {
+  if (!c || !lanes) return MTR_ERR_INVALID;
+  for (int i = 0; i < kScatterSlots; ++i) lanes[i] = c->tile_split[i] * scatter_columns(c->dim);
+  return MTR_OK;
+}
+
 int mtr_autotune(mtr_ctx* c, int reps, int* threads) {
   return guarded([&]() -> int {
     if (!c || reps <= 0) throw MtrError{MTR_ERR_INVALID, "null context or reps <= 0"};
@@ -1677,20 +1743,22 @@ int mtr_autotune(mtr_ctx* c, int reps, int* threads) {
       }
       if (!ready) throw MtrError{MTR_ERR_STATE, "grid kept growing during tuning"};
       TuneTimes tt;
-      int chosen[kTileSlots];
+      int chosen[kTileSlots], chosen_split[kScatterSlots];
       std::copy(c->tile_threads, c->tile_threads + kTileSlots, chosen);
+      std::copy(c->tile_split, c->tile_split + kScatterSlots, chosen_split);
       c->marks.on = true;
       for (int r = 0; r < reps; ++r)
-        for (int k = 0; k < 3; ++k) {
-          set_candidate(c->tile_threads, k);
+        for (int k = 0; k < kTuneRounds; ++k) {
+          set_candidate(c->tile_threads, c->tile_split, k);
           c->marks.reset();
           enqueue_step(c, parity);
           CK(cudaStreamSynchronize(c->stream));
           const auto& L = c->marks.list;
           for (size_t i = 1; i < L.size(); ++i) tt.add(L[i].first, c->marks.since_previous(i), k);
         }
-      tt.choose(chosen);
+      tt.choose(chosen, chosen_split);
       std::copy(chosen, chosen + kTileSlots, c->tile_threads);
+      std::copy(chosen_split, chosen_split + kScatterSlots, c->tile_split);
       *c->hH = saved;  // the trial steps leave no trace: clock, plates, counters as before
       write_header(c);
       CK(cudaStreamSynchronize(c->stream));
@@ -1778,6 +1846,7 @@ int mtr_batch_create(mtr_ctx* const* ctxs, int n, mtr_batch** out) {
     try {
       b->device = ctxs[0]->device;
       CK(cudaSetDevice(b->device));
+      CK(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device));
       CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
       for (int i = 0; i < n; ++i) {
         mtr_ctx* c = ctxs[i];
@@ -1797,6 +1866,7 @@ int mtr_batch_create(mtr_ctx* const* ctxs, int n, mtr_batch** out) {
           g->musl = musl;
           g->spm = spm;
           std::copy(c->tile_threads, c->tile_threads + kTileSlots, g->tile_threads);
+          std::copy(c->tile_split, c->tile_split + kScatterSlots, g->tile_split);
         }
         g->members.push_back(c);
       }
@@ -1859,6 +1929,20 @@ int mtr_batch_step(mtr_batch* b, int nsteps) {
 
 int mtr_batch_groups(mtr_batch* b) { return b ? (int)b->groups.size() : MTR_ERR_INVALID; }
 
+int mtr_batch_clocks(mtr_batch* b, mtr_clock* clocks, int n) {
+  if (!b || !clocks || n < (int)b->members.size()) return MTR_ERR_INVALID;
+  for (size_t i = 0; i < b->members.size(); ++i) {  // host mirrors, read at the end of mtr_batch_step
+    const StepHeader& H = *b->members[i]->hH;
+    clocks[i].time = H.time;
+    clocks[i].dt = H.dt;
+    clocks[i].step = H.step;
+    clocks[i].frame = H.frame;
+    clocks[i].done = H.done;
+    clocks[i].reserved = 0;
+  }
+  return (int)b->members.size();
+}
+
 int mtr_batch_get_group(mtr_batch* b, int group, mtr_group_info* info) {
   if (!b || !info || group < 0 || group >= (int)b->groups.size()) return MTR_ERR_INVALID;
   const mtr_batch_group& g = b->groups[group];
@@ -1869,7 +1953,19 @@ int mtr_batch_get_group(mtr_batch* b, int group, mtr_group_info* info) {
   info->plastic_model_kernel = g.spm;
   info->members = (int)g.members.size();
   std::copy(g.tile_threads, g.tile_threads + kTileSlots, info->tile_threads);
+  for (int i = 0; i < kScatterSlots; ++i) info->tile_lanes[i] = g.tile_split[i] * scatter_columns(g.dim);
   return MTR_OK;
+}
+
+int mtr_batch_set_tile_lanes(mtr_batch* b, int group, const int* lanes) {
+  return guarded([&]() -> int {
+    if (!b || !lanes || group < 0 || group >= (int)b->groups.size()) throw MtrError{MTR_ERR_INVALID, "bad group"};
+    mtr_batch_group& g = b->groups[group];
+    if (!valid_tile_lanes(g.dim, lanes)) throw MtrError{MTR_ERR_INVALID, "lanes per particle: 16 or 32 (3D), 4 or 8 (2D)"};
+    for (int i = 0; i < kScatterSlots; ++i) g.tile_split[i] = lanes[i] / scatter_columns(g.dim);
+    b->dirty = true;
+    return MTR_OK;
+  });
 }
 
 int mtr_batch_set_tile_threads(mtr_batch* b, int group, const int* threads) {
@@ -1926,13 +2022,16 @@ int mtr_batch_autotune(mtr_batch* b, int reps) {
       }
       if (!ready) throw MtrError{MTR_ERR_STATE, "grid kept growing during tuning"};
       std::vector<TuneTimes> tt(b->groups.size());
-      std::vector<std::vector<int>> chosen;
-      for (auto& g : b->groups) chosen.emplace_back(g.tile_threads, g.tile_threads + kTileSlots);
+      std::vector<std::vector<int>> chosen, chosen_split;
+      for (auto& g : b->groups) {
+        chosen.emplace_back(g.tile_threads, g.tile_threads + kTileSlots);
+        chosen_split.emplace_back(g.tile_split, g.tile_split + kScatterSlots);
+      }
       b->marks.on = true;
       b->trial = true;
       for (int r = 0; r < reps; ++r)
-        for (int k = 0; k < 3; ++k) {
-          for (auto& g : b->groups) set_candidate(g.tile_threads, k);
+        for (int k = 0; k < kTuneRounds; ++k) {
+          for (auto& g : b->groups) set_candidate(g.tile_threads, g.tile_split, k);
           b->marks.reset();
           b->marks.record("start", b->stream, -1);
           enqueue_batch_step(b);
@@ -1942,8 +2041,9 @@ int mtr_batch_autotune(mtr_batch* b, int reps) {
             if (b->marks.tag[i] == b->marks.tag[i - 1]) tt[b->marks.tag[i]].add(L[i].first, b->marks.since_previous(i), k);
         }
       for (size_t gi = 0; gi < b->groups.size(); ++gi) {
-        tt[gi].choose(chosen[gi].data());
+        tt[gi].choose(chosen[gi].data(), chosen_split[gi].data());
         std::copy(chosen[gi].begin(), chosen[gi].end(), b->groups[gi].tile_threads);
+        std::copy(chosen_split[gi].begin(), chosen_split[gi].end(), b->groups[gi].tile_split);
       }
     }
     for (size_t i = 0; i < b->members.size(); ++i) *b->members[i]->hH = saved[i];

@@ -698,7 +698,7 @@ constexpr size_t p2g_smem_bytes(int threads) {
   return p2g_crd_bytes<D, R>() + p2g_patch_bytes<D, R>() + sizeof(PStage<D, R>) * (size_t)threads;
 }
 
-template <int D, int DEG, typename R>
+template <int D, int DEG, typename R, int XS = 1>
 __device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t* __restrict__ perm, const uint32_t bid, const uint32_t nblk) {
   using TL = Tiling<D>;
   constexpr int PN = TL::PN, NODES = TL::NODES, NCH = TL::NCH, TB = TL::TB;
@@ -731,10 +731,12 @@ __device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t
   const bool apic = P.flip_ratio < 0;
   const bool mibf = P.use_mibf;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int LPP = D == 3 ? 16 : 4;
+  // XS lanes share a stencil column, each owning HN = 4 / XS of its x nodes
+  constexpr int COLS = D == 3 ? 16 : 4, LPP = COLS * XS, HN = 4 / XS;
   const int q = lane % LPP;
-  const int iy = D == 3 ? (q >> 2) : q;
-  const int iz = D == 3 ? (q & 3) : 0;
+  const int iy = D == 3 ? ((q % COLS) >> 2) : q % COLS;
+  const int iz = D == 3 ? ((q % COLS) & 3) : 0;
+  const int h0 = (q / COLS) * HN;
   // group g takes the consecutive staged particles [g*LPP, (g+1)*LPP) of the
   // warp's 32, so groups work on different cells and their flushes rarely
   // meet on one patch node (interleaving them made both groups flush the same
@@ -787,22 +789,23 @@ __device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t
       S.lb = packed;
     }
     __syncthreads();
-    {  // phase 2: a lane owns one (iy, iz) stencil column and its 4 ix nodes
-      R acc[4][NCH];
+    {  // phase 2: a lane owns one (iy, iz) stencil column and HN of its ix nodes
+      R acc[HN][NCH];
 #pragma unroll
-      for (int h = 0; h < 4; ++h)
+      for (int h = 0; h < HN; ++h)
 #pragma unroll
         for (int ch = 0; ch < NCH; ++ch) acc[h][ch] = R(0.0);
       int cur = -1;
       auto flush = [&]() {
         const int lbx = cur & 15, lby = (cur >> 4) & 15, lbz = cur >> 8;
 #pragma unroll
-        for (int h = 0; h < 4; ++h) {
+        for (int hh = 0; hh < HN; ++hh) {
+          const int h = h0 + hh;
           const int node = D == 3 ? ((lbx + h) * PN + (lby + iy)) * PN + (lbz + iz) : (lbx + h) * PN + (lby + iy);
 #pragma unroll
           for (int ch = 0; ch < NCH; ++ch) {
-            if (acc[h][ch] != R(0.0)) atomicAdd(&patch[ch][node], acc[h][ch]);
-            acc[h][ch] = R(0.0);
+            if (acc[hh][ch] != R(0.0)) atomicAdd(&patch[ch][node], acc[hh][ch]);
+            acc[hh][ch] = R(0.0);
           }
         }
       };
@@ -856,18 +859,19 @@ __device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t
         }
         const R mui = S.mui;
 #pragma unroll
-        for (int h = 0; h < 4; ++h) {
+        for (int hh = 0; hh < HN; ++hh) {
+          const int h = h0 + hh;
           const R wx = S.w[h], dwx = S.dw[h];
           const R weight = wx * wyz;
           if (weight > R(1e-25)) {
             const R pdx = stage_pd<D, R>(S, crd, 0, lbx, h);
-            acc[h][0] += weight;
+            acc[hh][0] += weight;
 #pragma unroll
-            for (int a = 0; a < D; ++a) acc[h][1 + a] += weight * (Tm[a] + Sm[a] * pdx);
-            if (mibf) acc[h][1 + 2 * D] += mui * weight;
+            for (int a = 0; a < D; ++a) acc[hh][1 + a] += weight * (Tm[a] + Sm[a] * pdx);
+            if (mibf) acc[hh][1 + 2 * D] += mui * weight;
           }
 #pragma unroll
-          for (int a = 0; a < D; ++a) acc[h][1 + D + a] += dwx * Pf[a] + wx * Qf[a];
+          for (int a = 0; a < D; ++a) acc[hh][1 + D + a] += dwx * Pf[a] + wx * Qf[a];
         }
       }
       if (cur >= 0) flush();
@@ -886,9 +890,9 @@ __device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t
   }
 }
 
-template <int D, int DEG, typename R>
+template <int D, int DEG, typename R, int XS = 1>
 __global__ void __launch_bounds__(kMaxTileThreads) k_p2g_w(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
-  p2g_w_body<D, DEG, R>(A, perm, blockIdx.x, gridDim.x);
+  p2g_w_body<D, DEG, R, XS>(A, perm, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1444,7 +1448,7 @@ constexpr size_t musl_smem_bytes(int threads) {
   return musl_crd_bytes<D, R>() + musl_patch_bytes<D, R>() + sizeof(MStage<D, R>) * (size_t)threads;
 }
 
-template <int D, int DEG, typename R>
+template <int D, int DEG, typename R, int XS = 1>
 __device__ __forceinline__ void g2p_musl_w_body(const StepArgsT<R>& A, const uint32_t* __restrict__ perm, const uint32_t bid, const uint32_t nblk) {
   using TL = Tiling<D>;
   constexpr int PN = TL::PN, NODES = TL::NODES;
@@ -1474,10 +1478,11 @@ __device__ __forceinline__ void g2p_musl_w_body(const StepArgsT<R>& A, const uin
   const R apicD = (R)P.apicDinverse;
   const bool apic = fr < 0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int LPP = D == 3 ? 16 : 4;
+  constexpr int COLS = D == 3 ? 16 : 4, LPP = COLS * XS, HN = 4 / XS;  // as in k_p2g_w
   const int q = lane % LPP;
-  const int iy = D == 3 ? (q >> 2) : q;
-  const int iz = D == 3 ? (q & 3) : 0;
+  const int iy = D == 3 ? ((q % COLS) >> 2) : q % COLS;
+  const int iz = D == 3 ? ((q % COLS) & 3) : 0;
+  const int h0 = (q / COLS) * HN;
   // consecutive particles per lane group, as in k_p2g_w
   const int kbeg = warp * 32 + (lane / LPP) * LPP, kend = kbeg + LPP;
   for (uint32_t c0 = pb; c0 < pe; c0 += blockDim.x) {
@@ -1561,21 +1566,22 @@ __device__ __forceinline__ void g2p_musl_w_body(const StepArgsT<R>& A, const uin
     }
     __syncthreads();
     {  // phase 2
-      R acc[4][D];
+      R acc[HN][D];
 #pragma unroll
-      for (int h = 0; h < 4; ++h)
+      for (int h = 0; h < HN; ++h)
 #pragma unroll
         for (int a = 0; a < D; ++a) acc[h][a] = R(0.0);
       int cur = -1;
       auto flush = [&]() {
         const int lbx = cur & 15, lby = (cur >> 4) & 15, lbz = cur >> 8;
 #pragma unroll
-        for (int h = 0; h < 4; ++h) {
+        for (int hh = 0; hh < HN; ++hh) {
+          const int h = h0 + hh;
           const int node = D == 3 ? ((lbx + h) * PN + (lby + iy)) * PN + (lbz + iz) : (lbx + h) * PN + (lby + iy);
 #pragma unroll
           for (int a = 0; a < D; ++a) {
-            if (acc[h][a] != R(0.0)) atomicAdd(&vsum[a][node], acc[h][a]);
-            acc[h][a] = R(0.0);
+            if (acc[hh][a] != R(0.0)) atomicAdd(&vsum[a][node], acc[hh][a]);
+            acc[hh][a] = R(0.0);
           }
         }
       };
@@ -1605,12 +1611,13 @@ __device__ __forceinline__ void g2p_musl_w_body(const StepArgsT<R>& A, const uin
           }
         }
 #pragma unroll
-        for (int h = 0; h < 4; ++h) {
+        for (int hh = 0; hh < HN; ++hh) {
+          const int h = h0 + hh;
           const R weight = S.w[h] * wyz;
           if (!(weight > R(1e-25))) continue;
           const R pdx = stage_pd<D, R>(S, crd, 0, lbx, h);
 #pragma unroll
-          for (int a = 0; a < D; ++a) acc[h][a] += weight * (Tm[a] + Sm[a] * pdx);
+          for (int a = 0; a < D; ++a) acc[hh][a] += weight * (Tm[a] + Sm[a] * pdx);
         }
       }
       if (cur >= 0) flush();
@@ -1629,9 +1636,9 @@ __device__ __forceinline__ void g2p_musl_w_body(const StepArgsT<R>& A, const uin
   }
 }
 
-template <int D, int DEG, typename R>
+template <int D, int DEG, typename R, int XS = 1>
 __global__ void __launch_bounds__(kMaxTileThreads) k_g2p_musl_w(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
-  g2p_musl_w_body<D, DEG, R>(A, perm, blockIdx.x, gridDim.x);
+  g2p_musl_w_body<D, DEG, R, XS>(A, perm, blockIdx.x, gridDim.x);
 }
 
 // musl.cpp:80-95: v2 /= (m_i / m_p) (zero where m_i == 0)
@@ -1771,13 +1778,12 @@ struct BatchView {
   int n;
 };
 
-// arguments of this block's scene, its block index b within the scene and the
-// scene's block count nb; null past the last scene
+// arguments of the scene that owns global block g, the block index b within
+// the scene and the scene's block count nb; null past the last scene
 template <typename R>
-__device__ __forceinline__ const StepArgsT<R>* batch_locate(const BatchView<R>& B, int kind, uint32_t& b,
-                                                            uint32_t& nb) {
+__device__ __forceinline__ const StepArgsT<R>* batch_locate_at(const BatchView<R>& B, int kind, uint32_t g,
+                                                               uint32_t& b, uint32_t& nb) {
   const uint32_t* o = B.off + (size_t)kind * (B.n + 1);
-  const uint32_t g = blockIdx.x;
   if (g >= o[B.n]) return nullptr;
   int lo = 0, hi = B.n - 1;  // last scene whose first block is <= g
   while (lo < hi) {
@@ -1791,6 +1797,28 @@ __device__ __forceinline__ const StepArgsT<R>* batch_locate(const BatchView<R>& 
   nb = o[lo + 1] - o[lo];
   const int cur = B.args[lo].H->cur;
   return B.args + (size_t)(cur & 1) * B.n + lo;
+}
+
+template <typename R>
+__device__ __forceinline__ const StepArgsT<R>* batch_locate(const BatchView<R>& B, int kind, uint32_t& b,
+                                                            uint32_t& nb) {
+  return batch_locate_at(B, kind, blockIdx.x, b, nb);
+}
+
+// Persistent form for the tile kernels: the grid is sized to the blocks the
+// GPU holds at once, and each block walks the global tile blocks of all scenes
+// g = blockIdx.x, blockIdx.x + gridDim.x, ...; `body(A, b)` runs one tile.  The
+// loop bound is uniform over the block, so the bodies' barriers stay matched,
+// and a barrier separates the tiles' shared-memory use.
+template <typename R, typename Body>
+__device__ __forceinline__ void batch_tiles(const BatchView<R>& B, Body&& body) {
+  const uint32_t total = B.off[(size_t)kBK_TILEK * (B.n + 1) + B.n];
+  for (uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
+    uint32_t b, nb;
+    const StepArgsT<R>* A = batch_locate_at(B, kBK_TILEK, g, b, nb);
+    __syncthreads();
+    body(*A, b, nb);
+  }
 }
 
 template <int D, typename R>
@@ -1862,11 +1890,9 @@ __global__ void __launch_bounds__(256) kb_tile_ranges(BatchView<R> B) {
   if (A) tile_ranges_body(*A, A->skeys, b, nb);
 }
 
-template <int D, int DEG, typename R>
+template <int D, int DEG, typename R, int XS = 1>
 __global__ void __launch_bounds__(kMaxTileThreads) kb_p2g_w(BatchView<R> B) {
-  uint32_t b, nb;
-  const StepArgsT<R>* A = batch_locate(B, kBK_TILEK, b, nb);
-  if (A) p2g_w_body<D, DEG, R>(*A, A->perm, b, nb);
+  batch_tiles(B, [&](const StepArgsT<R>& A, uint32_t b, uint32_t nb) { p2g_w_body<D, DEG, R, XS>(A, A.perm, b, nb); });
 }
 
 template <int D, typename R>
@@ -1878,16 +1904,14 @@ __global__ void __launch_bounds__(256) kb_grid(BatchView<R> B) {
 
 template <int D, int DEG, typename R, int PM = -1>
 __global__ void __launch_bounds__(kChunk, MTR_G2P_MIN_BLOCKS) kb_g2p_t(BatchView<R> B) {
-  uint32_t b, nb;
-  const StepArgsT<R>* A = batch_locate(B, kBK_TILEK, b, nb);
-  if (A) g2p_t_body<D, DEG, R, PM>(*A, A->perm, b, nb);
+  batch_tiles(B, [&](const StepArgsT<R>& A, uint32_t b, uint32_t nb) { g2p_t_body<D, DEG, R, PM>(A, A.perm, b, nb); });
 }
 
-template <int D, int DEG, typename R>
+template <int D, int DEG, typename R, int XS = 1>
 __global__ void __launch_bounds__(kMaxTileThreads) kb_g2p_musl_w(BatchView<R> B) {
-  uint32_t b, nb;
-  const StepArgsT<R>* A = batch_locate(B, kBK_TILEK, b, nb);
-  if (A) g2p_musl_w_body<D, DEG, R>(*A, A->perm, b, nb);
+  batch_tiles(B, [&](const StepArgsT<R>& A, uint32_t b, uint32_t nb) {
+    g2p_musl_w_body<D, DEG, R, XS>(A, A.perm, b, nb);
+  });
 }
 
 template <int D, typename R>
@@ -1899,9 +1923,9 @@ __global__ void __launch_bounds__(256) kb_musl_norm(BatchView<R> B) {
 
 template <int D, int DEG, typename R, int PM = -1>
 __global__ void __launch_bounds__(MTR_DEFGRAD_BOUNDS) kb_defgrad_t(BatchView<R> B) {
-  uint32_t b, nb;
-  const StepArgsT<R>* A = batch_locate(B, kBK_TILEK, b, nb);
-  if (A) defgrad_t_body<D, DEG, R, PM>(*A, A->perm, b, nb);
+  batch_tiles(B, [&](const StepArgsT<R>& A, uint32_t b, uint32_t nb) {
+    defgrad_t_body<D, DEG, R, PM>(A, A.perm, b, nb);
+  });
 }
 
 template <int D, typename R>

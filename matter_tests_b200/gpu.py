@@ -8,7 +8,8 @@ import os
 
 import numpy as np
 
-from .abi import MtrClock, MtrGroupInfo, MtrObject, MtrParams, MtrPlate, ERROR_NAMES, MTR_OK, SCALARS, TILE_SLOTS
+from .abi import (MtrClock, MtrGroupInfo, MtrObject, MtrParams, MtrPlate, ERROR_NAMES, MTR_OK, SCALARS, SCATTER_SLOTS,
+                  TILE_SLOTS)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmatter_gpu.so")
@@ -26,7 +27,8 @@ EXPORTS = (
     "mtr_footprint", "mtr_ctx_destroy", "mtr_last_error", "mtr_p2g_noalloc",
     "mtr_autotune", "mtr_set_tile_threads", "mtr_get_tile_threads", "mtr_batch_autotune", "mtr_batch_groups",
     "mtr_batch_get_group", "mtr_batch_set_tile_threads", "mtr_frame_columns", "mtr_frame_begin",
-    "mtr_frame_wait", "mtr_get_grid_friction", "mtr_set_levelset",
+    "mtr_frame_wait", "mtr_get_grid_friction", "mtr_set_levelset", "mtr_set_tile_lanes", "mtr_get_tile_lanes",
+    "mtr_batch_set_tile_lanes", "mtr_batch_clocks",
 )
 
 _lib = None
@@ -91,6 +93,10 @@ def load_library(path=LIB_PATH):
     lib.mtr_batch_groups.argtypes = [C.c_void_p]
     lib.mtr_batch_get_group.argtypes = [C.c_void_p, C.c_int, C.POINTER(MtrGroupInfo)]
     lib.mtr_batch_set_tile_threads.argtypes = [C.c_void_p, C.c_int, _I4]
+    lib.mtr_set_tile_lanes.argtypes = [C.c_void_p, _I4]
+    lib.mtr_get_tile_lanes.argtypes = [C.c_void_p, _I4]
+    lib.mtr_batch_set_tile_lanes.argtypes = [C.c_void_p, C.c_int, _I4]
+    lib.mtr_batch_clocks.argtypes = [C.c_void_p, C.POINTER(MtrClock), C.c_int]
     lib.mtr_frame_columns.argtypes = [C.c_void_p, C.POINTER(C.c_char_p), C.c_int]
     lib.mtr_frame_begin.argtypes = [C.c_void_p]
     lib.mtr_frame_wait.argtypes = [C.c_void_p, C.c_double, C.POINTER(_P), C.POINTER(C.c_uint32),
@@ -202,6 +208,20 @@ class GpuSim:
         cur.update(shapes)
         t = (C.c_int * 4)(*[cur[k] for k in TILE_SLOTS])
         _check(self.lib, "mtr_set_tile_threads", self.lib.mtr_set_tile_threads(self.h, t))
+
+    @property
+    def tile_lanes(self):
+        """Lanes per particle of the P2G and MUSL scatters (mtr_get_tile_lanes)."""
+        t = (C.c_int * 2)()
+        _check(self.lib, "mtr_get_tile_lanes", self.lib.mtr_get_tile_lanes(self.h, t))
+        return dict(zip(SCATTER_SLOTS, list(t)))
+
+    @tile_lanes.setter
+    def tile_lanes(self, lanes):
+        cur = self.tile_lanes
+        cur.update(lanes)
+        t = (C.c_int * 2)(*[cur[k] for k in SCATTER_SLOTS])
+        _check(self.lib, "mtr_set_tile_lanes", self.lib.mtr_set_tile_lanes(self.h, t))
 
     # -- stepping -------------------------------------------------------
     def step(self, n=1, check=True):
@@ -368,6 +388,14 @@ class GpuBatch:
     def launch_count(self):
         return self.lib.mtr_batch_launch_count(self.h)
 
+    def clocks(self):
+        """Each member's clock after the last step() (mtr_batch_clocks, no device round trip)."""
+        arr = (MtrClock * len(self.sims))()
+        n = self.lib.mtr_batch_clocks(self.h, arr, len(self.sims))
+        if n < 0:
+            _check(self.lib, "mtr_batch_clocks", n)
+        return [{"time": c.time, "dt": c.dt, "step": c.step, "frame": c.frame, "done": c.done} for c in arr[:n]]
+
     def autotune(self, reps=3):
         """mtr_batch_autotune; returns groups()."""
         _check(self.lib, "mtr_batch_autotune", self.lib.mtr_batch_autotune(self.h, int(reps)))
@@ -381,7 +409,8 @@ class GpuBatch:
             _check(self.lib, "mtr_batch_get_group", self.lib.mtr_batch_get_group(self.h, g, C.byref(info)))
             out.append({"dim": info.dim, "spline_deg": info.spline_deg, "fp32": bool(info.fp32),
                         "musl": bool(info.musl), "plastic_model_kernel": info.plastic_model_kernel,
-                        "members": info.members, "tile_threads": dict(zip(TILE_SLOTS, list(info.tile_threads)))})
+                        "members": info.members, "tile_threads": dict(zip(TILE_SLOTS, list(info.tile_threads))),
+                        "tile_lanes": dict(zip(SCATTER_SLOTS, list(info.tile_lanes)))})
         return out
 
     def set_tile_threads(self, group, shapes):
@@ -389,6 +418,12 @@ class GpuBatch:
         cur.update(shapes)
         t = (C.c_int * 4)(*[cur[k] for k in TILE_SLOTS])
         _check(self.lib, "mtr_batch_set_tile_threads", self.lib.mtr_batch_set_tile_threads(self.h, group, t))
+
+    def set_tile_lanes(self, group, lanes):
+        cur = self.groups()[group]["tile_lanes"]
+        cur.update(lanes)
+        t = (C.c_int * 2)(*[cur[k] for k in SCATTER_SLOTS])
+        _check(self.lib, "mtr_batch_set_tile_lanes", self.lib.mtr_batch_set_tile_lanes(self.h, group, t))
 
     def close(self):
         if getattr(self, "h", None):

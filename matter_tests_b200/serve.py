@@ -146,8 +146,7 @@ class Server:
                 self.tick_members.append(len(active))
                 self.peak_members = max(self.peak_members, len(active))
                 still = []
-                for r in active:
-                    ck = r.sim.clock()
+                for r, ck in zip(active, batch.clocks()):
                     if ck["step"] >= r.steps or ck["done"]:
                         r.done = now()
                         finishing.append(pool.submit(self._finish, r))
@@ -179,10 +178,13 @@ class Server:
         if any(self._key(gr) not in self.shapes for gr in groups):
             groups = batch.autotune(self.tune_reps)
             for gr in groups:
-                self.shapes.setdefault(self._key(gr), gr["tile_threads"])
+                self.shapes.setdefault(self._key(gr), {"threads": gr["tile_threads"], "lanes": gr["tile_lanes"]})
         for i, gr in enumerate(groups):
-            if gr["tile_threads"] != self.shapes[self._key(gr)]:
-                batch.set_tile_threads(i, self.shapes[self._key(gr)])
+            sh = self.shapes[self._key(gr)]
+            if gr["tile_threads"] != sh["threads"]:
+                batch.set_tile_threads(i, sh["threads"])
+            if gr["tile_lanes"] != sh["lanes"]:
+                batch.set_tile_lanes(i, sh["lanes"])
 
     # -- report ---------------------------------------------------------------
     def report(self, done):
@@ -190,6 +192,7 @@ class Server:
         wait = np.array([r.admitted - r.arrival for r in done])
         psteps = sum(r.scene.Np * r.steps for r in done)
         per_step = np.array(self.tick_ms) / self.tick_steps
+        frame = np.array(self.tick_ms)
         span = max(r.done for r in done) - min(r.arrival for r in done)
         return {
             "requests": len(done),
@@ -199,6 +202,8 @@ class Server:
             "request_latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "queue_wait_s": {"p50": float(np.percentile(wait, 50)), "p99": float(np.percentile(wait, 99))},
             "step_latency_ms": {"p50": float(np.percentile(per_step, 50)), "p99": float(np.percentile(per_step, 99))},
+            # a frame of the serving loop = one tick: tick_steps steps of every admitted scene
+            "frame_latency_ms": {"p50": float(np.percentile(frame, 50)), "p99": float(np.percentile(frame, 99))},
             "tick_steps": self.tick_steps,
             "ticks": len(self.tick_ms),
             "peak_members": self.peak_members,

@@ -22,6 +22,14 @@ SHAPES = [
     {"p2g": 256, "musl": 256, "g2p": 128, "defgrad": 256},
     {"p2g": 64, "musl": 256, "g2p": 96, "defgrad": 160},
 ]
+# x split of the scatters' stencil columns per shape: lanes per particle =
+# split x (16 in 3D, 4 in 2D)
+SPLITS = [(2, 2), (2, 1), (1, 2)]
+
+
+def lanes_of(dim, split):
+    cols = 16 if dim == 3 else 4
+    return {"p2g": split[0] * cols, "musl": split[1] * cols}
 
 
 def exact_state(g):
@@ -46,7 +54,8 @@ def test_every_shape_steps_as_the_default(shape):
         ref.close()
         g = make_sim(sc)
         g.tile_threads = SHAPES[shape]
-        assert g.tile_threads == SHAPES[shape]
+        g.tile_lanes = lanes_of(sc.dim, SPLITS[shape])
+        assert g.tile_threads == SHAPES[shape] and g.tile_lanes == lanes_of(sc.dim, SPLITS[shape])
         g.step(9)
         assert_same(state(g), want, sc.params.precision)
         g.close()
@@ -66,6 +75,8 @@ def test_autotune_leaves_the_scene_as_it_was_and_steps_the_same():
         assert all(t in (64, 128, 256) for t in chosen.values())
         assert chosen["g2p"] <= 128
         assert g.tile_threads == chosen
+        cols = 16 if sc.dim == 3 else 4
+        assert all(l in (cols, 2 * cols) for l in g.tile_lanes.values())
         assert_identical(exact_state(g), before)  # trial steps leave no trace
         g.step(7)
         assert_same(state(g), want, sc.params.precision)
@@ -93,6 +104,10 @@ def test_invalid_shapes_are_refused():
         with pytest.raises(MtrFailure):
             g.tile_threads = bad
     assert g.tile_threads == {k: 128 for k in TILE_SLOTS}
+    for bad in ({"p2g": 8}, {"musl": 64}, {"p2g": 4}):  # 3D: 16 or 32
+        with pytest.raises(MtrFailure):
+            g.tile_lanes = bad
+    assert g.tile_lanes == {"p2g": 16, "musl": 16}
     g.close()
 
 
@@ -116,7 +131,9 @@ def test_batch_autotune_and_per_group_shapes():
     for g, b in zip(sims, before):
         assert_identical(exact_state(g), b)
     batch.set_tile_threads(0, SHAPES[1])
-    assert batch.groups()[0]["tile_threads"] == SHAPES[1]
+    lanes = lanes_of(batch.groups()[0]["dim"], (2, 2))
+    batch.set_tile_lanes(0, lanes)
+    assert batch.groups()[0]["tile_threads"] == SHAPES[1] and batch.groups()[0]["tile_lanes"] == lanes
     batch.step(4)
     for sc, g, ref in zip(scs, sims, alone):
         assert_same(state(g), ref, sc.params.precision)
@@ -130,9 +147,11 @@ def test_batch_groups_start_with_their_first_members_shapes():
     sc = scene_set()[2]
     sims = [make_sim(sc), make_sim(sc)]
     sims[0].tile_threads = SHAPES[0]
+    sims[0].tile_lanes = lanes_of(sc.dim, (2, 1))
     batch = GpuBatch(sims)
     gr = batch.groups()
     assert len(gr) == 1 and gr[0]["members"] == 2 and gr[0]["tile_threads"] == SHAPES[0]
+    assert gr[0]["tile_lanes"] == lanes_of(sc.dim, (2, 1))
     assert gr[0]["fp32"] == (sc.params.precision == PREC_MIXED)
     assert sc.params.precision in (PREC_FP64, PREC_MIXED)
     batch.close()

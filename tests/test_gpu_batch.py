@@ -157,3 +157,20 @@ def test_footprint_matches_the_upload(prec):
     g.close()
     used = free0 - free1
     assert 0.8 * used <= est <= 1.25 * used + (32 << 20), (est, used)
+
+
+def test_batch_clocks_match_each_members_clock():
+    from matter_tests_b200.gpu import GpuBatch
+    scs = scene_set()
+    sims = [make_sim(sc) for sc in scs]
+    sims[1].set_step_limit(5)
+    batch = GpuBatch(sims)
+    batch.step(9)
+    got = batch.clocks()
+    assert len(got) == len(sims)
+    for g, ck in zip(sims, got):
+        assert ck == g.clock()
+    assert got[1]["step"] == 5 and got[0]["step"] == 9
+    batch.close()
+    for g in sims:
+        g.close()
