@@ -728,7 +728,6 @@ struct mtr_batch {
   int launches_per_step = 0;
   bool trial = false;  // trial steps: no kb_tail (see mtr_ctx::trial)
   EventMarks marks;    // tagged with the group index
-  int sms = 148;       // multiprocessors of the device (persistent tile-kernel grids)
 };
 
 namespace {
@@ -777,16 +776,11 @@ void build_group_tables(mtr_batch* b, mtr_batch_group& g) {
   CK(cudaStreamSynchronize(b->stream));
 }
 
-// Launches a persistent batched tile kernel (batch_tiles): as many blocks as
-// the GPU holds at once for this kernel and shape, at most one per tile block.
+// Launches a batched tile kernel: one block per tile block of every scene.
 template <typename R>
-void launch_tiles(const mtr_batch* b, void (*kernel)(BatchView<R>), uint32_t total, int threads, size_t smem,
-                  cudaStream_t st, const BatchView<R>& B) {
-  int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
-  const uint64_t cap = (uint64_t)std::max(per_sm, 1) * (uint64_t)b->sms;
-  const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(total, cap));
-  kernel<<<grid, threads, smem, st>>>(B);
+void launch_tiles(void (*kernel)(BatchView<R>), uint32_t total, int threads, size_t smem, cudaStream_t st,
+                  const BatchView<R>& B) {
+  kernel<<<std::max<uint32_t>(1, total), threads, smem, st>>>(B);
 }
 
 template <int D, int DEG, typename R>
@@ -808,14 +802,14 @@ int enqueue_group_step_t(mtr_batch* b, mtr_batch_group& g, int gi) {
   kb_tile_ranges<R><<<g.total[kBK_TILES], 256, 0, st>>>(B);
   b->marks.record("kb_tile_ranges", st, gi);
   const uint32_t tiles = g.total[kBK_TILEK];
-  launch_tiles<R>(b, g.tile_split[kSlotP2G] == 2 ? kb_p2g_w<D, DEG, R, 2> : kb_p2g_w<D, DEG, R, 1>, tiles,
+  launch_tiles<R>(g.tile_split[kSlotP2G] == 2 ? kb_p2g_w<D, DEG, R, 2> : kb_p2g_w<D, DEG, R, 1>, tiles,
                   tt[kSlotP2G], p2g_smem_bytes<D, R>(tt[kSlotP2G]), st, B);
   b->marks.record(kSlotMark[kSlotP2G], st, gi);
   kb_grid<D, R><<<g.total[kBK_NODES], 256, 0, st>>>(B);
   b->marks.record("kb_grid", st, gi);
   n += 3;
   if (g.musl) {
-    launch_tiles<R>(b, g.tile_split[kSlotMUSL] == 2 ? kb_g2p_musl_w<D, DEG, R, 2> : kb_g2p_musl_w<D, DEG, R, 1>,
+    launch_tiles<R>(g.tile_split[kSlotMUSL] == 2 ? kb_g2p_musl_w<D, DEG, R, 2> : kb_g2p_musl_w<D, DEG, R, 1>,
                     tiles, tt[kSlotMUSL], musl_smem_bytes<D, R>(tt[kSlotMUSL]), st, B);
     b->marks.record(kSlotMark[kSlotMUSL], st, gi);
     kb_musl_norm<D, R><<<g.total[kBK_NODES], 256, 0, st>>>(B);
@@ -824,7 +818,7 @@ int enqueue_group_step_t(mtr_batch* b, mtr_batch_group& g, int gi) {
     if constexpr (D == 3) {
       if (g.spm == MTR_PM_DPMUI) kd = kb_defgrad_t<D, DEG, R, MTR_PM_DPMUI>;
     }
-    launch_tiles<R>(b, kd, tiles, tt[kSlotDefgrad], 0, st, B);
+    launch_tiles<R>(kd, tiles, tt[kSlotDefgrad], 0, st, B);
     b->marks.record(kSlotMark[kSlotDefgrad], st, gi);
     n += 3;
   } else {
@@ -833,7 +827,7 @@ int enqueue_group_step_t(mtr_batch* b, mtr_batch_group& g, int gi) {
       if (g.spm == MTR_PM_DP) kg = kb_g2p_t<D, DEG, R, MTR_PM_DP>;
       if (g.spm == MTR_PM_MCCVISC) kg = kb_g2p_t<D, DEG, R, MTR_PM_MCCVISC>;
     }
-    launch_tiles<R>(b, kg, tiles, tt[kSlotG2P], 0, st, B);
+    launch_tiles<R>(kg, tiles, tt[kSlotG2P], 0, st, B);
     b->marks.record(kSlotMark[kSlotG2P], st, gi);
     ++n;
   }
@@ -1846,7 +1840,6 @@ int mtr_batch_create(mtr_ctx* const* ctxs, int n, mtr_batch** out) {
     try {
       b->device = ctxs[0]->device;
       CK(cudaSetDevice(b->device));
-      CK(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device));
       CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
       for (int i = 0; i < n; ++i) {
         mtr_ctx* c = ctxs[i];

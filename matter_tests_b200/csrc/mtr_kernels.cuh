@@ -1805,20 +1805,13 @@ __device__ __forceinline__ const StepArgsT<R>* batch_locate(const BatchView<R>& 
   return batch_locate_at(B, kind, blockIdx.x, b, nb);
 }
 
-// Persistent form for the tile kernels: the grid is sized to the blocks the
-// GPU holds at once, and each block walks the global tile blocks of all scenes
-// g = blockIdx.x, blockIdx.x + gridDim.x, ...; `body(A, b)` runs one tile.  The
-// loop bound is uniform over the block, so the bodies' barriers stay matched,
-// and a barrier separates the tiles' shared-memory use.
+// The tile kernels of a batch run one block per tile block of every scene;
+// `body(A, b, nb)` runs this block's tile.
 template <typename R, typename Body>
 __device__ __forceinline__ void batch_tiles(const BatchView<R>& B, Body&& body) {
-  const uint32_t total = B.off[(size_t)kBK_TILEK * (B.n + 1) + B.n];
-  for (uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
-    uint32_t b, nb;
-    const StepArgsT<R>* A = batch_locate_at(B, kBK_TILEK, g, b, nb);
-    __syncthreads();
-    body(*A, b, nb);
-  }
+  uint32_t b, nb;
+  const StepArgsT<R>* A = batch_locate(B, kBK_TILEK, b, nb);
+  if (A) body(*A, b, nb);
 }
 
 template <int D, typename R>
