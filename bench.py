@@ -158,9 +158,7 @@ class ClockSampler:
 # (profiles/p2g_musl_defgrad_collapse3d_mui.md, dram__bytes_read.sum +
 # dram__bytes_write.sum); reported as the roofline's traffic for that workload
 MEASURED_TRAFFIC = {
-    ("k_p2g", "fp64"): 189.2e6, ("k_p2g", "mixed"): 112.0e6,
-    ("k_g2p_musl", "fp64"): 148.4e6, ("k_g2p_musl", "mixed"): 86.5e6,
-    ("k_defgrad", "fp64"): 308.2e6, ("k_defgrad", "mixed"): 160.7e6,
+    ("k_p2g", "mixed"): 111.4e6, ("k_g2p_musl", "mixed"): 85.8e6, ("k_defgrad", "mixed"): 128.8e6,
 }
 
 
@@ -500,7 +498,8 @@ def ensemble_measure(args, local):
     ms = timed(batch, K)
     launches = batch.launch_count()
     # tuned against default shapes on the same batch, interleaved in rounds of
-    # 16 steps so that both see the same states
+    # 16 steps so that both see the same states; after each switch 8 untimed
+    # steps rebuild the batch's graph outside the timed window
     ab = None
     if not args.no_autotune:
         tuned = [(gr["tile_threads"], gr["tile_lanes"]) for gr in groups]
@@ -510,9 +509,11 @@ def ensemble_measure(args, local):
                 for gi, (th, ln) in enumerate(shapes):
                     batch.set_tile_threads(gi, th)
                     batch.set_tile_lanes(gi, ln)
+                batch.step(8)
                 t_ms[name] += timed(batch, 16)
         ab = {"tuned_over_default": t_ms["default"] / t_ms["tuned"], "steps_each": 64,
-              "timed": "4 interleaved rounds of 16 batched steps per shape set, CUDA events"}
+              "timed": "4 interleaved rounds of 16 batched steps per shape set (after 8 untimed steps each), "
+                       "CUDA events"}
     lat = []
     for _ in range(max(8, K // 8)):
         t0 = time.perf_counter()
