@@ -10,6 +10,11 @@ worker, and the memory it frees admits the next waiting request.  A tick
 advances every member by `tick_steps` steps; each member has a step limit,
 so it stops exactly after the steps it asked for.
 
+Finished contexts are released lazily: a request's result is read back when
+it completes, but its device memory is freed only when the budget needs the
+room for a waiting request (or at the end of the run), because freeing device
+memory waits for the whole GPU to go idle and would stall the running batch.
+
 Block shapes of the tile kernels: the first batch that holds a group key
 (dimension, spline, precision, USL/MUSL, return-mapping kernel) is tuned
 (mtr_batch_autotune, trial steps that leave the scenes as they were); later
@@ -80,6 +85,9 @@ class Server:
         req.result = {k: st[k] for k in self.keep}
         req.result["clock"] = req.sim.clock()
         req.result["status"] = req.sim.status()
+
+    @staticmethod
+    def _release(req):
         req.sim.close()
         req.sim = None
 
@@ -100,6 +108,7 @@ class Server:
         waiting = collections.deque()
         preparing = {}      # future -> request
         finishing = []      # futures
+        retired = collections.deque()  # (finish future, request): read back, memory still held
         active = []
         used = 0
         batch = None
@@ -112,6 +121,12 @@ class Server:
                 t = now()
                 while queue_in and (not realtime or queue_in[0].arrival <= t):
                     waiting.append(queue_in.popleft())
+                # lazy release: free finished requests' memory only when a waiting one needs it
+                while waiting and used + waiting[0].footprint > self.budget and retired:
+                    f, r = retired.popleft()
+                    f.result()
+                    pool.submit(self._release, r).result()
+                    used -= r.footprint
                 # admission: first come, first served, within the memory budget
                 while waiting and used + waiting[0].footprint <= self.budget:
                     r = waiting.popleft()
@@ -149,8 +164,9 @@ class Server:
                 for r, ck in zip(active, batch.clocks()):
                     if ck["step"] >= r.steps or ck["done"]:
                         r.done = now()
-                        finishing.append(pool.submit(self._finish, r))
-                        used -= r.footprint
+                        f = pool.submit(self._finish, r)
+                        finishing.append(f)
+                        retired.append((f, r))
                         done.append(r)
                     else:
                         still.append(r)
@@ -164,7 +180,9 @@ class Server:
                 batch.close()
             for f in finishing:
                 f.result()
-        self.wall_s = now()
+            self.wall_s = now()
+            for f, r in retired:
+                pool.submit(self._release, r).result()
         return done
 
     @staticmethod
