@@ -738,8 +738,11 @@ void free_batch_tables(mtr_batch* b) {
     b->graph = nullptr;
   }
   for (auto& g : b->groups) {
-    dfree(g.dargs);
-    dfree(g.doff);
+    // stream-ordered frees: a plain cudaFree waits for the whole GPU, which
+    // would stall other contexts' work (the serving loop rebuilds batches
+    // while new scenes upload)
+    if (g.dargs) cudaFreeAsync(g.dargs, b->stream);
+    if (g.doff) cudaFreeAsync(g.doff, b->stream);
     g.dargs = nullptr;
     g.doff = nullptr;
   }
@@ -769,8 +772,8 @@ void build_group_tables(mtr_batch* b, mtr_batch_group& g) {
     for (int k = 0; k < kBK_KINDS; ++k) off[(size_t)k * (n + 1) + s + 1] = off[(size_t)k * (n + 1) + s] + cnt[k];
   }
   for (int k = 0; k < kBK_KINDS; ++k) g.total[k] = off[(size_t)k * (n + 1) + n];
-  g.dargs = dalloc<unsigned char>(sizeof(StepArgsT<R>) * args.size());
-  g.doff = dalloc<uint32_t>(off.size());
+  CK(cudaMallocAsync(&g.dargs, sizeof(StepArgsT<R>) * args.size(), b->stream));
+  CK(cudaMallocAsync((void**)&g.doff, sizeof(uint32_t) * off.size(), b->stream));
   CK(cudaMemcpyAsync(g.dargs, args.data(), sizeof(StepArgsT<R>) * args.size(), cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(g.doff, off.data(), sizeof(uint32_t) * off.size(), cudaMemcpyHostToDevice, b->stream));
   CK(cudaStreamSynchronize(b->stream));

@@ -54,7 +54,8 @@ class Server:
     (None keeps it)."""
 
     def __init__(self, budget_bytes, device=0, tick_steps=8, precision=PREC_MIXED, keep_result=("x", "v"),
-                 autotune=True, tune_reps=2):
+                 autotune=True, tune_reps=2, workers=1):
+        self.workers = int(workers)  # threads that prepare, read back and release requests
         self.autotune = autotune
         self.tune_reps = int(tune_reps)
         self.shapes = {}         # group key -> tile-kernel block shapes
@@ -67,6 +68,8 @@ class Server:
         self.tick_members = []   # scenes stepped in each tick
         self.peak_members = 0
         self.peak_bytes = 0
+        # wall time outside the ticks, by cause (seconds)
+        self.host_s = {"idle": 0.0, "batch_build": 0.0, "release": 0.0}
 
     # -- worker-thread jobs -------------------------------------------------
     def _prepare(self, req):
@@ -116,17 +119,19 @@ class Server:
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0
         done = []
-        with cf.ThreadPoolExecutor(max_workers=1) as pool:
+        with cf.ThreadPoolExecutor(max_workers=self.workers) as pool:
             while queue_in or waiting or preparing or active:
                 t = now()
                 while queue_in and (not realtime or queue_in[0].arrival <= t):
                     waiting.append(queue_in.popleft())
                 # lazy release: free finished requests' memory only when a waiting one needs it
                 while waiting and used + waiting[0].footprint > self.budget and retired:
+                    tr = now()
                     f, r = retired.popleft()
                     f.result()
                     pool.submit(self._release, r).result()
                     used -= r.footprint
+                    self.host_s["release"] += now() - tr
                 # admission: first come, first served, within the memory budget
                 while waiting and used + waiting[0].footprint <= self.budget:
                     r = waiting.popleft()
@@ -139,19 +144,23 @@ class Server:
                     r.sim = f.result()
                     active.append(r)
                 if not active:
+                    ti = now()
                     if preparing:
                         cf.wait(list(preparing), return_when=cf.FIRST_COMPLETED)
                     elif queue_in:
                         time.sleep(max(0.0, min(0.05, queue_in[0].arrival - now())))
+                    self.host_s["idle"] += now() - ti
                     continue
                 key = tuple(r.rid for r in active)
                 if key != members_key:
+                    tb = now()
                     if batch is not None:
                         batch.close()
                     batch = GpuBatch([r.sim for r in active])
                     members_key = key
                     if self.autotune:
                         self._shape(batch)
+                    self.host_s["batch_build"] += now() - tb
                 ts = now()
                 for r in active:
                     if r.started is None:
@@ -227,6 +236,7 @@ class Server:
             "peak_members": self.peak_members,
             "mean_members": float(np.mean(self.tick_members)) if self.tick_members else 0.0,
             "peak_bytes": self.peak_bytes,
+            "host_s": dict(self.host_s),
             "budget_bytes": self.budget,
             "tile_threads": {"/".join(str(int(v)) for v in k): sh for k, sh in self.shapes.items()},
         }
