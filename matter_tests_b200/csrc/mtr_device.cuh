@@ -15,6 +15,16 @@
 
 namespace mtr {
 
+// FP64 transcendental functions as out-of-line calls for the return mapping:
+// its kernels stall most on instruction fetch, and one shared copy of each
+// function is smaller than an inlined copy per singular value, branch and
+// model.  The results are those of the functions themselves.
+static __device__ __noinline__ double ool_log(double x) { return log(x); }
+static __device__ __noinline__ double ool_exp(double x) { return exp(x); }
+static __device__ __noinline__ double ool_pow(double x, double y) { return pow(x, y); }
+static __device__ __noinline__ double ool_sinh(double x) { return sinh(x); }
+static __device__ __noinline__ double ool_asinh(double x) { return asinh(x); }
+
 // Constants of Simulation::simulate (simulation.cpp:94-136) plus the public
 // fields the step reads (simulation.hpp:36-106), packed for the device.
 struct DevParams {

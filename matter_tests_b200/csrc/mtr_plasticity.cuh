@@ -85,7 +85,7 @@ __device__ double limited_search(double epv, double epv_t, double epv_delta, dou
   double test_epv = epv;
   while (tries < max_tries) {
     test_epv = epv - scale * epv_delta;
-    double pp0 = SINH ? dmax(p0_min, K * sinh(-xi * test_epv + asinh(p00 / K))) : p00 * exp(-xi * test_epv);
+    double pp0 = SINH ? dmax(p0_min, K * ool_sinh(-xi * test_epv + ool_asinh(p00 / K))) : p00 * ool_exp(-xi * test_epv);
     double pp = K * (test_epv - epv_t) + p_t;
     double val = 2. * pp + (beta - 1.) * pp0;
     double midpoint = (pp0 - beta * pp0) * 0.5;
@@ -117,7 +117,7 @@ __device__ bool mcc_rma_implicit(double& p_io, double& q_io, double M, double p0
   double p = p_io, q = q_io;
   const double Msq = M * M;
   const double damping_factor = 1;
-  double p0 = SINH ? dmax(0.01, K * sinh(-xi * epv + asinh(p00 / K))) : p00 * exp(-xi * epv);
+  double p0 = SINH ? dmax(0.01, K * ool_sinh(-xi * epv + ool_asinh(p00 / K))) : p00 * ool_exp(-xi * epv);
   const double p0_t = p0;
   double y = Msq * (p * p + (beta - 1.) * p0 * p - beta * p0 * p0) + damping_factor * q * q;
   if (y <= 0) return false;
@@ -145,10 +145,10 @@ __device__ bool mcc_rma_implicit(double& p_io, double& q_io, double M, double p0
     p = (epv - epv_t) * K + p_t;
     double p0_helper = 0.0;
     if (SINH) {
-      p0_helper = K * sinh(-xi * epv + asinh(p00 / K));
+      p0_helper = K * ool_sinh(-xi * epv + ool_asinh(p00 / K));
       p0 = dmax(p0_min, p0_helper);
     } else {
-      p0 = p00 * exp(-xi * epv);
+      p0 = p00 * ool_exp(-xi * epv);
     }
     double denom = 2. * K * Msq * p + Msq * (beta - 1.) * K * p0;
     double dg_step = (p_t - p) / denom;
@@ -160,7 +160,7 @@ __device__ bool mcc_rma_implicit(double& p_io, double& q_io, double M, double p0
     double dp_depv = K;
     double dp0_depv;
     if (SINH) {
-      double h = -xi * K * cosh(-xi * epv + asinh(p00 / K));
+      double h = -xi * K * cosh(-xi * epv + ool_asinh(p00 / K));
       dp0_depv = (p0_helper > p0_min) ? 0.5 * (h + h - p0_min) : 0.5 * (h + p0_min - h);
     } else {
       dp0_depv = -xi * p0;
@@ -197,16 +197,16 @@ __device__ inline double perzyna_newton(const DevParams& P, double dt, double q_
     if (iter == max_iter - 1) flags |= MTR_STATUS_RMA_NOCONV;
     double tm = pv * delta_gamma + dt;
     double tmp = dt / tm;
-    double tmp1 = pow(tmp, pe);
+    double tmp1 = ool_pow(tmp, pe);
     double qdiff = 0.0;
     if (is_vm) {
-      double ex = exp(-P.xi * (eps_pl_dev + (1.0 / P.d_prefac) * delta_gamma));
+      double ex = ool_exp(-P.xi * (eps_pl_dev + (1.0 / P.d_prefac) * delta_gamma));
       q_yield = P.q_min + (P.q_max - P.q_min) * ex;
       qdiff = -P.xi / P.d_prefac * (P.q_max - P.q_min) * ex;
     }
     double residual = (q_trial - fm * delta_gamma) * tmp1 - q_yield;
     if (fabs(residual) < 1e-2) break;
-    double residual_diff = -fm * tmp1 + (q_trial - fm * delta_gamma) * pe * pow(tmp, pe - 1) * (-pv * dt) / (tm * tm);
+    double residual_diff = -fm * tmp1 + (q_trial - fm * delta_gamma) * pe * ool_pow(tmp, pe - 1) * (-pv * dt) / (tm * tm);
     if (is_vm) residual_diff -= qdiff;
     if (fabs(residual_diff) < 1e-14) flags |= MTR_STATUS_RESID_DIFF;
     delta_gamma -= residual / residual_diff;
@@ -233,7 +233,7 @@ __device__ __forceinline__ void hencky_tau(const DevParams& P, const double (&U)
 // tau = mu (F F^T - I) + lambda log(det F) I.
 template <int D>
 __device__ __forceinline__ void neohookean_tau(const DevParams& P, const double (&F)[D][D], double* tau) {
-  const double lj = log(mat_det<D>(F));
+  const double lj = ool_log(mat_det<D>(F));
   auto ffT = [&](int i, int j) {
     double s = F[i][0] * F[j][0];
 #pragma unroll
@@ -270,7 +270,7 @@ __device__ void initial_tau(const DevParams& P, const double (&F)[D][D], double*
   double U[D][D], V[D][D], S[D], h[D];
   svd<D>(F, U, S, V, P.svd_rel);
 #pragma unroll
-  for (int i = 0; i < D; ++i) h[i] = log(fabs(S[i]));
+  for (int i = 0; i < D; ++i) h[i] = ool_log(fabs(S[i]));
   hencky_tau<D>(P, U, h, tau);
 }
 
@@ -292,7 +292,7 @@ __device__ bool return_map(const DevParams& P, double dt, double (&F)[D][D], PSc
       double U[D][D], V[D][D], S[D], h[D];
       svd<D>(F, U, S, V, P.svd_rel);
 #pragma unroll
-      for (int i = 0; i < D; ++i) h[i] = log(fabs(S[i]));
+      for (int i = 0; i < D; ++i) h[i] = ool_log(fabs(S[i]));
       hencky_tau<D>(P, U, h, tau);
     }
     return false;
@@ -308,7 +308,7 @@ __device__ bool return_map(const DevParams& P, double dt, double (&F)[D][D], PSc
   svd<D>(F, U, S, V, P.svd_rel);
   double hencky[D], hdev[D];
 #pragma unroll
-  for (int i = 0; i < D; ++i) hencky[i] = log(dmax(fabs(S[i]), 1e-4));  // plasticity.cpp:21
+  for (int i = 0; i < D; ++i) hencky[i] = ool_log(dmax(fabs(S[i]), 1e-4));  // plasticity.cpp:21
   double hencky_trace = hencky[0];
 #pragma unroll
   for (int i = 1; i < D; ++i) hencky_trace += hencky[i];
@@ -370,12 +370,12 @@ __device__ bool return_map(const DevParams& P, double dt, double (&F)[D][D], PSc
     double p_trial = -K * hencky_trace;
     double q_trial = e_mu * hdn;
     double p_tip_orig = -qc / M;
-    double p_tip = p_tip_orig * exp(-P.xi * s.eps_pl_dev);
+    double p_tip = p_tip_orig * ool_exp(-P.xi * s.eps_pl_dev);
     double p_shift = P.use_pradhana ? -K * s.eps_pl_vol_pradhana : 0.0;
     double q_yield = M * (p_trial + p_shift) + (-p_tip * M);
     if ((p_trial + p_shift) <= p_tip) {
       plastic = true;
-      double p_proj = p_tip_orig * exp(-P.xi * s.eps_pl_dev);
+      double p_proj = p_tip_orig * ool_exp(-P.xi * s.eps_pl_dev);
       set_iso(p_proj);
       rewrite = true;
       double delta_gamma = d_pre * hdn;
@@ -392,7 +392,7 @@ __device__ bool return_map(const DevParams& P, double dt, double (&F)[D][D], PSc
     if ((p_trial + p_shift) > p_tip && q_trial > q_yield) {
       plastic = true;
       double temp_eps_pl_dev = s.eps_pl_dev + (hdn - q_yield / e_mu);
-      double p_proj = p_tip_orig * exp(-P.xi * temp_eps_pl_dev);
+      double p_proj = p_tip_orig * ool_exp(-P.xi * temp_eps_pl_dev);
       if ((p_trial + p_shift) < p_proj) {
         double delta_gamma = d_pre * hdn;
         s.delta_gamma = delta_gamma / dt;
@@ -414,9 +414,9 @@ __device__ bool return_map(const DevParams& P, double dt, double (&F)[D][D], PSc
     }
   } else if (pm == MTR_PM_VMVISC) {  // plasticity.cpp:164-238
     double q_trial = e_mu * hdn;
-    double q_yield = P.q_min + (P.q_max - P.q_min) * exp(-P.xi * s.eps_pl_dev);
+    double q_yield = P.q_min + (P.q_max - P.q_min) * ool_exp(-P.xi * s.eps_pl_dev);
     double p_trial = -K * hencky_trace;
-    if (p_trial < P.p_min * exp(-P.xi * s.eps_pl_vol)) {
+    if (p_trial < P.p_min * ool_exp(-P.xi * s.eps_pl_vol)) {
       double delta_gamma = q_trial / f_mu;
       double inst = -p_trial / K;
 #pragma unroll
@@ -543,10 +543,10 @@ __device__ bool return_map(const DevParams& P, double dt, double (&F)[D][D], PSc
     if (hl == MTR_HL_NOHARD && !mui) {
       perform_rma = mcc_rma_explicit(p_stress, q_stress, Mm, p0, beta, P.mu, K, P.rma_prefac);
     } else if (hl == MTR_HL_EXPOEXPL) {
-      p_c = dmax(st, p0 * exp(-xi * s.eps_pl_vol));
+      p_c = dmax(st, p0 * ool_exp(-xi * s.eps_pl_vol));
       perform_rma = mcc_rma_explicit(p_stress, q_stress, Mm, p_c, beta, P.mu, K, P.rma_prefac);
     } else if (hl == MTR_HL_SINHEXPL) {
-      p_c = dmax(st, K * sinh(-xi * s.eps_pl_vol + asinh(p0 / K)));
+      p_c = dmax(st, K * ool_sinh(-xi * s.eps_pl_vol + ool_asinh(p0 / K)));
       perform_rma = mcc_rma_explicit(p_stress, q_stress, Mm, p_c, beta, P.mu, K, P.rma_prefac);
     } else if (hl == MTR_HL_EXPOIMPL) {
       perform_rma = mcc_rma_implicit<false>(p_stress, q_stress, Mm, p0, beta, P.mu, K, xi, s.eps_pl_vol, flags);
@@ -568,9 +568,9 @@ __device__ bool return_map(const DevParams& P, double dt, double (&F)[D][D], PSc
         if (q_trial > (q_stress + st)) {
           const double mu_1 = P.mu_1, mu_2 = P.mu_2, fac_Q = P.fac_Q;
           if (hl == MTR_HL_EXPOIMPL)
-            p_c = dmax(p0 * exp(-xi * s.eps_pl_vol), p_stress + st);
+            p_c = dmax(p0 * ool_exp(-xi * s.eps_pl_vol), p_stress + st);
           else if (hl == MTR_HL_SINHIMPL)
-            p_c = dmax(K * sinh(-xi * s.eps_pl_vol + asinh(p0 / K)), p_stress + st);
+            p_c = dmax(K * ool_sinh(-xi * s.eps_pl_vol + ool_asinh(p0 / K)), p_stress + st);
           double p_special = p_stress + beta * p_c + st;
           double fac_a = f_mu * dt;
           double fac_b =
@@ -603,9 +603,9 @@ __device__ bool return_map(const DevParams& P, double dt, double (&F)[D][D], PSc
           q_stress = dmax(q_yield, q_trial - f_mu * delta_gamma);
           if (P.use_mibf) {
             if (hl == MTR_HL_EXPOIMPL)
-              p_c = dmax(0.0, p0 * exp(-xi * s.eps_pl_vol));
+              p_c = dmax(0.0, p0 * ool_exp(-xi * s.eps_pl_vol));
             else if (hl == MTR_HL_SINHIMPL)
-              p_c = dmax(0.0, K * sinh(-xi * s.eps_pl_vol + asinh(p0 / K)));
+              p_c = dmax(0.0, K * ool_sinh(-xi * s.eps_pl_vol + ool_asinh(p0 / K)));
             if ((p_stress < -beta * p_c + st) || (p_stress > p_c - st))
               s.muI = M;
             else
@@ -639,13 +639,13 @@ __device__ bool return_map(const DevParams& P, double dt, double (&F)[D][D], PSc
     double power = dmin(10.0 * one_minus_Jp, 5.0);
     double lambda0 = (P.E * P.nu) / ((1 + P.nu) * (1 - 2 * P.nu));
     double mu0 = P.E / (2 * (1 + P.nu));
-    double lam = exp(power) * lambda0;
-    double mu = exp(power) * mu0;
+    double lam = ool_exp(power) * lambda0;
+    double mu = ool_exp(power) * mu0;
     double tr = 0.0;
     double lse[D];
 #pragma unroll
     for (int i = 0; i < D; ++i) {
-      lse[i] = log(Sx[i]);
+      lse[i] = ool_log(Sx[i]);
       tr += lse[i];
     }
 #pragma unroll
@@ -658,13 +658,13 @@ __device__ bool return_map(const DevParams& P, double dt, double (&F)[D][D], PSc
   if (rewrite) {
     double e[D];
 #pragma unroll
-    for (int i = 0; i < D; ++i) e[i] = exp(hencky[i]);
+    for (int i = 0; i < D; ++i) e[i] = ool_exp(hencky[i]);
     usv<D>(U, e, V, F);
     hencky_tau<D>(P, U, hencky, tau);
   } else {
     double h[D];
 #pragma unroll
-    for (int i = 0; i < D; ++i) h[i] = log(fabs(S[i]));
+    for (int i = 0; i < D; ++i) h[i] = ool_log(fabs(S[i]));
     hencky_tau<D>(P, U, h, tau);
   }
   return plastic;
