@@ -1259,7 +1259,10 @@ __device__ __forceinline__ void gather_patch(const R* pv, const R* pf, const dou
 #pragma unroll
     for (int c = 0; c < D; ++c) Bp[r][c] = gv[r][c] = R(0.0);
   constexpr int KN = D == 3 ? 4 : 1;
-#pragma unroll
+  // the x layers of the stencil stay a loop: unrolling all 64 nodes made
+  // the return-mapping kernels that call this too large for the instruction
+  // cache
+#pragma unroll 1
   for (int ii = 0; ii < 4; ++ii)
 #pragma unroll
     for (int jj = 0; jj < 4; ++jj) {
