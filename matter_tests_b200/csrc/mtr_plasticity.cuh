@@ -305,7 +305,7 @@ __device__ bool return_map(const DevParams& P, double dt, double (&F)[D][D], PSc
   const double K = P.K, M = P.M, qc = P.q_cohesion;
   const double e_mu = P.e_mu_prefac, d_pre = P.d_prefac, f_mu = P.f_mu_prefac;
   double U[D][D], V[D][D], S[D];
-  svd<D>(F, U, S, V, P.svd_rel);
+  svd<D, PM != MTR_PM_DPMUI>(F, U, S, V, P.svd_rel);
   double hencky[D], hdev[D];
 #pragma unroll
   for (int i = 0; i < D; ++i) hencky[i] = ool_log(dmax(fabs(S[i]), 1e-4));  // plasticity.cpp:21
