@@ -158,7 +158,9 @@ class ClockSampler:
 # (profiles/p2g_musl_defgrad_collapse3d_mui.md, dram__bytes_read.sum +
 # dram__bytes_write.sum); reported as the roofline's traffic for that workload
 MEASURED_TRAFFIC = {
-    ("k_p2g", "mixed"): 111.4e6, ("k_g2p_musl", "mixed"): 85.8e6, ("k_defgrad", "mixed"): 128.8e6,
+    ("k_p2g", "fp64"): 184.4e6, ("k_p2g", "mixed"): 110.9e6,
+    ("k_g2p_musl", "fp64"): 163.8e6, ("k_g2p_musl", "mixed"): 97.2e6,
+    ("k_defgrad", "fp64"): 285.0e6, ("k_defgrad", "mixed"): 134.9e6,
 }
 
 
