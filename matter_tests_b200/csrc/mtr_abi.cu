@@ -880,7 +880,11 @@ void set_batch_attributes(const mtr_batch_group& g) {
   }
 }
 
-constexpr int kBatchGraphSteps = 8;
+// Steps per captured batch graph.  One: a batch is rebuilt (tables, capture,
+// instantiation) whenever its membership changes, which the serving loop does
+// often, and the capture cost grows with the steps captured, while replaying
+// a one-step graph n times costs n graph launches of a few microseconds.
+constexpr int kBatchGraphSteps = 1;
 
 // (re)builds the device tables of every group and captures kBatchGraphSteps steps
 void rebuild_batch(mtr_batch* b) {

@@ -54,7 +54,7 @@ class Server:
     (None keeps it)."""
 
     def __init__(self, budget_bytes, device=0, tick_steps=8, precision=PREC_MIXED, keep_result=("x", "v"),
-                 autotune=True, tune_reps=2, workers=1):
+                 autotune=True, tune_reps=1, workers=1):
         self.workers = int(workers)  # threads that prepare, read back and release requests
         self.autotune = autotune
         self.tune_reps = int(tune_reps)
