@@ -570,17 +570,19 @@ def serve_measure(args, local):
     import numpy as np
     from matter_tests_b200 import scenes
     from matter_tests_b200.serve import Request, Server, poisson_requests
-    # warm-up, untimed: one small request of every kind (dimension x collapse or
-    # incline x material) through a throwaway server loads the batched kernels
-    # of every group the measured run will meet
+    # start-up, untimed: one 200k-particle request of every kind (dimension x
+    # collapse or incline x material) through a warm-up server loads the
+    # batched kernels of every group the measured run will meet and tunes
+    # their shapes; the measured server starts from those shapes
     rng = np.random.default_rng(1)
-    warm = [Request(rid=i, scene=scenes.granular_scene(rng, dim, kind, 3000, mat, 1e6, 30.0, 2.0), steps=16,
+    warm = [Request(rid=i, scene=scenes.granular_scene(rng, dim, kind, 200_000, mat, 1e6, 30.0, 2.0), steps=16,
                     arrival=0.0)
             for i, (dim, kind, mat) in enumerate((d, k, m) for d in (2, 3) for k in ("collapse", "incline")
                                                  for m in ("dp", "mcc", "mui"))]
-    Server(budget_bytes=150e9, device=local, tick_steps=8, precision=PREC_MIXED).run(warm, realtime=False)
+    warm_srv = Server(budget_bytes=150e9, device=local, tick_steps=8, precision=PREC_MIXED)
+    warm_srv.run(warm, realtime=False)
     reqs = poisson_requests(args.serve_requests, rate=20.0, seed=4242, steps=200)
-    srv = Server(budget_bytes=150e9, device=local, tick_steps=8, precision=PREC_MIXED)
+    srv = Server(budget_bytes=150e9, device=local, tick_steps=8, precision=PREC_MIXED, shapes=warm_srv.shapes)
     done = srv.run(reqs)
     rep = srv.report(done)
     serial = {}

@@ -54,11 +54,13 @@ class Server:
     (None keeps it)."""
 
     def __init__(self, budget_bytes, device=0, tick_steps=8, precision=PREC_MIXED, keep_result=("x", "v"),
-                 autotune=True, tune_reps=1, workers=1):
+                 autotune=True, tune_reps=1, workers=1, shapes=None):
         self.workers = int(workers)  # threads that prepare, read back and release requests
         self.autotune = autotune
         self.tune_reps = int(tune_reps)
-        self.shapes = {}         # group key -> tile-kernel block shapes
+        # group key -> tile-kernel block shapes; a server can start from the
+        # shapes another one tuned (a warm-up run at start-up)
+        self.shapes = dict(shapes or {})
         self.budget = int(budget_bytes)
         self.device = device
         self.tick_steps = int(tick_steps)
