@@ -460,9 +460,10 @@ def ensemble_measure(args, local):
     """The batched ensemble: args.ensemble_size seeded DP column collapses
     (5k-300k particles, half 3D), mixed precision, stepped together through
     mtr_batch (one launch per phase per group, CUDA graphs) for
-    args.ensemble_steps timed steps after args.warmup, against the same scenes
-    run one after another through their own contexts.  Step latency: wall
-    time of each graph replay of 8 batched steps / 8."""
+    args.ensemble_steps timed steps after args.warmup and the shape tuner,
+    against the same scenes run one after another through their own contexts
+    (each tuned too).  Step latency: wall time of each mtr_batch_step(8) / 8.
+    shapes_ab: tuned against default shapes, interleaved on the same batch."""
     import numpy as np
     import torch
     from matter_tests_b200 import scenes
