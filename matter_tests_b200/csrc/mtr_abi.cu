@@ -763,7 +763,7 @@ void build_group_tables(mtr_batch* b, mtr_batch_group& g) {
     const uint32_t cnt[kBK_KINDS] = {
         (uint32_t)c->npartials,
         (uint32_t)c->sort_blocks,
-        256u,
+        (uint32_t)(256 / kScanDigitsPerBlock),
         cap_blocks(c->Np, 256, 148 * 8),
         cap_blocks(std::max<uint64_t>(c->cap_tiles, g.musl ? (uint64_t)g.dim * c->cap_nodes : 0), 256, 148 * 8),
         c->cap_tiles,

@@ -464,6 +464,32 @@ static __global__ void __launch_bounds__(256) k_sort_scan(StepCommon A) {
   sort_scan_body(A, blockIdx.x, gridDim.x);
 }
 
+// The same scan with one warp per digit, kScanDigitsPerBlock digits per
+// 256-thread block: the batched form, where most scenes have few sort blocks
+// and a block per digit and scene would leave the blocks nearly idle.
+constexpr int kScanDigitsPerBlock = 8;
+static __device__ __forceinline__ void sort_scan_warp_body(const StepCommon& A, const uint32_t bid) {
+  if (step_inactive(A.H)) return;
+  const int lane = threadIdx.x & 31;
+  const int dgt = (int)bid * kScanDigitsPerBlock + (int)(threadIdx.x >> 5);
+  if (dgt >= 256) return;  // no block-wide barrier below
+  uint32_t* row = A.hist + (size_t)dgt * A.sort_blocks;
+  uint32_t carry = 0;
+  for (int b0 = 0; b0 < A.sort_blocks; b0 += 32) {
+    const int b = b0 + lane;
+    const uint32_t v = b < A.sort_blocks ? row[b] : 0u;
+    uint32_t incl = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, off);
+      if (lane >= off) incl += t;
+    }
+    if (b < A.sort_blocks) row[b] = carry + incl - v;
+    carry += __shfl_sync(0xffffffffu, incl, 31);
+  }
+  if (lane == 0) A.dtot[dgt] = carry;
+}
+
 // Stable scatter.  Elements are ranked round by round (256 at a time, in
 // index order) with warp match + per-warp digit counts, which keeps equal
 // digits in input order.
@@ -1864,7 +1890,7 @@ template <typename R>
 __global__ void __launch_bounds__(256) kb_sort_scan(BatchView<R> B) {
   uint32_t b, nb;
   const StepArgsT<R>* A = batch_locate(B, kBK_SCAN, b, nb);
-  if (A) sort_scan_body(*A, b, nb);
+  if (A) sort_scan_warp_body(*A, b);
 }
 
 template <typename R>
