@@ -274,6 +274,10 @@ int mtr_set_step_limit(mtr_ctx* ctx, uint32_t last_step);
 int mtr_batch_create(mtr_ctx* const* ctxs, int n, mtr_batch** out);
 int mtr_batch_step(mtr_batch* batch, int nsteps);
 int64_t mtr_batch_launch_count(mtr_batch* batch);
+/* Host-side bookkeeping of mtr_batch_step since mtr_batch_create: members'
+ * grid regrowths and the wall milliseconds they took, and batch rebuilds
+ * (device tables and graph capture) and theirs.  Any pointer may be NULL. */
+int mtr_batch_stats(mtr_batch* batch, int64_t* regrowths, double* regrow_ms, int64_t* rebuilds, double* rebuild_ms);
 void* mtr_batch_stream(mtr_batch* batch);
 void mtr_batch_destroy(mtr_batch* batch);
 int mtr_footprint(const mtr_params* params, uint32_t Np, const double* x, uint64_t* bytes);

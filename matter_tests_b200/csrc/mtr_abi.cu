@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <mutex>
 #include <thread>
 #include <type_traits>
 #include <vector>
@@ -213,11 +214,46 @@ int guarded(F&& f) {
   }
 }
 
+// Grid buffers come from a stream-ordered memory pool per device that keeps
+// up to kGridPoolKeep bytes of freed memory for reuse: a spreading scene
+// regrows its grid several times, and a plain cudaFree + cudaMalloc of the
+// grid took 15-50 ms of host time per regrowth (a batch waits for it).
+constexpr uint64_t kGridPoolKeep = 2ull << 30;
+std::mutex g_grid_pool_mutex;
+cudaMemPool_t g_grid_pool[64] = {};
+
+cudaMemPool_t grid_pool(int device) {
+  std::lock_guard<std::mutex> lock(g_grid_pool_mutex);
+  if (device < 0 || device >= 64) throw MtrError{MTR_ERR_INVALID, "device index out of range"};
+  if (!g_grid_pool[device]) {
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    CK(cudaMemPoolCreate(&g_grid_pool[device], &props));
+    uint64_t keep = kGridPoolKeep;
+    CK(cudaMemPoolSetAttribute(g_grid_pool[device], cudaMemPoolAttrReleaseThreshold, &keep));
+  }
+  return g_grid_pool[device];
+}
+
+// n elements of T from the grid pool, ordered on the context's stream
+template <typename T>
+T* galloc(mtr_ctx* c, size_t n) {
+  void* p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMallocFromPoolAsync(&p, n * sizeof(T), grid_pool(c->device), c->stream);
+  if (e != cudaSuccess) throw MtrError{MTR_ERR_OOM, std::string("cudaMallocFromPoolAsync: ") + cudaGetErrorString(e)};
+  return static_cast<T*>(p);
+}
+
 void free_grid(mtr_ctx* c) {
   for (void* p : {(void*)c->gx, (void*)c->gy, (void*)c->gz, (void*)c->acc, (void*)c->nv,
                   (void*)c->nflip, (void*)c->nmass, (void*)c->nfric, (void*)c->v2, (void*)c->tile_begin,
                   (void*)c->tile_end})
-    dfree(p);
+    if (p) cudaFreeAsync(p, c->stream);
   c->gx = c->gy = c->gz = c->nv = c->v2 = nullptr;
   c->acc = c->nflip = c->nmass = c->nfric = nullptr;
   c->tile_begin = c->tile_end = nullptr;
@@ -249,17 +285,17 @@ void alloc_grid(mtr_ctx* c, const uint32_t want[3]) {
   c->cap_tiles = (uint32_t)tiles;
   const int nch = 2 + 2 * d;  // mass, momentum, force, friction
   const size_t rs = c->rsize;
-  c->gx = dalloc<double>(c->cap_axis[0]);
-  c->gy = dalloc<double>(c->cap_axis[1]);
-  c->gz = dalloc<double>(c->cap_axis[2]);
-  c->acc = dalloc<unsigned char>(rs * nch * nodes);
-  c->nv = dalloc<double>((size_t)d * nodes);
-  c->nflip = dalloc<unsigned char>(rs * d * nodes);
-  c->nmass = dalloc<unsigned char>(rs * nodes);
-  c->nfric = dalloc<unsigned char>(rs * nodes);
-  c->v2 = dalloc<double>((size_t)d * nodes);
-  c->tile_begin = dalloc<uint32_t>(tiles);
-  c->tile_end = dalloc<uint32_t>(tiles);
+  c->gx = galloc<double>(c, c->cap_axis[0]);
+  c->gy = galloc<double>(c, c->cap_axis[1]);
+  c->gz = galloc<double>(c, c->cap_axis[2]);
+  c->acc = galloc<unsigned char>(c, rs * nch * nodes);
+  c->nv = galloc<double>(c, (size_t)d * nodes);
+  c->nflip = galloc<unsigned char>(c, rs * d * nodes);
+  c->nmass = galloc<unsigned char>(c, rs * nodes);
+  c->nfric = galloc<unsigned char>(c, rs * nodes);
+  c->v2 = galloc<double>(c, (size_t)d * nodes);
+  c->tile_begin = galloc<uint32_t>(c, tiles);
+  c->tile_end = galloc<uint32_t>(c, tiles);
   CK(cudaMemsetAsync(c->acc, 0, rs * nch * nodes, c->stream));
   CK(cudaMemsetAsync(c->nv, 0, sizeof(double) * d * nodes, c->stream));
   CK(cudaMemsetAsync(c->nflip, 0, rs * d * nodes, c->stream));
@@ -537,12 +573,15 @@ unsigned frame_columns(const mtr_params& p, std::vector<const char*>* names) {
 }
 
 // The header kernel aborted a step because the grid outgrew its capacity
-// (H.N holds the extents it needed): reallocates the grid with 25% headroom and
-// clears the abort in the host copy of the header (the caller writes it back).
+// (H.N holds the extents it needed): reallocates the grid with 50% headroom
+// (a spreading flow outgrows 25% again within a few hundred steps, and every
+// regrowth frees and allocates device memory and, in a batch, recaptures the
+// batch) and clears the abort in the host copy of the header (the caller
+// writes it back).
 void regrow_grid(mtr_ctx* c, StepHeader& H) {
   uint32_t want[3];
   for (int a = 0; a < 3; ++a)
-    want[a] = (a < c->dim) ? std::max<uint32_t>(c->cap_axis[a], (uint32_t)std::ceil(H.N[a] * 1.25 + 8.0)) : 1u;
+    want[a] = (a < c->dim) ? std::max<uint32_t>(c->cap_axis[a], (uint32_t)std::ceil(H.N[a] * 1.5 + 8.0)) : 1u;
   for (int a = 0; a < c->dim; ++a)
     if (H.N[a] >= kMaxAxisNodes || H.N[a] < 4)
       throw MtrError{MTR_ERR_OOM, "grid extent exploded or collapsed (non-finite particle positions?)"};
@@ -728,6 +767,9 @@ struct mtr_batch {
   int launches_per_step = 0;
   bool trial = false;  // trial steps: no kb_tail (see mtr_ctx::trial)
   EventMarks marks;    // tagged with the group index
+  // host-side bookkeeping of mtr_batch_step (mtr_batch_stats)
+  int64_t regrowths = 0, rebuilds = 0;
+  double regrow_ms = 0.0, rebuild_ms = 0.0;
 };
 
 namespace {
@@ -885,6 +927,8 @@ void set_batch_attributes(const mtr_batch_group& g) {
 // often, and the capture cost grows with the steps captured, while replaying
 // a one-step graph n times costs n graph launches of a few microseconds.
 constexpr int kBatchGraphSteps = 1;
+// steps replayed between two reads of the members' headers in mtr_batch_step
+constexpr uint32_t kBatchCheckSteps = 8;
 
 // (re)builds the device tables of every group and captures kBatchGraphSteps steps
 void rebuild_batch(mtr_batch* b) {
@@ -1892,29 +1936,51 @@ int mtr_batch_step(mtr_batch* b, int nsteps) {
     }
     write_batch_headers(b);
     int64_t launches = 0;
-    for (int guard = 0; guard < 64; ++guard) {
+    int regrowths = 0;
+    for (;;) {
       uint32_t remaining = 0;
-      for (mtr_ctx* c : b->members)
+      uint64_t steps_before = 0;
+      for (mtr_ctx* c : b->members) {
+        steps_before += c->hH->step;
         if (!c->hH->done && c->hH->step < c->hH->stop_step)
           remaining = std::max(remaining, c->hH->stop_step - c->hH->step);
+      }
       if (remaining == 0) break;
-      if (b->dirty || !b->graph) rebuild_batch(b);
-      const uint32_t reps = (remaining + kBatchGraphSteps - 1) / kBatchGraphSteps;
+      if (b->dirty || !b->graph) {
+        const auto t0 = std::chrono::steady_clock::now();
+        rebuild_batch(b);
+        b->rebuilds += 1;
+        b->rebuild_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      }
+      // Replay in runs of at most kBatchCheckSteps steps and read the headers
+      // after each: a member whose grid outgrew its capacity sits out the
+      // rest of the run (its header aborts), and every step it missed costs
+      // a replay of the whole batch later, so a short run bounds that waste.
+      const uint32_t run = std::min<uint32_t>(remaining, kBatchCheckSteps);
+      const uint32_t reps = (run + kBatchGraphSteps - 1) / kBatchGraphSteps;
       for (uint32_t r = 0; r < reps; ++r) {
         CK(cudaGraphLaunch(b->graph, b->stream));
         launches += (int64_t)b->launches_per_step * kBatchGraphSteps;
       }
       read_batch_headers(b);
       bool regrown = false;
+      uint64_t steps_after = 0;
       for (mtr_ctx* c : b->members) {
         StepHeader& H = *c->hH;
+        steps_after += H.step;
         if (!H.abort) continue;
+        const auto t0 = std::chrono::steady_clock::now();
         regrow_grid(c, H);
+        b->regrowths += 1;
+        b->regrow_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         regrown = true;
       }
       if (regrown) {
+        if (++regrowths > 4096) throw MtrError{MTR_ERR_STATE, "batch grids kept growing"};
         write_batch_headers(b);
         b->dirty = true;
+      } else if (steps_after == steps_before) {
+        break;  // no member can advance (ended, or held by a frame stop)
       }
     }
     for (mtr_ctx* c : b->members) {
@@ -2054,6 +2120,15 @@ int mtr_batch_autotune(mtr_batch* b, int reps) {
 }
 
 int64_t mtr_batch_launch_count(mtr_batch* b) { return b ? b->launches_last : 0; }
+
+int mtr_batch_stats(mtr_batch* b, int64_t* regrowths, double* regrow_ms, int64_t* rebuilds, double* rebuild_ms) {
+  if (!b) return MTR_ERR_INVALID;
+  if (regrowths) *regrowths = b->regrowths;
+  if (regrow_ms) *regrow_ms = b->regrow_ms;
+  if (rebuilds) *rebuilds = b->rebuilds;
+  if (rebuild_ms) *rebuild_ms = b->rebuild_ms;
+  return MTR_OK;
+}
 
 void* mtr_batch_stream(mtr_batch* b) { return b ? (void*)b->stream : nullptr; }
 

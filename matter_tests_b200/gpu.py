@@ -28,7 +28,7 @@ EXPORTS = (
     "mtr_autotune", "mtr_set_tile_threads", "mtr_get_tile_threads", "mtr_batch_autotune", "mtr_batch_groups",
     "mtr_batch_get_group", "mtr_batch_set_tile_threads", "mtr_frame_columns", "mtr_frame_begin",
     "mtr_frame_wait", "mtr_get_grid_friction", "mtr_set_levelset", "mtr_set_tile_lanes", "mtr_get_tile_lanes",
-    "mtr_batch_set_tile_lanes", "mtr_batch_clocks",
+    "mtr_batch_set_tile_lanes", "mtr_batch_clocks", "mtr_batch_stats",
 )
 
 _lib = None
@@ -97,6 +97,7 @@ def load_library(path=LIB_PATH):
     lib.mtr_get_tile_lanes.argtypes = [C.c_void_p, _I4]
     lib.mtr_batch_set_tile_lanes.argtypes = [C.c_void_p, C.c_int, _I4]
     lib.mtr_batch_clocks.argtypes = [C.c_void_p, C.POINTER(MtrClock), C.c_int]
+    lib.mtr_batch_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int64), _P, C.POINTER(C.c_int64), _P]
     lib.mtr_frame_columns.argtypes = [C.c_void_p, C.POINTER(C.c_char_p), C.c_int]
     lib.mtr_frame_begin.argtypes = [C.c_void_p]
     lib.mtr_frame_wait.argtypes = [C.c_void_p, C.c_double, C.POINTER(_P), C.POINTER(C.c_uint32),
@@ -387,6 +388,14 @@ class GpuBatch:
 
     def launch_count(self):
         return self.lib.mtr_batch_launch_count(self.h)
+
+    def stats(self):
+        """Grid regrowths and batch rebuilds of step() so far, with their wall ms (mtr_batch_stats)."""
+        rg, rb = C.c_int64(), C.c_int64()
+        rgm, rbm = C.c_double(), C.c_double()
+        _check(self.lib, "mtr_batch_stats", self.lib.mtr_batch_stats(self.h, C.byref(rg), C.byref(rgm), C.byref(rb),
+                                                                     C.byref(rbm)))
+        return {"regrowths": rg.value, "regrow_ms": rgm.value, "rebuilds": rb.value, "rebuild_ms": rbm.value}
 
     def clocks(self):
         """Each member's clock after the last step() (mtr_batch_clocks, no device round trip)."""
