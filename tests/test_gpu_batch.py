@@ -124,6 +124,9 @@ def test_batch_members_stop_at_their_own_end_and_regrow_their_own_grid():
     batch.step(30)
     assert sims[0].clock()["done"] == 1
     assert sims[1].clock()["step"] == 30
+    st = batch.stats()  # the regrowths happened inside the batch, and each rebuilt it
+    assert st["regrowths"] >= 1 and st["rebuilds"] >= 1 + st["regrowths"] // len(scs)
+    assert st["regrow_ms"] >= 0 and st["rebuild_ms"] > 0
     for sc, g, ref in zip(scs, sims, alone):
         assert_same(state(g), ref, sc.params.precision)
     batch.close()
