@@ -5,8 +5,9 @@ arm import this module.  Two checkers share one interface:
 
 * ``Oracle``    — oracle/liboracle.so, the C restatement (mpm_oracle.c), any
                   dim (2|3) and spline degree (2|3);
-* ``Reference`` — oracle/_ref/libref_3d_q{2,3}.so, the reference's own
-                  src/simulation/*.cpp compiled by oracle/Makefile (3D only).
+* ``Reference`` — oracle/_ref/libref_{2,3}d_q{2,3}.so, the reference's own
+                  src/simulation/*.cpp compiled by oracle/Makefile (2D from a
+                  copy whose tools.hpp leaves THREEDIM undefined).
 
 Arrays are numpy float64, AoS per particle exactly as include/matter_gpu.h
 describes (vectors dim-wide, matrices column-major dim*dim, six scalars).
@@ -193,24 +194,52 @@ def svd(A):
     return U.reshape(d, d).T, S, V.reshape(d, d).T
 
 
+def p2g_grid(params, x, v, B, gx, gy, gz, dims):
+    """Oracle P2G of particles onto a given uniform grid (orc_p2g_grid): the
+    checker of mtr_p2g_noalloc.  x, v (Np, dim); B per particle column-major
+    dim*dim like set_particles, or None; returns (mass[G], v[G, dim],
+    particles left out)."""
+    lib = _load_oracle()
+    lib.orc_p2g_grid.restype = C.c_uint32
+    lib.orc_p2g_grid.argtypes = [C.POINTER(MtrParams), C.c_uint32, _P, _P, _P, _P, _P, _P, _U, _P, _P]
+    d = params.dim
+    x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, d)
+    n = x.shape[0]
+    v = np.ascontiguousarray(v, dtype=np.float64).reshape(n, d)
+    Bc = _f64(B, n * d * d)
+    gx = np.ascontiguousarray(gx, dtype=np.float64)
+    gy = np.ascontiguousarray(gy, dtype=np.float64)
+    gz = np.ascontiguousarray(gz if gz is not None and d == 3 else np.zeros(1), dtype=np.float64)
+    dd = (C.c_uint32 * 3)(*[int(a) for a in dims])
+    G = int(dims[0]) * int(dims[1]) * (int(dims[2]) if d == 3 else 1)
+    m, gv = np.zeros(G), np.zeros(G * d)
+    left = lib.orc_p2g_grid(C.byref(params), n, _ptr(x), _ptr(v), _ptr(Bc), _ptr(gx), _ptr(gy), _ptr(gz), dd,
+                            _ptr(m), _ptr(gv))
+    return m, gv.reshape(G, d), int(left)
+
+
 _ref_libs = {}
 
 
+def _ref_path(dim, deg):
+    return os.path.join(HERE, "_ref", f"libref_{dim}d_q{deg}.so")
+
+
 def reference_available(dim, deg):
-    return dim == 3 and os.path.exists(os.path.join(HERE, "_ref", f"libref_3d_q{deg}.so"))
+    return os.path.exists(_ref_path(dim, deg))
 
 
 class Reference(_Checker):
-    """The reference's own Simulation, compiled from its sources (3D only)."""
+    """The reference's own Simulation, compiled from its sources."""
     prefix = "ref_"
 
     def __init__(self, params, n_threads=1):
         if not reference_available(params.dim, params.spline_deg):
             raise RuntimeError("reference build for dim=%d deg=%d is not available"
                                % (params.dim, params.spline_deg))
-        key = params.spline_deg
+        key = (params.dim, params.spline_deg)
         if key not in _ref_libs:
-            lib = C.CDLL(os.path.join(HERE, "_ref", f"libref_3d_q{key}.so"))
+            lib = C.CDLL(_ref_path(*key))
             lib.ref_create.restype = C.c_void_p
             lib.ref_create.argtypes = [C.POINTER(MtrParams), C.c_int]
             _ref_libs[key] = lib

@@ -11,12 +11,13 @@
  * each function cites the file:line it follows.  Arithmetic is FP64 and the
  * operation order follows the reference expression by expression, so that the
  * restatement agrees with the reference compiled from source (oracle/_ref/,
- * see build_ref.sh) to round-off.  Matrices are stored per particle
+ * built by oracle/Makefile) bit for bit.  Matrices are stored per particle
  * column-major like Eigen's TM.
  *
- * Pinned against: the reference compiled from its own sources (3D, quadratic
- * and cubic) by tests/test_oracle_pin.py; 2D is covered by the restatement
- * only, because tools.hpp:20 hard-wires THREEDIM in the reference.
+ * Pinned against: the reference compiled from its own sources, 3D and 2D,
+ * quadratic and cubic (the 2D builds compile a copy of src/ in which the
+ * `#define THREEDIM` of tools.hpp:20 is commented out), by
+ * tests/test_oracle_pin.py.
  */
 #include <float.h>
 #include <math.h>
@@ -2184,3 +2185,64 @@ void orc_destroy(orc* s) {
 size_t orc_sizeof_params(void) { return sizeof(mtr_params); }
 size_t orc_sizeof_plate(void) { return sizeof(mtr_plate); }
 size_t orc_sizeof_object(void) { return sizeof(mtr_object); }
+
+/* ------------------------------------------------------------------------ */
+/* P2G alone onto a caller's grid: the checker of mtr_p2g_noalloc            */
+/* ------------------------------------------------------------------------ */
+/* The P2G of p2g.cpp:6-100 (via p2g() above) over a grid the caller gives
+ * (uniform axes gx, gy, gz at params->dx; dims nodes per axis), with
+ * mtr_p2g_noalloc's rule for particles the grid cannot hold: a particle whose
+ * cell floor((x - x0)/dx) lies outside [0, N) on any axis, or whose clamped
+ * stencil base + 3 reaches N, is left out.  x, v are AoS [Np][dim], B AoS
+ * column-major [Np][dim*dim] (read when flip_ratio < 0).  Writes grid_mass[G]
+ * and grid_v[G][dim]; returns the number of particles left out. */
+uint32_t orc_p2g_grid(const mtr_params* P, uint32_t Np, const double* x, const double* v, const double* B,
+                      const double* gx, const double* gy, const double* gz, const uint32_t* dims,
+                      double* grid_mass, double* grid_v) {
+  orc* s = orc_create(P);
+  if (!s) return 0xffffffffu;
+  int d = s->dim, dd = d * d;
+  uint32_t kept = 0;
+  double org[3] = {gx[0], gy[0], d == 3 ? gz[0] : 0.0};
+  /* the kept particles, in input order */
+  double* kx = xalloc((size_t)Np * d);
+  double* kv = xalloc((size_t)Np * d);
+  double* kB = xalloc((size_t)Np * dd);
+  for (uint32_t p = 0; p < Np; ++p) {
+    int ok = 1;
+    for (int a = 0; a < d; ++a) {
+      double u = (x[(size_t)p * d + a] - org[a]) * s->one_over_dx;
+      if (!(u >= 0.0 && u < (double)dims[a])) { ok = 0; break; }
+      int b = (int)floor(u) - 1;
+      if (b < 0) b = 0;
+      if (b + 3 >= (int)dims[a]) ok = 0;
+    }
+    if (!ok) continue;
+    memcpy(kx + (size_t)kept * d, x + (size_t)p * d, sizeof(double) * d);
+    memcpy(kv + (size_t)kept * d, v + (size_t)p * d, sizeof(double) * d);
+    if (B) memcpy(kB + (size_t)kept * dd, B + (size_t)p * dd, sizeof(double) * dd);
+    kept++;
+  }
+  orc_set_particles(s, kept, kx, kv, NULL, B ? kB : NULL, NULL);
+  free(kx); free(kv); free(kB);
+  s->Nx = dims[0];
+  s->Ny = dims[1];
+  s->Nz = d == 3 ? dims[2] : 1;
+  s->G = s->Nx * s->Ny * s->Nz;
+  s->gx = (double*)malloc(sizeof(double) * s->Nx);
+  s->gy = (double*)malloc(sizeof(double) * s->Ny);
+  s->gz = (double*)malloc(sizeof(double) * s->Nz);
+  memcpy(s->gx, gx, sizeof(double) * s->Nx);
+  memcpy(s->gy, gy, sizeof(double) * s->Ny);
+  if (d == 3) memcpy(s->gz, gz, sizeof(double) * s->Nz); else s->gz[0] = 0.0;
+  s->xc = org[0];
+  s->yc = org[1];
+  s->zc = org[2];
+  s->ng = 0;
+  resize_grid(s);
+  p2g(s);
+  memcpy(grid_mass, s->gmass, sizeof(double) * s->G);
+  memcpy(grid_v, s->gv, sizeof(double) * s->G * d);
+  orc_destroy(s);
+  return Np - kept;
+}

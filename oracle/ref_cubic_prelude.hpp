@@ -49,6 +49,7 @@ inline T dNdu(T u) {
   if (a < 2.0) return -0.5 * sgn(u) * (2.0 - a) * (2.0 - a);
   return 0;
 }
+#ifdef THREEDIM
 inline T wip(T xp, T yp, T zp, T xi, T yi, T zi, T h) {
   return N((xp - xi) * h) * N((yp - yi) * h) * N((zp - zi) * h);
 }
@@ -59,3 +60,13 @@ inline TV grad_wip(T xp, T yp, T zp, T xi, T yi, T zi, T h) {
   g(2) = dNdu((zp - zi) * h) * N((xp - xi) * h) * N((yp - yi) * h) * h;
   return g;
 }
+#else
+// the 2D forms (tools.hpp:247-258)
+inline T wip(T xp, T yp, T xi, T yi, T h) { return N((xp - xi) * h) * N((yp - yi) * h); }
+inline TV grad_wip(T xp, T yp, T xi, T yi, T h) {
+  TV g;
+  g(0) = dNdu((xp - xi) * h) * N((yp - yi) * h) * h;
+  g(1) = dNdu((yp - yi) * h) * N((xp - xi) * h) * h;
+  return g;
+}
+#endif

@@ -1,5 +1,5 @@
 // ref_harness.cpp — drives the reference's own Simulation class, compiled from
-// its unmodified sources (see build_ref.sh), behind the same C API as the C
+// its unmodified sources (oracle/Makefile), behind the same C API as the C
 // restatement (mpm_oracle.c), so tests can run both on one scene.
 //
 // TEST INFRASTRUCTURE ONLY.  Nothing in the product links this.

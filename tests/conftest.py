@@ -21,8 +21,8 @@ def _ensure_oracle():
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True,
                        stdout=subprocess.DEVNULL)
     ref_dir = os.path.join(ROOT, "oracle", "_ref")
-    if not os.path.exists(os.path.join(ref_dir, "libref_3d_q3.so")):
-        # builds only where the reference tree is readable (oracle/Makefile REF)
+    if not all(os.path.exists(os.path.join(ref_dir, f"libref_{d}d_q{q}.so")) for d in (2, 3) for q in (2, 3)):
+        # builds only where the reference checkout is readable (oracle/Makefile MATTER_REF)
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=False,
                        stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
     if not os.path.exists(os.path.join(ref_dir, "kat", "kat")):

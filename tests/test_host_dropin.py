@@ -20,7 +20,8 @@ HOST = os.path.join(ROOT, "matter_tests_b200", "host")
 SETUPS = os.path.join(ROOT, "tests", "host_setups")
 LIB = os.path.join(ROOT, "matter_tests_b200", "libmatter_gpu.so")
 KAT = os.path.join(ROOT, "oracle", "_ref", "kat", "kat")
-REF = "/root/reference"
+# copies of the reference's setup and test files, staged by oracle/Makefile (`stage`)
+SETUP_COPIES = os.path.join(ROOT, "oracle", "_ref", "setups")
 
 
 def build_setup(src, out_dir, dim=3, deg=2):
@@ -42,7 +43,7 @@ def test_host_builds_for_every_dimension_and_spline(tmp_path, dim, deg):
     assert os.path.exists(build_setup(os.path.join(SETUPS, "host_parity.cpp"), tmp_path, dim, deg))
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
+@pytest.mark.skipif(not os.path.isdir(SETUP_COPIES), reason="staged reference setup files not present")
 @pytest.mark.parametrize("setup", ["src/mpm.cpp", "examples/collapse.cpp", "examples/cube_rotating.cpp",
                                    "tests/tests.cpp"])
 def test_reference_setup_files_compile_unchanged(tmp_path, setup):
@@ -57,7 +58,7 @@ def test_reference_setup_files_compile_unchanged(tmp_path, setup):
     else:
         work = HOST
         extra = []
-    with open(os.path.join(REF, setup)) as f:
+    with open(os.path.join(SETUP_COPIES, setup)) as f:
         r = subprocess.run(["/usr/bin/g++", "-std=c++17", "-fsyntax-only", "-w", "-I", HOST, "-I",
                             os.path.join(ROOT, "include"), *extra, "-x", "c++", "-"], stdin=f, cwd=str(work),
                            capture_output=True, text=True)
