@@ -364,9 +364,20 @@ int mtr_batch_set_tile_threads(mtr_batch* batch, int group, const int* threads /
  * exit).  Inputs and outputs are device pointers the caller owns:
  *   x, v  [dim][Np] component-major; B [dim*dim][Np], entry (r,c) at r*dim+c
  *         (read only when params->flip_ratio < 0); gx, gy, gz the node
- *         coordinates per axis (gz unused in 2D); dims = nodes per axis (host);
+ *         coordinates per axis (gz unused in 2D), uniformly spaced at
+ *         params->dx (tiles and stencils are located from gx[0], gy[0],
+ *         gz[0] and 1/dx; other spacings deposit wrongly);
+ *         dims = nodes per axis (host);
  *   grid_mass [G], grid_v [dim][G] with G = dims product, node order
- *         (i*Ny + j)*Nz + k.
+ *         (i*Ny + j)*Nz + k;
+ *   status  optional (NULL: not written): one device uint32_t that receives
+ *         this call's MTR_STATUS_* word, written in stream order after the
+ *         transfer (no host synchronisation needed, readable by later work
+ *         on the stream).  MTR_STATUS_STENCIL_OOB means some particles were
+ *         dropped: those whose cell lies outside the grid, whose position is
+ *         not finite, or whose stencil reaches past the last node.  The
+ *         remaining particles are deposited exactly as if the dropped ones
+ *         were absent.
  * Uses params->dim, spline_deg, dx, flip_ratio, particle_mass.  Runs on
  * `stream` (cudaStream_t; NULL = legacy default stream) and returns without
  * synchronising.  More than MTR_NOALLOC_MAX_PARTICLES particles or
@@ -378,7 +389,7 @@ int mtr_batch_set_tile_threads(mtr_batch* batch, int group, const int* threads /
 #define MTR_NOALLOC_MAX_NODES (1u << 17)
 int mtr_p2g_noalloc(const mtr_params* params, const double* x, const double* v, const double* B, uint32_t Np,
                     const double* gx, const double* gy, const double* gz, const uint32_t dims[3], double* grid_mass,
-                    double* grid_v, void* stream);
+                    double* grid_v, uint32_t* status, void* stream);
 
 void mtr_ctx_destroy(mtr_ctx* ctx);
 

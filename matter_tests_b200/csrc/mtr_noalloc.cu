@@ -223,6 +223,36 @@ __global__ void __launch_bounds__(kChunk) k_p2g_noalloc(StepArgs A, const uint32
   }
 }
 
+// Cell keys of the first sort pass.  A particle whose cell lies outside the
+// caller's grid (or whose position is not finite) gets the sentinel key
+// ntiles * 64, one past every real tile: it sorts behind all real particles,
+// no tile range names it, and it is reported through the status word.  The
+// test is written on the same expression cell_key floors, so a particle kept
+// here has a tile index below ntiles.
+template <int D>
+__global__ void __launch_bounds__(256) k_noalloc_keys(StepCommon A) {
+  const StepHeader* H = A.H;
+  const double ioh = A.P->one_over_dx;
+  const uint32_t sentinel = H->ntiles * 64u;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < A.Np; i += gridDim.x * blockDim.x) {
+    double x[3] = {0.0, 0.0, 0.0};
+    bool inside = true;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      x[a] = A.xin[(size_t)a * A.Np + i];
+      const double u = (x[a] - H->org[a]) * ioh;
+      if (!(u >= 0.0 && u < (double)H->N[a])) inside = false;
+    }
+    if (inside) {
+      A.keys0[i] = cell_key<D>(H, ioh, x);
+    } else {
+      A.keys0[i] = sentinel;
+      atomicOr(&A.H->status, MTR_STATUS_STENCIL_OOB);
+      atomicMin(&A.H->first_bad, i);
+    }
+  }
+}
+
 template <int D>
 constexpr size_t noalloc_smem_bytes() {
   return sizeof(double) * ((1 + D) * Tiling<D>::NODES + 3 * Tiling<D>::PN) + sizeof(MStage<D>) * kChunk;
@@ -266,7 +296,9 @@ __global__ void k_noalloc_setup(StepHeader* H, DevParams* P, const double* gx, c
 // p2g.cpp:84-98: v = momentum / (sum of weights), mass *= particle mass.
 template <int D>
 __global__ void k_noalloc_finalize(const double* __restrict__ acc, uint32_t cap, uint32_t G, double particle_mass,
-                                   double* grid_mass, double* grid_v) {
+                                   double* grid_mass, double* grid_v, const StepHeader* __restrict__ H,
+                                   uint32_t* status) {
+  if (status && blockIdx.x == 0 && threadIdx.x == 0) *status = H->status;
   for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < G; l += gridDim.x * blockDim.x) {
     const double m = acc[l];
 #pragma unroll
@@ -276,9 +308,9 @@ __global__ void k_noalloc_finalize(const double* __restrict__ acc, uint32_t cap,
 }
 
 template <int D, int DEG>
-void set_attr() {
-  cudaFuncSetAttribute(k_p2g_noalloc<D, DEG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)noalloc_smem_bytes<D>());
+bool set_attr() {
+  return cudaFuncSetAttribute(k_p2g_noalloc<D, DEG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)noalloc_smem_bytes<D>()) == cudaSuccess;
 }
 
 // Once per device, with that device current: the device address of the
@@ -297,10 +329,10 @@ unsigned char* scratch_for_current_device(int* rc_out) {
       *rc_out = MTR_ERR_CUDA;
       return nullptr;
     }
-    set_attr<2, 2>();
-    set_attr<2, 3>();
-    set_attr<3, 2>();
-    set_attr<3, 3>();
+    if (!(set_attr<2, 2>() && set_attr<2, 3>() && set_attr<3, 2>() && set_attr<3, 3>())) {
+      *rc_out = MTR_ERR_CUDA;  // the device stays unset: the next call tries again
+      return nullptr;
+    }
     g_scratch_ptr[dev] = ptr;
   }
   *rc_out = MTR_OK;
@@ -310,7 +342,7 @@ unsigned char* scratch_for_current_device(int* rc_out) {
 template <int D, int DEG>
 int run_noalloc(unsigned char* base, const mtr_params& p, const double* x, const double* v, const double* B,
                 uint32_t Np, const double* gx, const double* gy, const double* gz, const uint32_t dims[3],
-                double* grid_mass, double* grid_v, cudaStream_t st) {
+                double* grid_mass, double* grid_v, uint32_t* status, cudaStream_t st) {
   constexpr int TB = Tiling<D>::TB;
   StepHeader* H = reinterpret_cast<StepHeader*>(base + kOffHeader);
   DevParams* P = reinterpret_cast<DevParams*>(base + kOffParams);
@@ -326,7 +358,7 @@ int run_noalloc(unsigned char* base, const mtr_params& p, const double* x, const
   A.gy = const_cast<double*>(gy);
   A.gz = const_cast<double*>(gz ? gz : gy);
   A.cap_nodes = (uint32_t)kMaxNodes;
-  A.cap_tiles = (uint32_t)kMaxTiles;
+  A.cap_tiles = (uint32_t)ntiles;  // k_tile_ranges skips the sentinel tile (index ntiles)
   A.acc = reinterpret_cast<double*>(base + kOffAcc);
   A.keys0 = reinterpret_cast<uint32_t*>(base + kOffKeys0);
   A.keysA = reinterpret_cast<uint32_t*>(base + kOffKeysA);
@@ -342,14 +374,17 @@ int run_noalloc(unsigned char* base, const mtr_params& p, const double* x, const
   A.xin = x;
   A.in.v = const_cast<double*>(v);
   A.in.B = const_cast<double*>(B);
-  k_noalloc_setup<<<1, 32, 0, st>>>(H, P, gx, gy, gz, nx, ny, nz, tx, ty, tz, 1.0 / p.dx, apicD, p.flip_ratio,
-                                    p.particle_mass, Np, D);
   // what must start at zero: the accumulators and the tile ranges of this grid
+  // (memsets first, so that a failure leaves nothing of this call queued)
   if (cudaMemsetAsync(A.acc, 0, sizeof(double) * 4 * kMaxNodes, st) != cudaSuccess) return MTR_ERR_CUDA;
   if (cudaMemsetAsync(A.tile_begin, 0, sizeof(uint32_t) * ntiles, st) != cudaSuccess) return MTR_ERR_CUDA;
   if (cudaMemsetAsync(A.tile_end, 0, sizeof(uint32_t) * ntiles, st) != cudaSuccess) return MTR_ERR_CUDA;
+  k_noalloc_setup<<<1, 32, 0, st>>>(H, P, gx, gy, gz, nx, ny, nz, tx, ty, tz, 1.0 / p.dx, apicD, p.flip_ratio,
+                                    p.particle_mass, Np, D);
+  k_noalloc_keys<D><<<(uint32_t)std::min<uint64_t>((Np + 255) / 256, 148 * 8), 256, 0, st>>>(A);
+  // enough digits for every real key (below ntiles * 64) and the sentinel (ntiles * 64)
   uint64_t keybits = 1;
-  while ((1ull << keybits) < ntiles * 64ull) ++keybits;
+  while ((1ull << keybits) < ntiles * 64ull + 1ull) ++keybits;
   const int passes = (int)((keybits + 7) / 8);
   const uint32_t* skeys = nullptr;
   const uint32_t* perm = nullptr;
@@ -359,10 +394,7 @@ int run_noalloc(unsigned char* base, const mtr_params& p, const double* x, const
     const uint32_t* vsrc = pass == 0 ? nullptr : ((pass & 1) ? A.valsB : A.valsA);
     uint32_t* kdst = (pass & 1) ? A.keysA : A.keysB;
     uint32_t* vdst = (pass & 1) ? A.valsA : A.valsB;
-    if (pass == 0)
-      k_sort_hist<D, true><<<A.sort_blocks, kSortThreads, 0, st>>>(A, nullptr, shift);
-    else
-      k_sort_hist<D, false><<<A.sort_blocks, kSortThreads, 0, st>>>(A, ksrc, shift);
+    k_sort_hist<D, false><<<A.sort_blocks, kSortThreads, 0, st>>>(A, ksrc, shift);
     k_sort_scan<<<256, 256, 0, st>>>(A);
     k_sort_scatter<<<A.sort_blocks, kSortThreads, 0, st>>>(A, ksrc, vsrc, kdst, vdst, shift);
     skeys = kdst;
@@ -371,7 +403,7 @@ int run_noalloc(unsigned char* base, const mtr_params& p, const double* x, const
   k_tile_ranges<<<(Np + 255) / 256, 256, 0, st>>>(A, skeys);
   k_p2g_noalloc<D, DEG><<<(uint32_t)ntiles, kChunk, noalloc_smem_bytes<D>(), st>>>(A, perm);
   k_noalloc_finalize<D><<<(uint32_t)std::min<uint64_t>((G + 255) / 256, 148 * 8), 256, 0, st>>>(
-      A.acc, (uint32_t)kMaxNodes, (uint32_t)G, p.particle_mass, grid_mass, grid_v);
+      A.acc, (uint32_t)kMaxNodes, (uint32_t)G, p.particle_mass, grid_mass, grid_v, H, status);
   return cudaGetLastError() == cudaSuccess ? MTR_OK : MTR_ERR_CUDA;
 }
 
@@ -379,7 +411,10 @@ int run_noalloc(unsigned char* base, const mtr_params& p, const double* x, const
 
 extern "C" int mtr_p2g_noalloc(const mtr_params* params, const double* x, const double* v, const double* B,
                                uint32_t Np, const double* gx, const double* gy, const double* gz,
-                               const uint32_t dims[3], double* grid_mass, double* grid_v, void* stream) {
+                               const uint32_t dims[3], double* grid_mass, double* grid_v, uint32_t* status,
+                               void* stream) {
+  // an error left by earlier, unrelated work of this thread is not this call's failure
+  (void)cudaGetLastError();
   if (!params || !x || !v || !gx || !gy || !dims || !grid_mass || !grid_v || Np == 0) return MTR_ERR_INVALID;
   const mtr_params& p = *params;
   if ((p.dim != 2 && p.dim != 3) || (p.spline_deg != 2 && p.spline_deg != 3) || !(p.dx > 0)) return MTR_ERR_INVALID;
@@ -393,8 +428,8 @@ extern "C" int mtr_p2g_noalloc(const mtr_params* params, const double* x, const 
   if (!base) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (p.dim == 3)
-    return p.spline_deg == 3 ? run_noalloc<3, 3>(base, p, x, v, B, Np, gx, gy, gz, dims, grid_mass, grid_v, st)
-                             : run_noalloc<3, 2>(base, p, x, v, B, Np, gx, gy, gz, dims, grid_mass, grid_v, st);
-  return p.spline_deg == 3 ? run_noalloc<2, 3>(base, p, x, v, B, Np, gx, gy, gz, dims, grid_mass, grid_v, st)
-                           : run_noalloc<2, 2>(base, p, x, v, B, Np, gx, gy, gz, dims, grid_mass, grid_v, st);
+    return p.spline_deg == 3 ? run_noalloc<3, 3>(base, p, x, v, B, Np, gx, gy, gz, dims, grid_mass, grid_v, status, st)
+                             : run_noalloc<3, 2>(base, p, x, v, B, Np, gx, gy, gz, dims, grid_mass, grid_v, status, st);
+  return p.spline_deg == 3 ? run_noalloc<2, 3>(base, p, x, v, B, Np, gx, gy, gz, dims, grid_mass, grid_v, status, st)
+                           : run_noalloc<2, 2>(base, p, x, v, B, Np, gx, gy, gz, dims, grid_mass, grid_v, status, st);
 }

@@ -84,7 +84,7 @@ def load_library(path=LIB_PATH):
     lib.mtr_footprint.argtypes = [C.POINTER(MtrParams), C.c_uint32, _P, C.POINTER(C.c_uint64)]
     lib.mtr_p2g_noalloc.argtypes = [C.POINTER(MtrParams), C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                     C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32), C.c_void_p,
-                                    C.c_void_p, C.c_void_p]
+                                    C.c_void_p, C.c_void_p, C.c_void_p]
     _I4 = C.POINTER(C.c_int)
     lib.mtr_autotune.argtypes = [C.c_void_p, C.c_int, _I4]
     lib.mtr_set_tile_threads.argtypes = [C.c_void_p, _I4]
