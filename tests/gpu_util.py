@@ -44,7 +44,27 @@ def run_oracle(scene, nsteps):
     return out
 
 
-def oracle_sensitivity(scene, nsteps, ulps=4.0, seed=11):
+def run_reference(scene, nsteps, threads=None):
+    """The reference compiled from its own sources (oracle/_ref), with OpenMP
+    threads; same result layout as run_oracle (keys excepted)."""
+    import os
+    from oracle.checkers import Reference
+    if threads is None:
+        try:
+            threads = len(os.sched_getaffinity(0))
+        except Exception:
+            threads = os.cpu_count() or 1
+        threads = max(1, min(threads, 32))
+    r = Reference(scene.params, n_threads=threads)
+    r.set_particles(scene.x, scene.v, scene.F, scene.B, scene.scalars)
+    r.set_objects(scene.plates, scene.objects)
+    n = r.step(nsteps)
+    out = dict(n=n, p=r.particles(), g=r.grid(), c=r.clock(), plates=r.plates())
+    r.close()
+    return out
+
+
+def oracle_sensitivity(scene, nsteps, ulps=4.0, seed=11, runner=None):
     """How far the reference's own algorithm moves, per field, when the initial
     positions, velocities and affine matrices are perturbed by a few ulps (the
     size of the reordering error of GPU atomics).  Fields the reference computes
@@ -60,7 +80,8 @@ def oracle_sensitivity(scene, nsteps, ulps=4.0, seed=11):
     sc.v = v * (1.0 + eps * rng.choice([-1.0, 1.0], size=v.shape))
     if scene.B is not None:
         sc.B = scene.B * (1.0 + eps * rng.choice([-1.0, 1.0], size=scene.B.shape))
-    a, b = run_oracle(scene, nsteps), run_oracle(sc, nsteps)
+    run = runner or run_oracle
+    a, b = run(scene, nsteps), run(sc, nsteps)
     from matter_tests_b200.abi import SCALARS
     out = {k: np.abs(a["p"]["scalars"][:, i] - b["p"]["scalars"][:, i]).max() for i, k in enumerate(SCALARS)}
     for k in ("x", "v", "F", "B", "pic", "flip"):
