@@ -10,17 +10,29 @@ cubic B-splines, 1,024,000 particles (box 0.5 x 1.0 x 0.5 m, dx 0.0125 m,
 one Simulation::advanceStep of the whole scene.  Both forms of the step run
 on the same scene: plain FP64 and mixed precision.
 
-value     mixed-precision particle-steps/s over K steps timed with CUDA events
-          on the context's stream, state resident in HBM (particle state
-          larger than the 126 MB L2 on both paths, so every step streams it
-          from HBM; no L2 flush is needed).  "fp64" holds the same figures for
-          the plain FP64 step, "mixed_error_vs_fp64" the state difference of
-          the two after the same W + K steps.
-e2e       the same metric through the C ABI with host buffers: mtr_upload from
-          pinned host memory + mtr_step(K) + mtr_download, wall clock.
+value     plain FP64 particle-steps/s (the reference's arithmetic) over K
+          steps timed with CUDA events on the context's stream, state
+          resident in HBM (particle state larger than the 126 MB L2 on both
+          paths, so every step streams it from HBM; no L2 flush is needed).
+mixed     the same figures for the mixed-precision step (FP32 state and
+          transfers, FP64 positions, SVD, return mapping and balances), its
+          speed-up over FP64 and its state error against the FP64 state after
+          the same W + K steps.
+configs   the three single-scene workloads at full size and full length
+          (2D DP collapse 2000 steps, 3D mu(I) collapse 1000, 3D Cam-Clay
+          incline 3000), each in both precisions: device-timed throughput,
+          per-kernel times, and the mixed state's position, velocity and
+          Kirchhoff-stress error against the FP64 state at the last step.
+e2e       the FP64 metric through the C ABI with host buffers: mtr_upload from
+          pinned host memory + mtr_step(K) + mtr_download, wall clock, into a
+          context that already holds a scene of that size (its buffers and
+          step graphs are refilled, not reallocated); the split into upload,
+          steps and download, and the first upload into a fresh context.
 roofline  the step's most expensive kernel: algorithmic bytes per launch
-          (compulsory particle and grid traffic) / its mean
-          CUDA-event duration, against the measured HBM copy bandwidth.
+          (compulsory particle and grid traffic) / its mean CUDA-event
+          duration, against the measured HBM copy bandwidth; traffic = that
+          kernel's DRAM bytes per launch from the committed ncu capture when
+          the capture was taken of the current kernel sources.
 cpu_baseline  the reference's own OpenMP step (src/simulation/*.cpp compiled
           from source, oracle/_ref) on a bounded sample of the same workload.
 --impl reference  times that reference build alone, on rank 0.
@@ -57,6 +69,8 @@ def parse():
     ap.add_argument("--ensemble-size", type=int, default=256, help="scenes of the batched ensemble")
     ap.add_argument("--ensemble-steps", type=int, default=500, help="timed steps of the batched ensemble")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the full-length runs of the three single-scene workloads")
     ap.add_argument("--serve-requests", type=int, default=60, help="requests of the serving measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
     ap.add_argument("--no-autotune", action="store_true",
@@ -153,15 +167,38 @@ class ClockSampler:
                 "power_w_max": max((float(r[3]) for r in rows if r[3].replace(".", "").isdigit()), default=None)}
 
 
-# DRAM bytes (read + write) per launch of the tile kernels on the 3D mu(I)
-# collapse at full size, from one ncu capture of each
-# (profiles/p2g_musl_defgrad_collapse3d_mui.md, dram__bytes_read.sum +
-# dram__bytes_write.sum); reported as the roofline's traffic for that workload
-MEASURED_TRAFFIC = {
-    ("k_p2g", "fp64"): 184.4e6, ("k_p2g", "mixed"): 110.9e6,
-    ("k_g2p_musl", "fp64"): 163.8e6, ("k_g2p_musl", "mixed"): 97.2e6,
-    ("k_defgrad", "fp64"): 285.0e6, ("k_defgrad", "mixed"): 134.9e6,
-}
+# DRAM bytes (read + write) per launch of the dominant kernels, from ncu
+# captures (dram__bytes_read.sum + dram__bytes_write.sum), stored with the
+# hash of the kernel sources they were captured on; a figure whose hash does
+# not match the sources being run is reported as stale (traffic null).
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dram_traffic.json")
+
+
+def kernel_source_hash():
+    import hashlib
+    h = hashlib.sha256()
+    csrc = os.path.join(ROOT, "matter_tests_b200", "csrc")
+    for f in sorted(os.listdir(csrc)):
+        if f.endswith((".cu", ".cuh")):
+            with open(os.path.join(csrc, f), "rb") as fh:
+                h.update(f.encode() + b"\0" + fh.read())
+    return h.hexdigest()[:16]
+
+
+def measured_traffic(workload, scale, kernel, precision):
+    """(bytes per launch, source) of the ncu capture for this kernel, or (None, why)."""
+    try:
+        with open(TRAFFIC_FILE) as f:
+            tab = json.load(f)
+    except Exception:
+        return None, "no capture file"
+    for e in tab.get("captures", []):
+        if (e.get("workload") == workload and float(e.get("scale", 1.0)) == scale and e.get("kernel") == kernel
+                and e.get("precision") == precision):
+            if e.get("source_hash") != kernel_source_hash():
+                return None, "capture predates the current kernel sources"
+            return float(e["dram_bytes_per_launch"]), "ncu capture (profiles/dram_traffic.json): " + e.get("note", "")
+    return None, "no capture of this kernel"
 
 
 def hbm_peak():
@@ -399,24 +436,34 @@ def measure(args, world, rank, local, sc, precision, sampler=None):
     t0 = time.perf_counter()
     g.upload(hx, hv, hF, hB, hs)
     g.set_objects(sc.plates, sc.objects)
+    t1 = time.perf_counter()
     g.step(args.steps)
+    t2 = time.perf_counter()
     rc = g.lib.mtr_download(g.h, dp(ox), dp(ov), dp(oF), dp(oB), dp(os_))
     assert rc == 0, rc
-    e2e_s = time.perf_counter() - t0
-    e2e_s = max_over_ranks(world, e2e_s, local)
+    t3 = time.perf_counter()
+    e2e_s = max_over_ranks(world, t3 - t0, local)
     io_bytes = 8 * sc.Np * (2 * d + 2 * d * d + 6)
-    e2e = {"value": sc.Np * args.steps * world / e2e_s, "unit": METRIC,
-           "h2d_bytes_per_step": io_bytes / args.steps, "d2h_bytes_per_step": io_bytes / args.steps,
-           "timed": "mtr_upload (pinned host) + mtr_step(K) + mtr_download, wall clock"}
     status, _ = g.status()
     g.close()
-    traffic = None
-    if args.workload == "collapse3d_mui" and args.scale == 1.0:
-        traffic = MEASURED_TRAFFIC.get((dom, "mixed" if precision == PREC_MIXED else "fp64"))
+    # the first upload into a fresh context (allocation included), for reference
+    g2 = GpuSim(p, device=local)
+    t4 = time.perf_counter()
+    g2.upload(hx, hv, hF, hB, hs)
+    t5 = time.perf_counter()
+    g2.close()
+    e2e = {"value": sc.Np * args.steps * world / e2e_s, "unit": METRIC,
+           "h2d_bytes_per_step": io_bytes / args.steps, "d2h_bytes_per_step": io_bytes / args.steps,
+           "split_ms": {"upload": (t1 - t0) * 1e3, "steps": (t2 - t1) * 1e3, "download": (t3 - t2) * 1e3},
+           "fresh_context_upload_ms": (t5 - t4) * 1e3,
+           "timed": "mtr_upload (pinned host) + mtr_step(K) + mtr_download, wall clock, into a context already "
+                    "holding a scene of this size"}
+    traffic, traffic_src = measured_traffic(args.workload, args.scale, dom,
+                                            "mixed" if precision == PREC_MIXED else "fp64")
     out = {"value": value, "ms_per_step": ms_max / args.steps,
            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                        "traffic": traffic, "traffic_source": "ncu capture, profiles/" if traffic else None,
+                        "traffic": traffic, "traffic_source": traffic_src,
                         "peak_source": peak_kind,
                         "kernel_ms": dom_ms, "kernel_algorithmic_bytes": dom_bytes,
                         "step_algorithmic_GBps": whole, "step_frac": whole / peak,
@@ -454,6 +501,62 @@ def mixed_error(sc, ref, got):
             "v_max_rel": float(np.abs(got["v"] - ref["v"]).max() / vs) if vs > 0 else None,
             "tau_max_rel": float(np.abs(tg - tr).max() / ts) if ts > 0 else None,
             "F_max_abs": float(np.abs(got["F"] - ref["F"]).max())}
+
+
+# the single-scene workloads at full size and their full lengths
+CONFIG_RUNS = (("collapse2d", 2000), ("collapse3d_mui", 1000), ("incline3d_mcc", 3000))
+
+
+def config_runs(args, local):
+    """Each single-scene workload at full size over its full length, plain
+    FP64 and mixed: device-timed particle-steps/s (16 untimed steps first,
+    which capture the step graphs; the block shapes tuned after them), the
+    per-kernel times of 3 profiled steps after the run, and the mixed
+    state's error against the FP64 state at the last step."""
+    import copy
+    import torch
+    from matter_tests_b200 import scenes
+    from matter_tests_b200.abi import PREC_FP64, PREC_MIXED
+    from matter_tests_b200.gpu import GpuSim
+    out = {}
+    for name, nsteps in CONFIG_RUNS:
+        sc = scenes.WORKLOADS[name](scale=1.0)
+        res, states = {}, {}
+        for prec, key in ((PREC_FP64, "fp64"), (PREC_MIXED, "mixed")):
+            p = copy.copy(sc.params)
+            p.precision = prec
+            g = GpuSim(p, device=local)
+            g.upload(sc.x, sc.v, sc.F, sc.B, sc.scalars)
+            g.set_objects(sc.plates, sc.objects)
+            warm = 16
+            g.step(warm)
+            if not args.no_autotune:
+                g.autotune(args.tune_reps)
+            st = torch.cuda.ExternalStream(g.stream, device=torch.device("cuda", local))
+            torch.cuda.synchronize(local)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            g.step(nsteps - warm)
+            b.record(st)
+            b.synchronize()
+            ms = a.elapsed_time(b)
+            ck = g.clock()
+            states[key] = g.particles()
+            status, _ = g.status()
+            slots = g.profile(3)
+            agg, cnt = {}, {}
+            for kn, t in slots:
+                agg[kn] = agg.get(kn, 0.0) + t
+                cnt[kn] = cnt.get(kn, 0) + 1
+            g.close()
+            res[key] = {"value": sc.Np * (nsteps - warm) / (ms / 1e3), "ms_per_step": ms / (nsteps - warm),
+                        "steps": int(ck["step"]), "status_flags": status,
+                        "kernel_ms": {k: round(agg[k] / cnt[k], 5) for k in agg}}
+        err = mixed_error(sc, states["fp64"], states["mixed"])
+        out[name] = {"Np": sc.Np, "steps": nsteps, "fp64": res["fp64"], "mixed": res["mixed"],
+                     "mixed_over_fp64": res["mixed"]["value"] / res["fp64"]["value"],
+                     "mixed_error_vs_fp64": err}
+    return out
 
 
 def ensemble_measure(args, local):
@@ -633,6 +736,12 @@ def gpu_arm(args, world, rank, local):
     sampler.start()
     fp64, st64 = measure(args, world, rank, local, sc, PREC_FP64)
     mixed, st32 = measure(args, world, rank, local, sc, PREC_MIXED)
+    cfgs = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        try:
+            cfgs = config_runs(args, local)
+        except Exception as e:  # reported, not fatal: the headline line still prints
+            cfgs = {"error": f"{type(e).__name__}: {e}"}
     ens = None
     if rank == 0 and world == 1 and not args.no_ensemble:
         try:
@@ -656,20 +765,23 @@ def gpu_arm(args, world, rank, local):
 
     if rank == 0:
         cfg = config_of(args, sc)
-        cfg["precision"] = "mixed (FP32 state and transfers, FP64 positions, SVD, return mapping, balances)"
-        line = {"metric": METRIC, "value": mixed["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": mixed["ms_per_step"], "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        line = {"metric": METRIC, "value": fp64["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": fp64["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded jittered lattice)", "config": cfg,
-                "roofline": mixed["roofline"], "kernel_ms": mixed["kernel_ms"],
-                "profiled_step_ms": mixed["profiled_step_ms"], "cpu_baseline": cpu, "e2e": mixed["e2e"],
-                "gpu_launches": mixed["gpu_launches"] + fp64["gpu_launches"], "clocks": clocks,
-                "tile_threads": mixed["tile_threads"],
-                "fp64": {k: fp64[k] for k in ("value", "ms_per_step", "roofline", "kernel_ms", "e2e",
-                                              "gpu_launches", "status_flags", "tile_threads")},
-                "mixed_over_fp64": mixed["value"] / fp64["value"],
-                "mixed_error_vs_fp64": err, "ensemble": ens, "serving": served,
-                "sim_clock": mixed["sim_clock"], "status_flags": mixed["status_flags"]}
+                "roofline": fp64["roofline"], "kernel_ms": fp64["kernel_ms"],
+                "profiled_step_ms": fp64["profiled_step_ms"], "cpu_baseline": cpu, "e2e": fp64["e2e"],
+                "gpu_launches": fp64["gpu_launches"], "clocks": clocks, "tile_threads": fp64["tile_threads"],
+                "mixed": {"value": mixed["value"], "unit": METRIC, "ms_per_step": mixed["ms_per_step"],
+                          "dtype": "f32+f64",
+                          "precision": "FP32 state and transfers; FP64 positions, SVD, Hencky log/exp, return "
+                                       "mapping projections, balances",
+                          "mixed_over_fp64": mixed["value"] / fp64["value"], "error_vs_fp64": err,
+                          "roofline": mixed["roofline"], "kernel_ms": mixed["kernel_ms"], "e2e": mixed["e2e"],
+                          "gpu_launches": mixed["gpu_launches"], "tile_threads": mixed["tile_threads"],
+                          "status_flags": mixed["status_flags"]},
+                "configs": cfgs, "ensemble": ens, "serving": served,
+                "sim_clock": fp64["sim_clock"], "status_flags": fp64["status_flags"]}
         print(json.dumps(line), flush=True)
     return 0
 

@@ -168,6 +168,7 @@ struct mtr_ctx {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int host_parity = 0;
   int64_t launches_last = 0;
+  int64_t uploads_reused = 0;  // uploads that refilled the buffers already there
   int launches_per_step = 0;
   bool use_graphs = true;
   uint32_t step_limit = 0xffffffffu;  // mtr_set_step_limit: no step beyond this step count
@@ -269,6 +270,18 @@ void free_graphs(mtr_ctx* c) {
 
 int tile_edge(int d) { return d == 3 ? 4 : 8; }
 
+// Zeroes the grid channels a fresh grid starts from.
+void clear_grid(mtr_ctx* c) {
+  const int d = c->dim;
+  const int nch = 2 + 2 * d;
+  const size_t rs = c->rsize, nodes = c->cap_nodes;
+  CK(cudaMemsetAsync(c->acc, 0, rs * nch * nodes, c->stream));
+  CK(cudaMemsetAsync(c->nv, 0, sizeof(double) * d * nodes, c->stream));
+  CK(cudaMemsetAsync(c->nflip, 0, rs * d * nodes, c->stream));
+  CK(cudaMemsetAsync(c->nmass, 0, rs * nodes, c->stream));
+  CK(cudaMemsetAsync(c->v2, 0, sizeof(double) * d * nodes, c->stream));
+}
+
 // (Re)allocates the grid for per-axis node capacities.
 void alloc_grid(mtr_ctx* c, const uint32_t want[3]) {
   free_grid(c);
@@ -296,11 +309,7 @@ void alloc_grid(mtr_ctx* c, const uint32_t want[3]) {
   c->v2 = galloc<double>(c, (size_t)d * nodes);
   c->tile_begin = galloc<uint32_t>(c, tiles);
   c->tile_end = galloc<uint32_t>(c, tiles);
-  CK(cudaMemsetAsync(c->acc, 0, rs * nch * nodes, c->stream));
-  CK(cudaMemsetAsync(c->nv, 0, sizeof(double) * d * nodes, c->stream));
-  CK(cudaMemsetAsync(c->nflip, 0, rs * d * nodes, c->stream));
-  CK(cudaMemsetAsync(c->nmass, 0, rs * nodes, c->stream));
-  CK(cudaMemsetAsync(c->v2, 0, sizeof(double) * d * nodes, c->stream));
+  clear_grid(c);
   uint64_t keybits = 1;
   while ((1ull << keybits) < tiles * 64ull) ++keybits;
   c->passes = (int)((keybits + 7) / 8);
@@ -1088,44 +1097,52 @@ int mtr_upload(mtr_ctx* c, const double* x, const double* v, const double* F, co
     if (!c || !x || Np == 0) throw MtrError{MTR_ERR_INVALID, "null context/positions or Np == 0"};
     CK(cudaSetDevice(c->device));
     const int d = c->dim, dd = d * d, ns = nsym(d);
-    free_graphs(c);
-    for (void* p : c->pallocs) dfree(p);
-    c->pallocs.clear();
-    for (void* p : {(void*)c->keys0, (void*)c->keysA, (void*)c->valsA, (void*)c->keysB, (void*)c->valsB,
-                    (void*)c->hist, (void*)c->dtot, (void*)c->partials, (void*)c->staging})
-      dfree(p);
-    c->Np = Np;
-    c->hp.Np = Np;
-    const size_t rs = c->rsize;
-    for (int s = 0; s < 2; ++s) {
-      double* xb = dalloc<double>((size_t)Np * d);  // positions: FP64 on both paths
-      unsigned char* blk = dalloc<unsigned char>(rs * Np * (d + 2 * dd + MTR_NUM_SCALARS + ns));
-      c->pallocs.push_back(xb);
-      c->pallocs.push_back(blk);
-      c->buf[s].x = xb;
-      c->buf[s].v = blk;
-      c->buf[s].F = blk + rs * Np * d;
-      c->buf[s].B = blk + rs * Np * (d + dd);
-      c->buf[s].sc = blk + rs * Np * (d + 2 * dd);
-      c->buf[s].tau = blk + rs * Np * (d + 2 * dd + MTR_NUM_SCALARS);
-      c->buf[s].id = dalloc<uint32_t>(Np);
-      c->pallocs.push_back(c->buf[s].id);
+    // A new scene of the same particle count refills the buffers it already
+    // has: their addresses, and with them the captured step graphs, stay valid
+    // (freeing and allocating them again costs more than the copies).
+    const bool reuse = c->uploaded && c->Np == Np && !c->pallocs.empty();
+    c->uploaded = false;
+    if (!reuse) {
+      free_graphs(c);
+      for (void* p : c->pallocs) dfree(p);
+      c->pallocs.clear();
+      for (void* p : {(void*)c->keys0, (void*)c->keysA, (void*)c->valsA, (void*)c->keysB, (void*)c->valsB,
+                      (void*)c->hist, (void*)c->dtot, (void*)c->partials, (void*)c->staging})
+        dfree(p);
+      c->Np = Np;
+      c->hp.Np = Np;
+      const size_t rs = c->rsize;
+      for (int s = 0; s < 2; ++s) {
+        double* xb = dalloc<double>((size_t)Np * d);  // positions: FP64 on both paths
+        unsigned char* blk = dalloc<unsigned char>(rs * Np * (d + 2 * dd + MTR_NUM_SCALARS + ns));
+        c->pallocs.push_back(xb);
+        c->pallocs.push_back(blk);
+        c->buf[s].x = xb;
+        c->buf[s].v = blk;
+        c->buf[s].F = blk + rs * Np * d;
+        c->buf[s].B = blk + rs * Np * (d + dd);
+        c->buf[s].sc = blk + rs * Np * (d + 2 * dd);
+        c->buf[s].tau = blk + rs * Np * (d + 2 * dd + MTR_NUM_SCALARS);
+        c->buf[s].id = dalloc<uint32_t>(Np);
+        c->pallocs.push_back(c->buf[s].id);
+      }
+      c->pic = dalloc<unsigned char>(rs * Np * d);
+      c->flip = dalloc<unsigned char>(rs * Np * d);
+      c->pallocs.push_back(c->pic);
+      c->pallocs.push_back(c->flip);
+      c->sort_blocks = (int)((Np + kSortTile - 1) / kSortTile);
+      c->keys0 = dalloc<uint32_t>(Np);
+      c->keysA = dalloc<uint32_t>(Np);
+      c->valsA = dalloc<uint32_t>(Np);
+      c->keysB = dalloc<uint32_t>(Np);
+      c->valsB = dalloc<uint32_t>(Np);
+      c->hist = dalloc<uint32_t>((size_t)256 * c->sort_blocks);
+      c->dtot = dalloc<uint32_t>(256);
+      c->npartials = (int)std::min<uint32_t>((Np + 255) / 256, 148 * 4);
+      c->partials = dalloc<BBoxPartial>(c->npartials);
+      c->staging = dalloc<double>((size_t)Np * std::max<int>(dd, (int)MTR_NUM_SCALARS));
     }
-    c->pic = dalloc<unsigned char>(rs * Np * d);
-    c->flip = dalloc<unsigned char>(rs * Np * d);
-    c->pallocs.push_back(c->pic);
-    c->pallocs.push_back(c->flip);
-    c->sort_blocks = (int)((Np + kSortTile - 1) / kSortTile);
-    c->keys0 = dalloc<uint32_t>(Np);
-    c->keysA = dalloc<uint32_t>(Np);
-    c->valsA = dalloc<uint32_t>(Np);
-    c->keysB = dalloc<uint32_t>(Np);
-    c->valsB = dalloc<uint32_t>(Np);
-    c->hist = dalloc<uint32_t>((size_t)256 * c->sort_blocks);
-    c->dtot = dalloc<uint32_t>(256);
-    c->npartials = (int)std::min<uint32_t>((Np + 255) / 256, 148 * 4);
-    c->partials = dalloc<BBoxPartial>(c->npartials);
-    c->staging = dalloc<double>((size_t)Np * std::max<int>(dd, (int)MTR_NUM_SCALARS));
+    c->uploads_reused += reuse ? 1 : 0;
     // state -> buffer 0 (AoS host layout -> SoA)
     const uint32_t blocks = (Np + 255) / 256;
     auto put = [&](const double* host, void* dst, int width, int kind, const double* fill) {
@@ -1175,10 +1192,17 @@ int mtr_upload(mtr_ctx* c, const double* x, const double* v, const double* F, co
       scp = sc.data();
     }
     put(scp, c->buf[0].sc, MTR_NUM_SCALARS, 2, nullptr);
-    // initial grid allocation
+    // initial grid: kept when the new scene's extent fits the grid there is
     uint32_t want[3];
     initial_grid_extent(c, x, want);
-    alloc_grid(c, want);
+    bool fits = reuse && c->gx != nullptr;
+    for (int a = 0; a < d; ++a) fits = fits && want[a] <= c->cap_axis[a];
+    if (fits) {
+      clear_grid(c);
+    } else {
+      free_graphs(c);  // captured with the old grid's addresses
+      alloc_grid(c, want);
+    }
     // header
     std::memset(c->hH, 0, sizeof(StepHeader));
     c->hH->first_bad = 0xffffffffu;

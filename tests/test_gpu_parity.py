@@ -187,3 +187,31 @@ def test_periodic(dim, deg, musl, fr, nsteps):
     compare_states(g, o, REL_ONE_STEP if nsteps == 1 else 1e-9, sens=oracle_sensitivity(sc, nsteps))
     x0 = g["p"]["x"][:, 0]
     assert x0.min() >= 0.0 and x0.max() <= sc.params.L[0]
+
+
+def test_reupload_into_a_used_context():
+    """mtr_upload of a scene with the same particle count into a context that
+    already stepped another keeps its buffers and step graphs and refills
+    them; the result equals a fresh context's.  Then a scene of the same count
+    spread over three times the extent, whose grid no longer fits, and one of
+    another count."""
+    from matter_tests_b200.gpu import GpuSim
+    a = cases.apply(cases.block(3, 3, n=6, seed=3), plastic_model=cases.PM.DPMui, use_musl=1, flip_ratio=-0.95)
+    b = cases.apply(cases.block(3, 3, n=6, seed=8), plastic_model=cases.PM.DPMui, use_musl=1, flip_ratio=-0.95)
+    b.x = b.x + np.array([0.013, 0.002, -0.007])
+    wide = cases.apply(cases.block(3, 3, n=6, seed=9), plastic_model=cases.PM.DPMui, use_musl=1, flip_ratio=-0.95)
+    wide.x = wide.x * 3.0
+    other = cases.apply(cases.block(3, 3, n=5, seed=4), plastic_model=cases.PM.DPMui, use_musl=1, flip_ratio=-0.95)
+    assert a.Np == b.Np == wide.Np != other.Np
+    g = GpuSim(a.params)
+    for sc in (a, b, wide, other, b):
+        g.upload(sc.x, sc.v, sc.F, sc.B, sc.scalars)
+        g.set_scene_objects(sc)
+        g.step(20)
+        got = g.particles()
+        assert g.clock()["step"] == 20
+        ref = run_gpu(sc, 20, keep_pic_flip=False)
+        for k in ("x", "v", "F", "B"):
+            scale = max(np.abs(ref["p"][k]).max(), 1e-300)
+            assert np.abs(got[k] - ref["p"][k]).max() <= 1e-10 * scale, (sc.name, k)
+    g.close()
