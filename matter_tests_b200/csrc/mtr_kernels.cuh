@@ -684,6 +684,12 @@ constexpr int kMaxTileThreads = 256;
 #ifndef MTR_DEFGRAD_MIN_BLOCKS_F32
 #define MTR_DEFGRAD_MIN_BLOCKS_F32 6
 #endif
+// The return mapping takes its SVD from the symmetric eigenproblem of F F^T
+// (svd_sym); 0 selects the two-sided Jacobi iteration with the reference's
+// ordering and sign conventions instead.
+#ifndef MTR_SYM_SVD
+#define MTR_SYM_SVD 1
+#endif
 #ifndef MTR_G2P_MIN_BLOCKS
 #define MTR_G2P_MIN_BLOCKS 3
 #endif
@@ -719,6 +725,25 @@ __device__ __forceinline__ R stage_pd(const PStage<D, R>& S, const double (*crd)
     return S.pd[a * 4 + o];
 }
 
+// Particles staged per chunk by a scatter block of `threads` threads:
+// threads / DIV.  A smaller chunk needs less shared memory per block (more
+// resident blocks per SM) at the price of more chunk barriers and shorter
+// register runs per lane group.  Measured on the 1M 3D collapse and the 1.2M
+// incline (ms per launch at each kernel's best block shape): P2G with half
+// chunks FP64 0.461 -> 0.449, mixed 0.252 -> 0.245, at 256 threads FP64
+// 0.682 -> 0.471; the MUSL scatter slower with them (mixed 0.252 -> 0.309),
+// so it keeps full chunks.
+#ifndef MTR_P2G_CHUNK_DIV
+#define MTR_P2G_CHUNK_DIV 2
+#endif
+#ifndef MTR_MUSL_CHUNK_DIV
+#define MTR_MUSL_CHUNK_DIV 1
+#endif
+template <typename S, int DIV>
+constexpr size_t stage_bytes(int threads) {
+  return sizeof(S) * (size_t)(threads / DIV);
+}
+
 template <int D, typename R>
 constexpr size_t p2g_crd_bytes() {
   return align16(sizeof(double) * 3 * Tiling<D>::PN);
@@ -729,7 +754,7 @@ constexpr size_t p2g_patch_bytes() {
 }
 template <int D, typename R>
 constexpr size_t p2g_smem_bytes(int threads) {
-  return p2g_crd_bytes<D, R>() + p2g_patch_bytes<D, R>() + sizeof(PStage<D, R>) * (size_t)threads;
+  return p2g_crd_bytes<D, R>() + p2g_patch_bytes<D, R>() + stage_bytes<PStage<D, R>, MTR_P2G_CHUNK_DIV>(threads);
 }
 
 template <int D, int DEG, typename R, int XS = 1>
@@ -775,9 +800,14 @@ __device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t
   // warp's 32, so groups work on different cells and their flushes rarely
   // meet on one patch node (interleaving them made both groups flush the same
   // cell at once, which measured slower despite fewer bank conflicts)
-  const int kbeg = warp * 32 + (lane / LPP) * LPP, kend = kbeg + LPP;
-  for (uint32_t c0 = pb; c0 < pe; c0 += blockDim.x) {
-    {  // phase 1: stage one particle per thread
+  // (with a chunk of blockDim / MTR_P2G_CHUNK_DIV particles, a group takes
+  // LPP / MTR_P2G_CHUNK_DIV of them)
+  static_assert(LPP % MTR_P2G_CHUNK_DIV == 0, "chunk divisor must divide the lanes per particle");
+  constexpr int PPG = LPP / MTR_P2G_CHUNK_DIV;
+  const int chunk = (int)blockDim.x / MTR_P2G_CHUNK_DIV;
+  const int kbeg = ((int)threadIdx.x / LPP) * PPG, kend = kbeg + PPG;
+  for (uint32_t c0 = pb; c0 < pe; c0 += chunk) {
+    if ((int)threadIdx.x < chunk) {  // phase 1: stage one particle per thread
       const uint32_t s = c0 + threadIdx.x;
       PStage<D, R>& S = st[threadIdx.x];
       int packed = -1;
@@ -1197,7 +1227,7 @@ __device__ __forceinline__ void defgrad_and_store(const StepArgsT<R>& A, uint32_
 #pragma unroll
     for (int c = 0; c < D; ++c) p.F[r][c] = p.F[r][c] + T2[r][c];
   double tau[Sym<D>::n];
-  plastic = return_map<D, PM>(*A.P, dt, p.F, p.s, tau, flags);
+  plastic = return_map<D, PM, MTR_SYM_SVD != 0>(*A.P, dt, p.F, p.s, tau, flags);
   store_defgrad<D, R>(A.out, A.Np, s, p.F, p.s, tau);
 }
 
@@ -1482,7 +1512,7 @@ constexpr size_t musl_patch_bytes() {
 }
 template <int D, typename R>
 constexpr size_t musl_smem_bytes(int threads) {
-  return musl_crd_bytes<D, R>() + musl_patch_bytes<D, R>() + sizeof(MStage<D, R>) * (size_t)threads;
+  return musl_crd_bytes<D, R>() + musl_patch_bytes<D, R>() + stage_bytes<MStage<D, R>, MTR_MUSL_CHUNK_DIV>(threads);
 }
 
 template <int D, int DEG, typename R, int XS = 1>
@@ -1521,9 +1551,12 @@ __device__ __forceinline__ void g2p_musl_w_body(const StepArgsT<R>& A, const uin
   const int iz = D == 3 ? ((q % COLS) & 3) : 0;
   const int h0 = (q / COLS) * HN;
   // consecutive particles per lane group, as in k_p2g_w
-  const int kbeg = warp * 32 + (lane / LPP) * LPP, kend = kbeg + LPP;
-  for (uint32_t c0 = pb; c0 < pe; c0 += blockDim.x) {
-    {  // phase 1
+  static_assert(LPP % MTR_MUSL_CHUNK_DIV == 0, "chunk divisor must divide the lanes per particle");
+  constexpr int PPG = LPP / MTR_MUSL_CHUNK_DIV;
+  const int chunk = (int)blockDim.x / MTR_MUSL_CHUNK_DIV;
+  const int kbeg = ((int)threadIdx.x / LPP) * PPG, kend = kbeg + PPG;
+  for (uint32_t c0 = pb; c0 < pe; c0 += chunk) {
+    if ((int)threadIdx.x < chunk) {  // phase 1
       const uint32_t s = c0 + threadIdx.x;
       MStage<D, R>& S = st[threadIdx.x];
       int packed = -1;

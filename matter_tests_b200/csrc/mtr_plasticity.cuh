@@ -281,7 +281,10 @@ __device__ void initial_tau(const DevParams& P, const double (&F)[D][D], double*
 // model is then known at compile time and the other models' code is not
 // emitted: a smaller kernel that fits the instruction cache); PM = -1 reads
 // the model from P at run time.
-template <int D, int PM = -1>
+// SYM selects the SVD through the symmetric eigenproblem of F F^T
+// (svd_sym); otherwise the two-sided Jacobi iteration with the reference's
+// conventions.
+template <int D, int PM = -1, bool SYM = false>
 __device__ bool return_map(const DevParams& P, double dt, double (&F)[D][D], PScalars& s, double* tau,
                            uint32_t& flags) {
   const int pm = PM >= 0 ? PM : P.plastic_model;
@@ -290,7 +293,10 @@ __device__ bool return_map(const DevParams& P, double dt, double (&F)[D][D], PSc
       neohookean_tau<D>(P, F, tau);
     } else {
       double U[D][D], V[D][D], S[D], h[D];
-      svd<D>(F, U, S, V, P.svd_rel);
+      if constexpr (SYM)
+        svd_sym<D>(F, U, S, V, P.svd_rel);
+      else
+        svd<D>(F, U, S, V, P.svd_rel);
 #pragma unroll
       for (int i = 0; i < D; ++i) h[i] = ool_log(fabs(S[i]));
       hencky_tau<D>(P, U, h, tau);
@@ -305,7 +311,10 @@ __device__ bool return_map(const DevParams& P, double dt, double (&F)[D][D], PSc
   const double K = P.K, M = P.M, qc = P.q_cohesion;
   const double e_mu = P.e_mu_prefac, d_pre = P.d_prefac, f_mu = P.f_mu_prefac;
   double U[D][D], V[D][D], S[D];
-  svd<D, PM != MTR_PM_DPMUI>(F, U, S, V, P.svd_rel);
+  if constexpr (SYM)
+    svd_sym<D>(F, U, S, V, P.svd_rel);
+  else
+    svd<D, PM != MTR_PM_DPMUI>(F, U, S, V, P.svd_rel);
   double hencky[D], hdev[D];
 #pragma unroll
   for (int i = 0; i < D; ++i) hencky[i] = ool_log(dmax(fabs(S[i]), 1e-4));  // plasticity.cpp:21

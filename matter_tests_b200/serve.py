@@ -68,6 +68,8 @@ class Server:
         self.keep = keep_result
         self.tick_ms = []        # wall time of each tick
         self.tick_members = []   # scenes stepped in each tick
+        self.tick_particles = []  # particles stepped in each tick
+        self.tick_rebuilt = []   # the tick's batch was (re)built just before it
         self.peak_members = 0
         self.peak_bytes = 0
         # wall time outside the ticks, by cause (seconds)
@@ -154,7 +156,8 @@ class Server:
                     self.host_s["idle"] += now() - ti
                     continue
                 key = tuple(r.rid for r in active)
-                if key != members_key:
+                rebuilt = key != members_key
+                if rebuilt:
                     tb = now()
                     if batch is not None:
                         batch.close()
@@ -170,6 +173,8 @@ class Server:
                 batch.step(self.tick_steps)
                 self.tick_ms.append((now() - ts) * 1e3)
                 self.tick_members.append(len(active))
+                self.tick_particles.append(sum(r.scene.Np for r in active))
+                self.tick_rebuilt.append(rebuilt)
                 self.peak_members = max(self.peak_members, len(active))
                 still = []
                 for r, ck in zip(active, batch.clocks()):
@@ -216,6 +221,18 @@ class Server:
                 batch.set_tile_lanes(i, sh["lanes"])
 
     # -- report ---------------------------------------------------------------
+    def _split(self, frame):
+        rb = np.array(self.tick_rebuilt, dtype=bool)
+        mp = np.array(self.tick_particles, dtype=np.float64) / 1e6
+        out = {}
+        for name, m in (("after_rebuild", rb), ("steady", ~rb)):
+            if m.any():
+                out[name] = {"ticks": int(m.sum()), "p50": float(np.percentile(frame[m], 50)),
+                             "p99": float(np.percentile(frame[m], 99)),
+                             "per_mparticle_p50": float(np.percentile(frame[m] / np.maximum(mp[m], 1e-9), 50)),
+                             "per_mparticle_p99": float(np.percentile(frame[m] / np.maximum(mp[m], 1e-9), 99))}
+        return out
+
     def report(self, done):
         lat = np.array([r.done - r.arrival for r in done])
         wait = np.array([r.admitted - r.arrival for r in done])
@@ -233,6 +250,10 @@ class Server:
             "step_latency_ms": {"p50": float(np.percentile(per_step, 50)), "p99": float(np.percentile(per_step, 99))},
             # a frame of the serving loop = one tick: tick_steps steps of every admitted scene
             "frame_latency_ms": {"p50": float(np.percentile(frame, 50)), "p99": float(np.percentile(frame, 99))},
+            # the same, split into ticks right after a membership change (their batch
+            # was rebuilt: new tables and a new step graph) and the other ticks; and
+            # per million particles stepped, which takes out the batch's size
+            "frame_latency_split_ms": self._split(frame),
             "tick_steps": self.tick_steps,
             "ticks": len(self.tick_ms),
             "peak_members": self.peak_members,
