@@ -69,6 +69,8 @@ def parse():
     ap.add_argument("--ensemble-size", type=int, default=256, help="scenes of the batched ensemble")
     ap.add_argument("--ensemble-steps", type=int, default=500, help="timed steps of the batched ensemble")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
+                    help="forms of the step to time (one form only: for profiler captures)")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the full-length runs of the three single-scene workloads")
     ap.add_argument("--serve-requests", type=int, default=60, help="requests of the serving measurement")
@@ -734,6 +736,21 @@ def gpu_arm(args, world, rank, local):
         pass
     sampler = ClockSampler(uuid)
     sampler.start()
+    if args.precision != "both":  # one form alone (profiler captures): a reduced line
+        prec = PREC_FP64 if args.precision == "fp64" else PREC_MIXED
+        one, _ = measure(args, world, rank, local, sc, prec)
+        clocks = sampler.stop()
+        if rank == 0:
+            cfg = config_of(args, sc)
+            cfg["precision"] = args.precision
+            print(json.dumps({"metric": METRIC, "value": one["value"], "unit": METRIC, "n_gpus": world,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": one["ms_per_step"],
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                              "dtype": "f64" if prec == PREC_FP64 else "f32+f64",
+                              "data": "synthetic (seeded jittered lattice)", "config": cfg,
+                              "roofline": one["roofline"], "kernel_ms": one["kernel_ms"], "e2e": one["e2e"],
+                              "gpu_launches": one["gpu_launches"], "clocks": clocks}), flush=True)
+        return 0
     fp64, st64 = measure(args, world, rank, local, sc, PREC_FP64)
     mixed, st32 = measure(args, world, rank, local, sc, PREC_MIXED)
     cfgs = None

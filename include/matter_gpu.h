@@ -272,6 +272,15 @@ int mtr_balance(mtr_ctx* ctx, double* grid_mass, double* grid_momentum, double* 
  * steps than the others ends exactly on time. */
 int mtr_set_step_limit(mtr_ctx* ctx, uint32_t last_step);
 int mtr_batch_create(mtr_ctx* const* ctxs, int n, mtr_batch** out);
+/* Replaces the members of a batch (no counterpart in the reference): the
+ * batch keeps its stream, the block shapes of every group whose key stays in
+ * use and its instantiated step graph, which the next mtr_batch_step updates
+ * in place when the launch sequence is unchanged (same groups and radix
+ * passes) instead of instantiating it again.  A serving loop calls it when
+ * scenes join or leave.  Members that leave stay alive. */
+int mtr_batch_set_members(mtr_batch* batch, mtr_ctx* const* ctxs, int n);
+/* How many batch rebuilds updated the instantiated graph in place. */
+int mtr_batch_graph_updates(mtr_batch* batch);
 int mtr_batch_step(mtr_batch* batch, int nsteps);
 int64_t mtr_batch_launch_count(mtr_batch* batch);
 /* Host-side bookkeeping of mtr_batch_step since mtr_batch_create: members'

@@ -439,7 +439,7 @@ int enqueue_step_t(mtr_ctx* c, int parity) {
   k_bbox<D, R><<<c->npartials, 256, 0, st>>>(A);
   ++n;
   mark(c, "k_bbox");
-  k_header<D><<<1, 32, 0, st>>>(A);
+  k_header<D><<<1, 256, 0, st>>>(A);
   ++n;
   mark(c, "k_header");
   // sort
@@ -472,7 +472,7 @@ int enqueue_step_t(mtr_ctx* c, int parity) {
   mark(c, "k_tile_ranges");
   const int* tt = c->tile_threads;
   {
-    const size_t sm = p2g_smem_bytes<D, R>(tt[kSlotP2G]);
+    const size_t sm = p2g_smem_bytes<D, R>(tt[kSlotP2G], c->prm.use_mibf != 0);
     if (c->tile_split[kSlotP2G] == 2)
       k_p2g_w<D, DEG, R, 2><<<c->cap_tiles, tt[kSlotP2G], sm, st>>>(A, perm);
     else
@@ -778,16 +778,23 @@ struct mtr_batch {
   EventMarks marks;    // tagged with the group index
   // host-side bookkeeping of mtr_batch_step (mtr_batch_stats)
   int64_t regrowths = 0, rebuilds = 0;
+  int64_t updates = 0;  // rebuilds that updated the instantiated graph in place
   double regrow_ms = 0.0, rebuild_ms = 0.0;
 };
 
 namespace {
 
-void free_batch_tables(mtr_batch* b) {
+void free_batch_graph(mtr_batch* b) {
   if (b->graph) {
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
   }
+}
+
+// Frees the argument and offset tables.  The instantiated step graph is kept:
+// rebuild_batch updates it in place from the next capture when the step's
+// launch sequence is unchanged.
+void free_batch_tables(mtr_batch* b) {
   for (auto& g : b->groups) {
     // stream-ordered frees: a plain cudaFree waits for the whole GPU, which
     // would stall other contexts' work (the serving loop rebuilds batches
@@ -844,7 +851,7 @@ int enqueue_group_step_t(mtr_batch* b, mtr_batch_group& g, int gi) {
   const int* tt = g.tile_threads;
   int n = 0;
   kb_bbox<D, R><<<g.total[kBK_BBOX], 256, 0, st>>>(B);
-  kb_header<D, R><<<g.total[kBK_ONE], 32, 0, st>>>(B);
+  kb_header<D, R><<<g.total[kBK_ONE], 256, 0, st>>>(B);
   kb_clear<D, R><<<g.total[kBK_CLEAR], 256, 0, st>>>(B);
   n += 3;
   for (int pass = 0; pass < g.passes; ++pass) {
@@ -960,7 +967,20 @@ void rebuild_batch(mtr_batch* b) {
     throw;
   }
   CK(cudaStreamEndCapture(b->stream, &graph));
-  cudaError_t e = cudaGraphInstantiate(&b->graph, graph, 0);
+  // A membership change or a regrown grid changes launch sizes and table
+  // addresses but usually not the launch sequence: the instantiated graph is
+  // then updated in place (much cheaper than instantiating it again).
+  if (b->graph) {
+    cudaGraphExecUpdateResultInfo info{};
+    if (cudaGraphExecUpdate(b->graph, graph, &info) == cudaSuccess) {
+      b->updates += 1;
+    } else {
+      (void)cudaGetLastError();
+      free_batch_graph(b);
+    }
+  }
+  cudaError_t e = cudaSuccess;
+  if (!b->graph) e = cudaGraphInstantiate(&b->graph, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) throw MtrError{MTR_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)};
   b->launches_per_step = n / kBatchGraphSteps;
@@ -983,36 +1003,57 @@ void write_batch_headers(mtr_batch* b) {
 // Block-shape tuning over kTuneRounds candidates: candidate k runs every tile
 // kernel with kTileCandidates[k % 3] threads (capped at the slot's maximum)
 // and the scatters with x split 1 + k / 3 (16 or 32 lanes per particle in 3D,
-// 4 or 8 in 2D).  best[slot][k] is the shortest time seen for the slot's
-// kernel with candidate k (infinity: not measured); for the gathers, whose
-// shape is the thread count alone, rounds k and k + 3 are the same candidate.
-// A slot keeps its current shape unless another candidate was more than 2%
-// faster, so timing noise does not flip an equal choice.
+// 4 or 8 in 2D).  The candidates are interleaved: each repetition times every
+// candidate once, so slow drifts of the state or the clock touch them all
+// alike.  samples[slot][k] holds the times of the slot's kernel with
+// candidate k; for the gathers, whose shape is the thread count alone,
+// rounds k and k + 3 are the same candidate.  A candidate's time is the
+// median of its samples and its noise the half-range of its samples relative
+// to that median; a slot keeps its current shape unless another candidate is
+// faster by more than 2% and by more than the noise of the two together, so
+// timing noise does not trade an equal shape for a slower one.
 constexpr int kTuneRounds = 6;
 
 struct TuneTimes {
-  double best[kTileSlots][kTuneRounds];
-  TuneTimes() {
-    for (auto& r : best)
-      for (double& v : r) v = 1e300;
-  }
+  std::vector<double> samples[kTileSlots][kTuneRounds];
   void add(const char* name, float ms, int k) {
     for (int sl = 0; sl < kTileSlots; ++sl)
-      if (std::strcmp(name, kSlotMark[sl]) == 0) best[sl][k] = std::min(best[sl][k], (double)ms);
+      if (std::strcmp(name, kSlotMark[sl]) == 0) samples[sl][k].push_back((double)ms);
+  }
+  // (median, relative half-range) of one candidate of a slot; median < 0: not measured
+  std::pair<double, double> stats(int sl, int k) const {
+    std::vector<double> v = samples[sl][k];
+    if (sl >= kScatterSlots) v.insert(v.end(), samples[sl][k + 3].begin(), samples[sl][k + 3].end());
+    if (v.empty()) return {-1.0, 0.0};
+    std::sort(v.begin(), v.end());
+    const size_t n = v.size();
+    const double med = n % 2 ? v[n / 2] : 0.5 * (v[n / 2 - 1] + v[n / 2]);
+    return {med, med > 0.0 ? 0.5 * (v.back() - v.front()) / med : 0.0};
   }
   void choose(int* threads, int* split) const {
     for (int sl = 0; sl < kTileSlots; ++sl) {
       const bool scatter = sl < kScatterSlots;
       const int nk = scatter ? kTuneRounds : 3;
-      auto time_of = [&](int k) { return scatter ? best[sl][k] : std::min(best[sl][k], best[sl][k + 3]); };
       int cur = -1, arg = -1;
+      double tcur = 0.0, ncur = 0.0, targ = 0.0, narg = 0.0;
       for (int k = 0; k < nk; ++k) {
-        if (kTileCandidates[k % 3] > kSlotMax[sl] || time_of(k) >= 1e300) continue;
-        if (kTileCandidates[k % 3] == threads[sl] && (!scatter || 1 + k / 3 == split[sl])) cur = k;
-        if (arg < 0 || time_of(k) < time_of(arg)) arg = k;
+        if (kTileCandidates[k % 3] > kSlotMax[sl]) continue;
+        const auto st = stats(sl, k);
+        if (st.first < 0.0) continue;
+        if (kTileCandidates[k % 3] == threads[sl] && (!scatter || 1 + k / 3 == split[sl])) {
+          cur = k;
+          tcur = st.first;
+          ncur = st.second;
+        }
+        if (arg < 0 || st.first < targ) {
+          arg = k;
+          targ = st.first;
+          narg = st.second;
+        }
       }
       if (arg < 0) continue;  // the slot's kernel does not run in this step
-      if (cur >= 0 && time_of(cur) <= 1.02 * time_of(arg)) continue;
+      const double margin = std::max(0.02, ncur + narg);
+      if (cur >= 0 && tcur <= (1.0 + margin) * targ) continue;
       threads[sl] = kTileCandidates[arg % 3];
       if (scatter) split[sl] = 1 + arg / 3;
     }
@@ -1138,7 +1179,7 @@ int mtr_upload(mtr_ctx* c, const double* x, const double* v, const double* F, co
       c->valsB = dalloc<uint32_t>(Np);
       c->hist = dalloc<uint32_t>((size_t)256 * c->sort_blocks);
       c->dtot = dalloc<uint32_t>(256);
-      c->npartials = (int)std::min<uint32_t>((Np + 255) / 256, 148 * 4);
+      c->npartials = (int)std::min<uint32_t>((Np + 255) / 256, 148 * 8);
       c->partials = dalloc<BBoxPartial>(c->npartials);
       c->staging = dalloc<double>((size_t)Np * std::max<int>(dd, (int)MTR_NUM_SCALARS));
     }
@@ -1899,50 +1940,93 @@ int mtr_footprint(const mtr_params* params, uint32_t Np, const double* x, uint64
   });
 }
 
+}  // extern "C"
+
+namespace {
+
+// Checks a member list and (re)groups it into b: groups keep their order and
+// block shapes when their key (dim, spline, precision, MUSL, return-mapping
+// kernel) stays in use, new keys are appended with the shapes of their first
+// member, and groups left without members are dropped.
+void assign_members(mtr_batch* b, mtr_ctx* const* ctxs, int n) {
+  if (!ctxs || n <= 0) throw MtrError{MTR_ERR_INVALID, "null argument or n <= 0"};
+  for (int i = 0; i < n; ++i) {
+    if (!ctxs[i] || !ctxs[i]->uploaded) throw MtrError{MTR_ERR_STATE, "every member needs mtr_upload first"};
+    check_levelsets(ctxs[i]);
+    if (ctxs[i]->device != ctxs[0]->device) throw MtrError{MTR_ERR_INVALID, "members must share one device"};
+    if (ctxs[i]->prm.pbc) throw MtrError{MTR_ERR_INVALID, "periodic scenes step on their own, not in a batch"};
+    for (int j = 0; j < i; ++j)
+      if (ctxs[j] == ctxs[i]) throw MtrError{MTR_ERR_INVALID, "a context appears twice"};
+  }
+  if (!b->members.empty() && ctxs[0]->device != b->device)
+    throw MtrError{MTR_ERR_INVALID, "members must share the batch's device"};
+  b->members.clear();
+  for (auto& g : b->groups) g.members.clear();
+  for (int i = 0; i < n; ++i) {
+    mtr_ctx* c = ctxs[i];
+    CK(cudaStreamSynchronize(c->stream));  // nothing of the member may still run on its own stream
+    b->members.push_back(c);
+    mtr_batch_group* g = nullptr;
+    const int musl = c->prm.use_musl ? 1 : 0;
+    const int spm = rm_specialization(c->dim, musl != 0, c->prm.plastic_model);
+    for (auto& q : b->groups)
+      if (q.dim == c->dim && q.deg == c->deg && q.fp32 == c->fp32 && q.musl == musl && q.spm == spm) g = &q;
+    if (!g) {
+      b->groups.emplace_back();
+      g = &b->groups.back();
+      g->dim = c->dim;
+      g->deg = c->deg;
+      g->fp32 = c->fp32;
+      g->musl = musl;
+      g->spm = spm;
+      std::copy(c->tile_threads, c->tile_threads + kTileSlots, g->tile_threads);
+      std::copy(c->tile_split, c->tile_split + kScatterSlots, g->tile_split);
+    }
+    g->members.push_back(c);
+  }
+  for (size_t i = 0; i < b->groups.size();) {
+    if (b->groups[i].members.empty()) {
+      mtr_batch_group& g = b->groups[i];
+      if (g.dargs) cudaFreeAsync(g.dargs, b->stream);
+      if (g.doff) cudaFreeAsync(g.doff, b->stream);
+      b->groups.erase(b->groups.begin() + (long)i);
+    } else {
+      ++i;
+    }
+  }
+  b->dirty = true;
+}
+
+}  // namespace
+
+extern "C" {
+
 int mtr_batch_create(mtr_ctx* const* ctxs, int n, mtr_batch** out) {
   return guarded([&]() -> int {
     if (!ctxs || !out || n <= 0) throw MtrError{MTR_ERR_INVALID, "null argument or n <= 0"};
     *out = nullptr;
-    for (int i = 0; i < n; ++i) {
-      if (!ctxs[i] || !ctxs[i]->uploaded) throw MtrError{MTR_ERR_STATE, "every member needs mtr_upload first"};
-      check_levelsets(ctxs[i]);
-      if (ctxs[i]->device != ctxs[0]->device) throw MtrError{MTR_ERR_INVALID, "members must share one device"};
-      if (ctxs[i]->prm.pbc) throw MtrError{MTR_ERR_INVALID, "periodic scenes step on their own, not in a batch"};
-      for (int j = 0; j < i; ++j)
-        if (ctxs[j] == ctxs[i]) throw MtrError{MTR_ERR_INVALID, "a context appears twice"};
-    }
     mtr_batch* b = new mtr_batch();
     try {
+      if (!ctxs[0]) throw MtrError{MTR_ERR_INVALID, "null member"};
       b->device = ctxs[0]->device;
       CK(cudaSetDevice(b->device));
       CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-      for (int i = 0; i < n; ++i) {
-        mtr_ctx* c = ctxs[i];
-        CK(cudaStreamSynchronize(c->stream));  // nothing of the member may still run on its own stream
-        b->members.push_back(c);
-        mtr_batch_group* g = nullptr;
-        const int musl = c->prm.use_musl ? 1 : 0;
-        const int spm = rm_specialization(c->dim, musl != 0, c->prm.plastic_model);
-        for (auto& q : b->groups)
-          if (q.dim == c->dim && q.deg == c->deg && q.fp32 == c->fp32 && q.musl == musl && q.spm == spm) g = &q;
-        if (!g) {
-          b->groups.emplace_back();
-          g = &b->groups.back();
-          g->dim = c->dim;
-          g->deg = c->deg;
-          g->fp32 = c->fp32;
-          g->musl = musl;
-          g->spm = spm;
-          std::copy(c->tile_threads, c->tile_threads + kTileSlots, g->tile_threads);
-          std::copy(c->tile_split, c->tile_split + kScatterSlots, g->tile_split);
-        }
-        g->members.push_back(c);
-      }
+      assign_members(b, ctxs, n);
     } catch (...) {
       mtr_batch_destroy(b);
       throw;
     }
     *out = b;
+    return MTR_OK;
+  });
+}
+
+int mtr_batch_set_members(mtr_batch* b, mtr_ctx* const* ctxs, int n) {
+  return guarded([&]() -> int {
+    if (!b) throw MtrError{MTR_ERR_INVALID, "null batch"};
+    CK(cudaSetDevice(b->device));
+    CK(cudaStreamSynchronize(b->stream));
+    assign_members(b, ctxs, n);
     return MTR_OK;
   });
 }
@@ -2145,6 +2229,8 @@ int mtr_batch_autotune(mtr_batch* b, int reps) {
 
 int64_t mtr_batch_launch_count(mtr_batch* b) { return b ? b->launches_last : 0; }
 
+int mtr_batch_graph_updates(mtr_batch* b) { return b ? (int)std::min<int64_t>(b->updates, 0x7fffffff) : MTR_ERR_INVALID; }
+
 int mtr_batch_stats(mtr_batch* b, int64_t* regrowths, double* regrow_ms, int64_t* rebuilds, double* rebuild_ms) {
   if (!b) return MTR_ERR_INVALID;
   if (regrowths) *regrowths = b->regrowths;
@@ -2160,6 +2246,7 @@ void mtr_batch_destroy(mtr_batch* b) {
   if (!b) return;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
+  free_batch_graph(b);
   free_batch_tables(b);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;

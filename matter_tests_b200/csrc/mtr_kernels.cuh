@@ -155,6 +155,7 @@ template <int D, typename R>
 __device__ __forceinline__ void bbox_body(const StepArgsT<R>& A, const uint32_t bid, const uint32_t nblk) {
   if (step_inactive(A.H)) return;
   double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300}, v2 = 0.0, vs[3] = {0.0, 0.0, 0.0};
+#pragma unroll 4
   for (uint32_t i = bid * blockDim.x + threadIdx.x; i < A.Np; i += nblk * blockDim.x) {
     double vv[3];
 #pragma unroll
@@ -219,9 +220,11 @@ __device__ __forceinline__ void header_body(const StepCommon& A) {
   StepHeader* H = A.H;
   const DevParams& P = *A.P;
   if (step_inactive(H)) return;
-  const int lane = threadIdx.x;
+  // the block (blockDim.x a multiple of 32, at most 256) reduces the bbox
+  // partials; warp 0 then does the rest
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300}, v2 = 0.0, vs[3] = {0.0, 0.0, 0.0};
-  for (int b = lane; b < A.npartials; b += 32) {
+  for (int b = threadIdx.x; b < A.npartials; b += blockDim.x) {
     const BBoxPartial& q = A.partials[b];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -240,6 +243,29 @@ __device__ __forceinline__ void header_body(const StepCommon& A) {
       vs[a] += __shfl_xor_sync(0xffffffffu, vs[a], off);
     }
     v2 = fmax(v2, __shfl_xor_sync(0xffffffffu, v2, off));
+  }
+  if (nw > 1) {
+    __shared__ BBoxPartial wred[8];
+    if (lane == 0) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        wred[wid].mn[a] = mn[a];
+        wred[wid].mx[a] = mx[a];
+        wred[wid].vsum[a] = vs[a];
+      }
+      wred[wid].v2 = v2;
+    }
+    __syncthreads();
+    if (wid != 0) return;
+    for (int w = 1; w < nw; ++w) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        mn[a] = fmin(mn[a], wred[w].mn[a]);
+        mx[a] = fmax(mx[a], wred[w].mx[a]);
+        vs[a] += wred[w].vsum[a];
+      }
+      v2 = fmax(v2, wred[w].v2);
+    }
   }
   __shared__ double s_low[3], s_high[3], s_stop[3];
   __shared__ int s_ok;
@@ -366,7 +392,7 @@ __device__ __forceinline__ void header_body(const StepCommon& A) {
 }
 
 template <int D>
-__global__ void __launch_bounds__(32) k_header(StepCommon A) {
+__global__ void __launch_bounds__(256) k_header(StepCommon A) {
   header_body<D>(A);
 }
 
@@ -733,6 +759,20 @@ __device__ __forceinline__ R stage_pd(const PStage<D, R>& S, const double (*crd)
 // chunks FP64 0.461 -> 0.449, mixed 0.252 -> 0.245, at 256 threads FP64
 // 0.682 -> 0.471; the MUSL scatter slower with them (mixed 0.252 -> 0.309),
 // so it keeps full chunks.
+// The scatters stage B already multiplied by D^-1 (apicDinverse) and P2G the
+// stress already multiplied by 1/dx, so phase 2 (run by every lane of a
+// particle's group) does not repeat those products.
+// The scatters' test of the reference's weight threshold as a select (a
+// zero weight adds nothing) instead of a branch around each node's sums; the
+// branch split the unrolled node loop.  Measured (ms per launch at the best
+// shape): FP64 P2G 0.391 -> 0.370 on the 1M collapse and 0.511 -> 0.471 on the
+// 1.2M incline, mixed P2G 0.244 -> 0.237, FP64 MUSL 0.397 -> 0.375.
+#ifndef MTR_SCATTER_SELECT
+#define MTR_SCATTER_SELECT 1
+#endif
+#ifndef MTR_SCATTER_PRESCALE
+#define MTR_SCATTER_PRESCALE 1
+#endif
 #ifndef MTR_P2G_CHUNK_DIV
 #define MTR_P2G_CHUNK_DIV 2
 #endif
@@ -748,13 +788,16 @@ template <int D, typename R>
 constexpr size_t p2g_crd_bytes() {
   return align16(sizeof(double) * 3 * Tiling<D>::PN);
 }
+// The patch's last channel (MIBF friction) is allocated only under MIBF: a
+// block without it needs 2.7 KB (FP64, 3D) less shared memory, which lets
+// five FP64 P2G blocks of 128 threads share an SM instead of four.
 template <int D, typename R>
-constexpr size_t p2g_patch_bytes() {
-  return align16(sizeof(R) * Tiling<D>::NCH * Tiling<D>::NODES);
+__host__ __device__ constexpr size_t p2g_patch_bytes(bool mibf) {
+  return align16(sizeof(R) * (Tiling<D>::NCH - (mibf ? 0 : 1)) * Tiling<D>::NODES);
 }
 template <int D, typename R>
-constexpr size_t p2g_smem_bytes(int threads) {
-  return p2g_crd_bytes<D, R>() + p2g_patch_bytes<D, R>() + stage_bytes<PStage<D, R>, MTR_P2G_CHUNK_DIV>(threads);
+constexpr size_t p2g_smem_bytes(int threads, bool mibf = true) {
+  return p2g_crd_bytes<D, R>() + p2g_patch_bytes<D, R>(mibf) + stage_bytes<PStage<D, R>, MTR_P2G_CHUNK_DIV>(threads);
 }
 
 template <int D, int DEG, typename R, int XS = 1>
@@ -772,11 +815,14 @@ __device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double(*crd)[PN] = reinterpret_cast<double(*)[PN]>(smem_raw);
   R(*patch)[NODES] = reinterpret_cast<R(*)[NODES]>(smem_raw + p2g_crd_bytes<D, R>());
-  PStage<D, R>* st = reinterpret_cast<PStage<D, R>*>(smem_raw + p2g_crd_bytes<D, R>() + p2g_patch_bytes<D, R>());
+  const bool mibf = P.use_mibf;
+  const int nch = mibf ? NCH : NCH - 1;  // channels the patch holds
+  PStage<D, R>* st =
+      reinterpret_cast<PStage<D, R>*>(smem_raw + p2g_crd_bytes<D, R>() + p2g_patch_bytes<D, R>(mibf));
   int tc[3];
   tile_coords<D>(H, t, tc);
   const int n0[3] = {tc[0] * TB - 1, tc[1] * TB - 1, D == 3 ? tc[2] * TB - 1 : 0};
-  for (int i = threadIdx.x; i < NCH * NODES; i += blockDim.x) (&patch[0][0])[i] = R(0.0);
+  for (int i = threadIdx.x; i < nch * NODES; i += blockDim.x) (&patch[0][0])[i] = R(0.0);
   for (int i = threadIdx.x; i < D * PN; i += blockDim.x) {
     const int a = i / PN, o = i % PN;
     const int g = n0[a] + o;
@@ -788,7 +834,6 @@ __device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t
   const double ioh = P.one_over_dx;
   const R iohR = (R)ioh, apicD = (R)P.apicDinverse;
   const bool apic = P.flip_ratio < 0;
-  const bool mibf = P.use_mibf;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // XS lanes share a stencil column, each owning HN = 4 / XS of its x nodes
   constexpr int COLS = D == 3 ? 16 : 4, LPP = COLS * XS, HN = 4 / XS;
@@ -827,9 +872,12 @@ __device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t
           if (lb[a] < 0 || lb[a] > PN - 4 || b + 3 >= (int)H->N[a]) oob = true;
         }
 #pragma unroll
-        for (int q = 0; q < D * D; ++q) S.B[q] = apic ? A.in.B[(size_t)q * Np + j] : R(0.0);
+        for (int q = 0; q < D * D; ++q)
+          S.B[q] = apic ? (MTR_SCATTER_PRESCALE ? apicD * A.in.B[(size_t)q * Np + j] : A.in.B[(size_t)q * Np + j])
+                        : R(0.0);
 #pragma unroll
-        for (int q = 0; q < NS; ++q) S.tau[q] = A.in.tau[(size_t)q * Np + j];
+        for (int q = 0; q < NS; ++q)
+          S.tau[q] = MTR_SCATTER_PRESCALE ? iohR * A.in.tau[(size_t)q * Np + j] : A.in.tau[(size_t)q * Np + j];
         // MIBF friction is accumulated as the deviation from its initial value
         // mui0, so a uniform field reproduces mui0 exactly at every node
         S.mui = mibf ? (R)((double)A.in.sc[(size_t)MTR_SCALAR_MUI * Np + j] - P.mui0) : R(0.0);
@@ -867,7 +915,7 @@ __device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t
           const int h = h0 + hh;
           const int node = D == 3 ? ((lbx + h) * PN + (lby + iy)) * PN + (lbz + iz) : (lbx + h) * PN + (lby + iy);
 #pragma unroll
-          for (int ch = 0; ch < NCH; ++ch) {
+          for (int ch = 0; ch < NCH; ++ch) {  // the friction accumulator stays zero without MIBF
             if (acc[hh][ch] != R(0.0)) atomicAdd(&patch[ch][node], acc[hh][ch]);
             acc[hh][ch] = R(0.0);
           }
@@ -888,13 +936,19 @@ __device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t
         if constexpr (D == 3) {
           const R wz = S.w[8 + iz], dwz = S.dw[8 + iz];
           wyz = wy * wz;
-          G0 = wyz * iohR;
-          G1 = dwy * wz * iohR;
-          G2 = wy * dwz * iohR;
+          if constexpr (MTR_SCATTER_PRESCALE) {
+            G0 = wyz;
+            G1 = dwy * wz;
+            G2 = wy * dwz;
+          } else {
+            G0 = wyz * iohR;
+            G1 = dwy * wz * iohR;
+            G2 = wy * dwz * iohR;
+          }
         } else {
           wyz = wy;
-          G0 = wy * iohR;
-          G1 = dwy * iohR;
+          G0 = MTR_SCATTER_PRESCALE ? wy : wy * iohR;
+          G1 = MTR_SCATTER_PRESCALE ? dwy : dwy * iohR;
         }
         // force f_a = tau_a . grad w = dwx * Pf_a + wx * Qf_a
         R Pf[D], Qf[D];
@@ -914,8 +968,8 @@ __device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t
           if (apic) {
             R byz = S.B[a * D + 1] * pdy;
             if constexpr (D == 3) byz += S.B[a * D + 2] * pdz;
-            Tm[a] = S.v[a] + apicD * byz;
-            Sm[a] = apicD * S.B[a * D];
+            Tm[a] = S.v[a] + (MTR_SCATTER_PRESCALE ? byz : apicD * byz);
+            Sm[a] = MTR_SCATTER_PRESCALE ? S.B[a * D] : apicD * S.B[a * D];
           } else {
             Tm[a] = S.v[a];
             Sm[a] = R(0.0);
@@ -927,7 +981,15 @@ __device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t
           const int h = h0 + hh;
           const R wx = S.w[h], dwx = S.dw[h];
           const R weight = wx * wyz;
-          if (weight > R(1e-25)) {
+          if constexpr (MTR_SCATTER_SELECT) {
+            // p2g.cpp:35 skips weights <= 1e-25; a zero weight adds nothing
+            const R ws = weight > R(1e-25) ? weight : R(0.0);
+            const R pdx = stage_pd<D, R>(S, crd, 0, lbx, h);
+            acc[hh][0] += ws;
+#pragma unroll
+            for (int a = 0; a < D; ++a) acc[hh][1 + a] += ws * (Tm[a] + Sm[a] * pdx);
+            if (mibf) acc[hh][1 + 2 * D] += mui * ws;
+          } else if (weight > R(1e-25)) {
             const R pdx = stage_pd<D, R>(S, crd, 0, lbx, h);
             acc[hh][0] += weight;
 #pragma unroll
@@ -948,6 +1010,7 @@ __device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t
     if (!patch_node<D>(H, n0, n, l)) continue;
 #pragma unroll
     for (int ch = 0; ch < NCH; ++ch) {
+      if (ch >= nch) break;  // no friction channel without MIBF
       const R val = patch[ch][n];
       if (val != R(0.0)) atomicAdd(&A.acc[(size_t)ch * cap + l], val);
     }
@@ -1080,32 +1143,41 @@ __device__ __forceinline__ void grid_body(const StepArgsT<R>& A, const uint32_t 
   __syncthreads();
   double sum_m = 0.0, sum_p[3] = {0.0, 0.0, 0.0};  // mass and momentum balance (simulation.cpp:292-333)
   for (uint32_t l = bid * blockDim.x + threadIdx.x; l < G; l += nblk * blockDim.x) {
+    // every load of the node first, ahead of the branches on its mass: one
+    // round of memory latency per node instead of several in a row
     const double mraw = A.acc[l];
+    double pacc[3] = {0, 0, 0}, facc[3] = {0, 0, 0};
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      pacc[a] = A.acc[(size_t)(1 + a) * cap + l];
+      facc[a] = A.acc[(size_t)(1 + D + a) * cap + l];
+    }
+    const double fracc = P.use_mibf ? (double)A.acc[(size_t)(1 + 2 * D) * cap + l] : 0.0;
+    const uint32_t k = D == 3 ? l % H->N[2] : 0;
+    const uint32_t r = D == 3 ? l / H->N[2] : l;
+    const uint32_t jj = r % H->N[1], i = r / H->N[1];
+    const double Xi0 = A.gx[i], Xi1 = A.gy[jj], Xi2 = D == 3 ? A.gz[k] : 0.0;
     double v[3] = {0, 0, 0}, vold[3] = {0, 0, 0};
     double fric = 0.0;
     sum_m += mraw;
     if (mraw > 0) {
 #pragma unroll
       for (int a = 0; a < D; ++a) {
-        const double pa = A.acc[(size_t)(1 + a) * cap + l];
-        sum_p[a] += pa;
-        v[a] = pa / mraw;
+        sum_p[a] += pacc[a];
+        v[a] = pacc[a] / mraw;
       }
     }
-    if (P.use_mibf) fric = P.mui0 + (double)A.acc[(size_t)(1 + 2 * D) * cap + l] / mraw;
+    if (P.use_mibf) fric = P.mui0 + fracc / mraw;
     const double mi = mraw * P.particle_mass;
     double fl[3] = {0, 0, 0};
     if (mi > 0) {
-      uint32_t k = D == 3 ? l % H->N[2] : 0;
-      uint32_t r = D == 3 ? l / H->N[2] : l;
-      uint32_t jj = r % H->N[1], i = r / H->N[1];
 #pragma unroll
       for (int a = 0; a < D; ++a) {
-        double inc = -dtpv * (double)A.acc[(size_t)(1 + D + a) * cap + l] / mi + dtg[a];
+        double inc = -dtpv * facc[a] / mi + dtg[a];
         vold[a] = v[a];
         v[a] = vold[a] + inc;
       }
-      double Xi[3] = {A.gx[i], A.gy[jj], D == 3 ? A.gz[k] : 0.0};
+      double Xi[3] = {Xi0, Xi1, Xi2};
       if (!boundary_collision<D>(P, plates, fric, Xi, dt, v)) raise_status(H, MTR_STATUS_BAD_BC, 0xffffffffu);
 #pragma unroll
       for (int a = 0; a < D; ++a) fl[a] = v[a] - vold[a];
@@ -1606,7 +1678,7 @@ __device__ __forceinline__ void g2p_musl_w_body(const StepArgsT<R>& A, const uin
           for (int c = 0; c < D; ++c) {
             const R b = apic ? Bp[r][c] : R(0.0);
             A.out.B[(size_t)(r * D + c) * Np + s] = b;
-            S.B[r * D + c] = b;
+            S.B[r * D + c] = MTR_SCATTER_PRESCALE ? apicD * b : b;
           }
         A.out.id[s] = pid;
         if (P.store_pic_flip) {
@@ -1673,8 +1745,8 @@ __device__ __forceinline__ void g2p_musl_w_body(const StepArgsT<R>& A, const uin
           if (apic) {
             R byz = S.B[a * D + 1] * pdy;
             if constexpr (D == 3) byz += S.B[a * D + 2] * pdz;
-            Tm[a] = S.v[a] + apicD * byz;
-            Sm[a] = apicD * S.B[a * D];
+            Tm[a] = S.v[a] + (MTR_SCATTER_PRESCALE ? byz : apicD * byz);
+            Sm[a] = MTR_SCATTER_PRESCALE ? S.B[a * D] : apicD * S.B[a * D];
           } else {
             Tm[a] = S.v[a];
             Sm[a] = R(0.0);
@@ -1684,10 +1756,17 @@ __device__ __forceinline__ void g2p_musl_w_body(const StepArgsT<R>& A, const uin
         for (int hh = 0; hh < HN; ++hh) {
           const int h = h0 + hh;
           const R weight = S.w[h] * wyz;
-          if (!(weight > R(1e-25))) continue;
-          const R pdx = stage_pd<D, R>(S, crd, 0, lbx, h);
+          if constexpr (MTR_SCATTER_SELECT) {
+            const R ws = weight > R(1e-25) ? weight : R(0.0);  // musl.cpp:51 skips weights <= 1e-25
+            const R pdx = stage_pd<D, R>(S, crd, 0, lbx, h);
 #pragma unroll
-          for (int a = 0; a < D; ++a) acc[hh][a] += weight * (Tm[a] + Sm[a] * pdx);
+            for (int a = 0; a < D; ++a) acc[hh][a] += ws * (Tm[a] + Sm[a] * pdx);
+          } else {
+            if (!(weight > R(1e-25))) continue;
+            const R pdx = stage_pd<D, R>(S, crd, 0, lbx, h);
+#pragma unroll
+            for (int a = 0; a < D; ++a) acc[hh][a] += weight * (Tm[a] + Sm[a] * pdx);
+          }
         }
       }
       if (cur >= 0) flush();
@@ -1892,7 +1971,7 @@ __global__ void __launch_bounds__(256) kb_bbox(BatchView<R> B) {
 }
 
 template <int D, typename R>
-__global__ void __launch_bounds__(32) kb_header(BatchView<R> B) {
+__global__ void __launch_bounds__(256) kb_header(BatchView<R> B) {
   uint32_t b, nb;
   const StepArgsT<R>* A = batch_locate(B, kBK_ONE, b, nb);
   if (A) header_body<D>(*A);

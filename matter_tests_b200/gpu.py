@@ -28,7 +28,8 @@ EXPORTS = (
     "mtr_autotune", "mtr_set_tile_threads", "mtr_get_tile_threads", "mtr_batch_autotune", "mtr_batch_groups",
     "mtr_batch_get_group", "mtr_batch_set_tile_threads", "mtr_frame_columns", "mtr_frame_begin",
     "mtr_frame_wait", "mtr_get_grid_friction", "mtr_set_levelset", "mtr_set_tile_lanes", "mtr_get_tile_lanes",
-    "mtr_batch_set_tile_lanes", "mtr_batch_clocks", "mtr_batch_stats",
+    "mtr_batch_set_tile_lanes", "mtr_batch_clocks", "mtr_batch_stats", "mtr_batch_set_members",
+    "mtr_batch_graph_updates",
 )
 
 _lib = None
@@ -74,6 +75,8 @@ def load_library(path=LIB_PATH):
     lib.mtr_balance.argtypes = [C.c_void_p, _P, _P, _P, _P]
     lib.mtr_set_step_limit.argtypes = [C.c_void_p, C.c_uint32]
     lib.mtr_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]
+    lib.mtr_batch_set_members.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_int]
+    lib.mtr_batch_graph_updates.argtypes = [C.c_void_p]
     lib.mtr_batch_step.argtypes = [C.c_void_p, C.c_int]
     lib.mtr_batch_launch_count.argtypes = [C.c_void_p]
     lib.mtr_batch_launch_count.restype = C.c_int64
@@ -381,6 +384,18 @@ class GpuBatch:
 
     def step(self, n=1):
         _check(self.lib, "mtr_batch_step", self.lib.mtr_batch_step(self.h, n))
+
+    def set_members(self, sims):
+        """Replaces the members (mtr_batch_set_members): the batch keeps its
+        stream, the group shapes and its step graph, updated in place."""
+        sims = list(sims)
+        arr = (C.c_void_p * len(sims))(*[s.h.value if isinstance(s.h, C.c_void_p) else s.h for s in sims])
+        _check(self.lib, "mtr_batch_set_members", self.lib.mtr_batch_set_members(self.h, arr, len(sims)))
+        self.sims = sims
+
+    def graph_updates(self):
+        """Rebuilds that updated the instantiated step graph in place."""
+        return self.lib.mtr_batch_graph_updates(self.h)
 
     @property
     def stream(self):

@@ -6,7 +6,10 @@ Continuous batching: a request that arrives while others run is prepared
 (context created, particles uploaded) on a worker thread while the batch
 keeps stepping, and joins at the next tick; a finished scene leaves at the
 tick it completes, its result is read back and its memory freed on the
-worker, and the memory it frees admits the next waiting request.  A tick
+worker, and the memory it frees admits the next waiting request.  One batch
+lives through the whole run: joining and leaving replace its members
+(mtr_batch_set_members), which keeps its stream, its groups' block shapes
+and its step graph, updated in place rather than instantiated again.  A tick
 advances every member by `tick_steps` steps; each member has a step limit,
 so it stops exactly after the steps it asked for.
 
@@ -54,7 +57,7 @@ class Server:
     (None keeps it)."""
 
     def __init__(self, budget_bytes, device=0, tick_steps=8, precision=PREC_MIXED, keep_result=("x", "v"),
-                 autotune=True, tune_reps=1, workers=1, shapes=None):
+                 autotune=True, tune_reps=3, workers=1, shapes=None):
         self.workers = int(workers)  # threads that prepare, read back and release requests
         self.autotune = autotune
         self.tune_reps = int(tune_reps)
@@ -74,6 +77,7 @@ class Server:
         self.peak_bytes = 0
         # wall time outside the ticks, by cause (seconds)
         self.host_s = {"idle": 0.0, "batch_build": 0.0, "release": 0.0}
+        self.graph_updates = 0   # batch rebuilds that updated the step graph in place
 
     # -- worker-thread jobs -------------------------------------------------
     def _prepare(self, req):
@@ -159,9 +163,10 @@ class Server:
                 rebuilt = key != members_key
                 if rebuilt:
                     tb = now()
-                    if batch is not None:
-                        batch.close()
-                    batch = GpuBatch([r.sim for r in active])
+                    if batch is None:
+                        batch = GpuBatch([r.sim for r in active])
+                    else:
+                        batch.set_members([r.sim for r in active])
                     members_key = key
                     if self.autotune:
                         self._shape(batch)
@@ -187,12 +192,18 @@ class Server:
                     else:
                         still.append(r)
                 if len(still) != len(active):
-                    # the members leave the batch before their contexts are freed
-                    batch.close()
-                    batch = None
-                    members_key = None
+                    # the finished members leave the batch before their contexts are freed
+                    if still:
+                        batch.set_members([r.sim for r in still])
+                        members_key = tuple(r.rid for r in still)
+                    else:
+                        self.graph_updates += batch.graph_updates()
+                        batch.close()
+                        batch = None
+                        members_key = None
                 active = still
             if batch is not None:
+                self.graph_updates += batch.graph_updates()
                 batch.close()
             for f in finishing:
                 f.result()
@@ -260,6 +271,7 @@ class Server:
             "mean_members": float(np.mean(self.tick_members)) if self.tick_members else 0.0,
             "peak_bytes": self.peak_bytes,
             "host_s": dict(self.host_s),
+            "graph_updates": self.graph_updates,
             "budget_bytes": self.budget,
             "tile_threads": {"/".join(str(int(v)) for v in k): sh for k, sh in self.shapes.items()},
         }

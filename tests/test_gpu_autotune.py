@@ -157,3 +157,37 @@ def test_batch_groups_start_with_their_first_members_shapes():
     batch.close()
     for g in sims:
         g.close()
+
+
+@pytest.mark.parametrize("prec", [PREC_FP64, PREC_MIXED])
+def test_tuned_shapes_are_not_slower_than_the_defaults(prec):
+    """On the 1M-particle 3D collapse after 20 steps, the shapes mtr_autotune
+    picks (3 interleaved repetitions, median, noise margin) against the
+    default shapes on the same scene: both timed interleaved, 5 rounds of 4
+    profiled steps each (CUDA events per kernel), the median over rounds of
+    the tile kernels' summed time.  A 3% allowance covers timing noise."""
+    import copy
+    from matter_tests_b200 import scenes
+    from matter_tests_b200.gpu import GpuSim
+    sc = scenes.collapse3d_mui(scale=1.0)
+    p = copy.copy(sc.params)
+    p.precision = prec
+    g = GpuSim(p)
+    g.upload(sc.x, sc.v, sc.F, sc.B, sc.scalars)
+    g.set_objects(sc.plates, sc.objects)
+    g.step(20)
+    default = (g.tile_threads, g.tile_lanes)
+    g.autotune(3)
+    tuned = (g.tile_threads, g.tile_lanes)
+    kernels = ("k_p2g", "k_g2p_musl", "k_defgrad")
+    times = {"default": [], "tuned": []}
+    for _ in range(5):
+        for name, (tt, ln) in (("default", default), ("tuned", tuned)):
+            g.tile_threads = tt
+            g.tile_lanes = ln
+            g.profile(1)
+            times[name].append(sum(t for k, t in g.profile(4) if k in kernels))
+    g.close()
+    med = {k: float(np.median(v)) for k, v in times.items()}
+    print(prec, default, tuned, med)
+    assert med["tuned"] <= 1.03 * med["default"], (tuned, med)

@@ -180,3 +180,36 @@ def test_batch_clocks_match_each_members_clock():
     batch.close()
     for g in sims:
         g.close()
+
+
+def test_members_join_and_leave_one_batch():
+    """mtr_batch_set_members: one batch whose members change between calls
+    (scenes join after others have stepped, leave and continue alone), each
+    scene ending exactly as when stepped alone for the same number of steps;
+    membership changes within the same groups update the step graph in place."""
+    from matter_tests_b200.gpu import GpuBatch
+    scs = scene_set()
+    # a second scene of scene 1's group (3D, quadratic, FP64, USL, Drucker-Prager)
+    scs.append(cases.apply(cases.block(3, 2, n=5, seed=21), plastic_model=cases.PM.DP, M=0.6, flip_ratio=-2.0))
+    sims = [make_sim(sc) for sc in scs]
+    # scene i steps: in the batch for the calls it is a member of, then alone to 36;
+    # the first two changes keep the same groups (1 <-> 5, then both)
+    plan = [(0, 1, 2), (0, 5, 2), (0, 1, 2, 5), (1, 2, 3, 4, 5), (3, 4), (0, 1, 2, 3, 4, 5)]
+    b = GpuBatch([sims[i] for i in plan[0]])
+    done = [0] * len(scs)
+    for members in plan:
+        b.set_members([sims[i] for i in members])
+        b.step(6)
+        for i in members:
+            done[i] += 6
+    updates = b.graph_updates()
+    b.close()
+    for i, g in enumerate(sims):
+        g.step(36 - done[i])
+    for i, sc in enumerate(scs):
+        alone = make_sim(sc)
+        alone.step(36)
+        assert_same(state(sims[i]), state(alone), sc.params.precision)
+        alone.close()
+        sims[i].close()
+    assert updates >= 2, updates
