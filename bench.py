@@ -197,7 +197,7 @@ def measured_traffic(workload, scale, kernel, precision):
     for e in tab.get("captures", []):
         if (e.get("workload") == workload and float(e.get("scale", 1.0)) == scale and e.get("kernel") == kernel
                 and e.get("precision") == precision):
-            if e.get("source_hash") != kernel_source_hash():
+            if e.get("source_hash", tab.get("source_hash")) != kernel_source_hash():
                 return None, "capture predates the current kernel sources"
             return float(e["dram_bytes_per_launch"]), "ncu capture (profiles/dram_traffic.json): " + e.get("note", "")
     return None, "no capture of this kernel"

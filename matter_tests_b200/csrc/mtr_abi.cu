@@ -107,7 +107,7 @@ enum { kSlotP2G = 0, kSlotMUSL = 1, kSlotG2P = 2, kSlotDefgrad = 3, kTileSlots =
 // mark names that end each slot's kernel in a step
 const char* const kSlotMark[kTileSlots] = {"k_p2g", "k_g2p_musl", "k_g2p", "k_defgrad"};
 // largest block of each slot (k_g2p_t is register-bounded per 128 threads)
-const int kSlotMax[kTileSlots] = {kMaxTileThreads, kMaxTileThreads, kChunk, kMaxTileThreads};
+const int kSlotMax[kTileSlots] = {kMaxTileThreads, MTR_MUSL_MAX_THREADS, kChunk, kMaxTileThreads};
 const int kTileCandidates[3] = {64, 128, 256};
 
 bool valid_tile_threads(const int* t) {
@@ -317,16 +317,17 @@ void alloc_grid(mtr_ctx* c, const uint32_t want[3]) {
 
 void mark(mtr_ctx* c, const char* name) { c->marks.record(name, c->stream); }
 
+template <typename K>
+void scatter_attributes(K kernel, size_t smem) {
+  CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+}
+
 template <int D, int DEG, typename R>
 void set_kernel_attributes_t() {
-  CK(cudaFuncSetAttribute(k_p2g_w<D, DEG, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)p2g_smem_bytes<D, R>(kMaxTileThreads)));
-  CK(cudaFuncSetAttribute(k_p2g_w<D, DEG, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)p2g_smem_bytes<D, R>(kMaxTileThreads)));
-  CK(cudaFuncSetAttribute(k_g2p_musl_w<D, DEG, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)musl_smem_bytes<D, R>(kMaxTileThreads)));
-  CK(cudaFuncSetAttribute(k_g2p_musl_w<D, DEG, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)musl_smem_bytes<D, R>(kMaxTileThreads)));
+  scatter_attributes(k_p2g_w<D, DEG, R, 1>, p2g_smem_bytes<D, R>(kMaxTileThreads));
+  scatter_attributes(k_p2g_w<D, DEG, R, 2>, p2g_smem_bytes<D, R>(kMaxTileThreads));
+  scatter_attributes(k_g2p_musl_w<D, DEG, R, 1>, musl_smem_bytes<D, R>(MTR_MUSL_MAX_THREADS));
+  scatter_attributes(k_g2p_musl_w<D, DEG, R, 2>, musl_smem_bytes<D, R>(MTR_MUSL_MAX_THREADS));
 }
 
 void set_kernel_attributes(bool fp32) {
@@ -918,14 +919,10 @@ int enqueue_batch_step(mtr_batch* b) {
 
 template <int D, int DEG, typename R>
 void set_batch_attributes_t() {
-  CK(cudaFuncSetAttribute(kb_p2g_w<D, DEG, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)p2g_smem_bytes<D, R>(kMaxTileThreads)));
-  CK(cudaFuncSetAttribute(kb_p2g_w<D, DEG, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)p2g_smem_bytes<D, R>(kMaxTileThreads)));
-  CK(cudaFuncSetAttribute(kb_g2p_musl_w<D, DEG, R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)musl_smem_bytes<D, R>(kMaxTileThreads)));
-  CK(cudaFuncSetAttribute(kb_g2p_musl_w<D, DEG, R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)musl_smem_bytes<D, R>(kMaxTileThreads)));
+  scatter_attributes(kb_p2g_w<D, DEG, R, 1>, p2g_smem_bytes<D, R>(kMaxTileThreads));
+  scatter_attributes(kb_p2g_w<D, DEG, R, 2>, p2g_smem_bytes<D, R>(kMaxTileThreads));
+  scatter_attributes(kb_g2p_musl_w<D, DEG, R, 1>, musl_smem_bytes<D, R>(MTR_MUSL_MAX_THREADS));
+  scatter_attributes(kb_g2p_musl_w<D, DEG, R, 2>, musl_smem_bytes<D, R>(MTR_MUSL_MAX_THREADS));
 }
 
 void set_batch_attributes(const mtr_batch_group& g) {

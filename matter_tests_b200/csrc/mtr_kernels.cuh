@@ -773,8 +773,26 @@ __device__ __forceinline__ R stage_pd(const PStage<D, R>& S, const double (*crd)
 #ifndef MTR_SCATTER_PRESCALE
 #define MTR_SCATTER_PRESCALE 1
 #endif
+// With half chunks, every P2G thread takes part in staging: two threads per
+// staged particle (otherwise half the block waits at the barrier after the
+// staging, the kernel's top stall): FP64 P2G 0.369 -> 0.356 ms on the 1M
+// collapse and 0.473 -> 0.452 on the 1.2M incline, mixed 0.238 -> 0.232.
+#ifndef MTR_P2G_PAIR_STAGE
+#define MTR_P2G_PAIR_STAGE 1
+#endif
 #ifndef MTR_P2G_CHUNK_DIV
 #define MTR_P2G_CHUNK_DIV 2
+#endif
+// Largest block of the MUSL scatter and the resident blocks of that size its
+// register bound asks for.  Capped at 128 threads with five resident blocks
+// (at most 102 registers; the FP64 form had 124): FP64 MUSL 0.413 -> 0.399 ms,
+// mixed 0.297 -> 0.265 on the 1M collapse at step 300 (256-thread blocks,
+// which the bound rules out, never measured fastest for this kernel).
+#ifndef MTR_MUSL_MAX_THREADS
+#define MTR_MUSL_MAX_THREADS 128
+#endif
+#ifndef MTR_MUSL_MIN_BLOCKS
+#define MTR_MUSL_MIN_BLOCKS 5
 #endif
 #ifndef MTR_MUSL_CHUNK_DIV
 #define MTR_MUSL_CHUNK_DIV 1
@@ -852,7 +870,71 @@ __device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t
   const int chunk = (int)blockDim.x / MTR_P2G_CHUNK_DIV;
   const int kbeg = ((int)threadIdx.x / LPP) * PPG, kend = kbeg + PPG;
   for (uint32_t c0 = pb; c0 < pe; c0 += chunk) {
-    if ((int)threadIdx.x < chunk) {  // phase 1: stage one particle per thread
+    if constexpr (MTR_P2G_PAIR_STAGE && MTR_P2G_CHUNK_DIV == 2) {
+      // phase 1, two threads per staged particle: thread t < chunk loads the
+      // position, velocity and B and evaluates the weights; thread t + chunk
+      // loads the stress and mu(I) and evaluates the weight derivatives
+      const int role = (int)threadIdx.x >= chunk ? 1 : 0;
+      const int slot = (int)threadIdx.x - role * chunk;
+      const uint32_t s = c0 + (uint32_t)slot;
+      PStage<D, R>& S = st[slot];
+      int packed = -1;
+      if (s < pe) {
+        const uint32_t j = perm[s];
+        double xp[3] = {0.0, 0.0, 0.0};
+        int lb[3] = {0, 0, 0};
+        bool oob = false;
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+          xp[a] = A.in.x[(size_t)a * Np + j];
+          int b = (int)floor((xp[a] - H->org[a]) * ioh) - 1;
+          b = b < 0 ? 0 : b;  // p2g.cpp:21-24 clamps at zero
+          lb[a] = b - n0[a];
+          if (lb[a] < 0 || lb[a] > PN - 4 || b + 3 >= (int)H->N[a]) oob = true;
+        }
+        if (role == 0) {
+#pragma unroll
+          for (int a = 0; a < D; ++a) {
+            if constexpr (kFP64<R>) S.x[a] = xp[a];
+            S.v[a] = A.in.v[(size_t)a * Np + j];
+          }
+#pragma unroll
+          for (int q = 0; q < D * D; ++q)
+            S.B[q] = apic ? (MTR_SCATTER_PRESCALE ? apicD * A.in.B[(size_t)q * Np + j] : A.in.B[(size_t)q * Np + j])
+                          : R(0.0);
+          if (oob) {
+            raise_status(A.H, MTR_STATUS_STENCIL_OOB, A.in.id[j]);
+          } else {
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+#pragma unroll
+              for (int o = 0; o < 4; ++o) {
+                const double c = crd[a][lb[a] + o];
+                S.w[a * 4 + o] = bspline_N<DEG>((R)((xp[a] - c) * ioh));
+                if constexpr (!kFP64<R>) S.pd[a * 4 + o] = (R)(c - xp[a]);
+              }
+            }
+            packed = lb[0] | (lb[1] << 4) | (lb[2] << 8);
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < NS; ++q)
+            S.tau[q] = MTR_SCATTER_PRESCALE ? iohR * A.in.tau[(size_t)q * Np + j] : A.in.tau[(size_t)q * Np + j];
+          S.mui = mibf ? (R)((double)A.in.sc[(size_t)MTR_SCALAR_MUI * Np + j] - P.mui0) : R(0.0);
+          if (!oob) {
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+#pragma unroll
+              for (int o = 0; o < 4; ++o) {
+                const double c = crd[a][lb[a] + o];
+                S.dw[a * 4 + o] = bspline_dN<DEG>((R)((xp[a] - c) * ioh));
+              }
+            }
+          }
+        }
+      }
+      if (role == 0) S.lb = packed;
+    } else if ((int)threadIdx.x < chunk) {  // phase 1: stage one particle per thread
       const uint32_t s = c0 + threadIdx.x;
       PStage<D, R>& S = st[threadIdx.x];
       int packed = -1;
@@ -1786,7 +1868,8 @@ __device__ __forceinline__ void g2p_musl_w_body(const StepArgsT<R>& A, const uin
 }
 
 template <int D, int DEG, typename R, int XS = 1>
-__global__ void __launch_bounds__(kMaxTileThreads) k_g2p_musl_w(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
+__global__ void __launch_bounds__(MTR_MUSL_MAX_THREADS, MTR_MUSL_MIN_BLOCKS)
+    k_g2p_musl_w(StepArgsT<R> A, const uint32_t* __restrict__ perm) {
   g2p_musl_w_body<D, DEG, R, XS>(A, perm, blockIdx.x, gridDim.x);
 }
 
@@ -2050,7 +2133,7 @@ __global__ void __launch_bounds__(kChunk, MTR_G2P_MIN_BLOCKS) kb_g2p_t(BatchView
 }
 
 template <int D, int DEG, typename R, int XS = 1>
-__global__ void __launch_bounds__(kMaxTileThreads) kb_g2p_musl_w(BatchView<R> B) {
+__global__ void __launch_bounds__(MTR_MUSL_MAX_THREADS, MTR_MUSL_MIN_BLOCKS) kb_g2p_musl_w(BatchView<R> B) {
   batch_tiles(B, [&](const StepArgsT<R>& A, uint32_t b, uint32_t nb) {
     g2p_musl_w_body<D, DEG, R, XS>(A, A.perm, b, nb);
   });

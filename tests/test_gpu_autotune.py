@@ -19,8 +19,8 @@ pytestmark = [pytest.mark.gpu, needs_gpu]
 
 SHAPES = [
     {"p2g": 64, "musl": 64, "g2p": 64, "defgrad": 64},
-    {"p2g": 256, "musl": 256, "g2p": 128, "defgrad": 256},
-    {"p2g": 64, "musl": 256, "g2p": 96, "defgrad": 160},
+    {"p2g": 256, "musl": 128, "g2p": 128, "defgrad": 256},
+    {"p2g": 64, "musl": 96, "g2p": 96, "defgrad": 160},
 ]
 # x split of the scatters' stencil columns per shape: lanes per particle =
 # split x (16 in 3D, 4 in 2D)
@@ -100,7 +100,7 @@ def test_autotune_at_the_first_step_and_after_the_end():
 def test_invalid_shapes_are_refused():
     from matter_tests_b200.gpu import MtrFailure
     g = make_sim(scene_set()[1])
-    for bad in ({"p2g": 48}, {"p2g": 512}, {"g2p": 256}, {"defgrad": 0}):
+    for bad in ({"p2g": 48}, {"p2g": 512}, {"g2p": 256}, {"musl": 256}, {"defgrad": 0}):
         with pytest.raises(MtrFailure):
             g.tile_threads = bad
     assert g.tile_threads == {k: 128 for k in TILE_SLOTS}
