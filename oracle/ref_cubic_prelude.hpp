@@ -6,7 +6,7 @@
 // renamed out of the way, then supplies the cubic basis under the original
 // names.  The cubic formulas are the ones of tools.hpp:110-134 (the uniform
 // cubic B-spline and its derivative), evaluated in the same operation order so
-// that this build and the C restatement agree to the last bit.  apicDinverse
+// that the cubic reference build and the C restatement agree to the last bit.  apicDinverse
 // (simulation.cpp:94-96) is set to 3/dx^2 by ref_harness.cpp.
 #include <assert.h>
 
