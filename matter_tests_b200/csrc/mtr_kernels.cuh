@@ -703,7 +703,9 @@ constexpr int kMaxTileThreads = 256;
 // 3D collapse; three blocks measured best for k_g2p_t on the 3D Cam-Clay incline.
 // The FP32-storage form holds fewer live values and gains from a tighter bound:
 // six blocks of 128 threads (80 registers) measured 6% faster for its
-// k_defgrad_t on the 3D collapse than four, while the FP64 form lost 1%.
+// k_defgrad_t on the 3D collapse than four.  The FP64 form keeps four: six
+// measured 2% faster (0.295 -> 0.287 ms at step 300 of the 1M collapse) but
+// spilled to DRAM, writing 378 MB per launch instead of 150 MB (ncu).
 #ifndef MTR_DEFGRAD_MIN_BLOCKS
 #define MTR_DEFGRAD_MIN_BLOCKS 4
 #endif
@@ -1452,11 +1454,13 @@ __device__ __forceinline__ void load_velocity_patch(const StepCommon& A, const S
 // R.  pv holds node velocities minus vref: B-spline weights sum to one and
 // reproduce linears, so pic = vref + sum w dv, while B and grad v need the
 // deviations only.
+// The sums over the stencil's x layers ii0 .. ii1-1: ps = sum w v (deviations
+// from vref on the mixed path), B, flip and grad v (unscaled).
 template <int D, int DEG, bool GRADV, typename R>
-__device__ __forceinline__ void gather_patch(const R* pv, const R* pf, const double (*crd)[Tiling<D>::PN],
-                                             const int (&lb)[3], const double (&xp)[3], double ioh,
-                                             const double (&vref)[3], double (&pic)[3], R (&Bp)[D][D], R (&flp)[3],
-                                             R (&gv)[D][D], bool want_b, bool want_flip) {
+__device__ __forceinline__ void gather_sums(const R* pv, const R* pf, const double (*crd)[Tiling<D>::PN],
+                                            const int (&lb)[3], const double (&xp)[3], double ioh, R (&ps)[3],
+                                            R (&Bp)[D][D], R (&flp)[3], R (&gv)[D][D], bool want_b, bool want_flip,
+                                            int ii0, int ii1) {
   constexpr int PN = Tiling<D>::PN, NODES = Tiling<D>::NODES;
   R w[3][4], dw[3][4], pd[3][4];
 #pragma unroll
@@ -1469,7 +1473,6 @@ __device__ __forceinline__ void gather_patch(const R* pv, const R* pf, const dou
       dw[a][o] = GRADV ? bspline_dN<DEG>(u) : R(0.0);
       pd[a][o] = (R)(c - xp[a]);
     }
-  R ps[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) ps[a] = flp[a] = R(0.0);
 #pragma unroll
@@ -1481,7 +1484,7 @@ __device__ __forceinline__ void gather_patch(const R* pv, const R* pf, const dou
   // the return-mapping kernels that call this too large for the instruction
   // cache
 #pragma unroll 1
-  for (int ii = 0; ii < 4; ++ii)
+  for (int ii = ii0; ii < ii1; ++ii)
 #pragma unroll
     for (int jj = 0; jj < 4; ++jj) {
       const R wxy = w[0][ii] * w[1][jj];
@@ -1523,6 +1526,13 @@ __device__ __forceinline__ void gather_patch(const R* pv, const R* pf, const dou
         }
       }
     }
+}
+
+// pic = vref + ps (the FP64 path gathers the velocities themselves), grad v
+// scaled by 1/dx
+template <int D, bool GRADV, typename R>
+__device__ __forceinline__ void gather_finish(const R (&ps)[3], const double (&vref)[3], double ioh, double (&pic)[3],
+                                              R (&gv)[D][D]) {
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     if constexpr (kFP64<R>)
@@ -1537,6 +1547,16 @@ __device__ __forceinline__ void gather_patch(const R* pv, const R* pf, const dou
 #pragma unroll
       for (int c = 0; c < D; ++c) gv[r][c] *= iohR;
   }
+}
+
+template <int D, int DEG, bool GRADV, typename R>
+__device__ __forceinline__ void gather_patch(const R* pv, const R* pf, const double (*crd)[Tiling<D>::PN],
+                                             const int (&lb)[3], const double (&xp)[3], double ioh,
+                                             const double (&vref)[3], double (&pic)[3], R (&Bp)[D][D], R (&flp)[3],
+                                             R (&gv)[D][D], bool want_b, bool want_flip) {
+  R ps[3];
+  gather_sums<D, DEG, GRADV, R>(pv, pf, crd, lb, xp, ioh, ps, Bp, flp, gv, want_b, want_flip, 0, 4);
+  gather_finish<D, GRADV, R>(ps, vref, ioh, pic, gv);
 }
 
 // ---------------------------------------------------------------------------
@@ -1704,6 +1724,57 @@ __device__ __forceinline__ void g2p_musl_w_body(const StepArgsT<R>& A, const uin
   const int iy = D == 3 ? ((q % COLS) >> 2) : q % COLS;
   const int iz = D == 3 ? ((q % COLS) & 3) : 0;
   const int h0 = (q / COLS) * HN;
+  // a staged particle after its gather: velocity blend, position update,
+  // outputs and the re-scatter stencil; returns the packed stencil base
+  // (-1: none)
+  auto finish = [&](MStage<D, R>& S, uint32_t s, uint32_t pid, const double (&xp)[3], const double (&vp)[3],
+                    const double (&pic)[3], const R (&flp)[3], const R (&Bp)[D][D], bool ok) -> int {
+    int packed = -1;
+    double xn[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      const double vn = blend_v(fr, vp[a], (double)flp[a], pic[a]);
+      if constexpr (kFP64<R>) S.x[a] = xp[a];
+      S.v[a] = (R)vn;
+      xn[a] = xp[a] + dt * pic[a];  // positionUpdate: x + dt pic
+      A.out.v[(size_t)a * Np + s] = (R)vn;
+    }
+    wrap_and_teleport(P, xn);
+#pragma unroll
+    for (int a = 0; a < D; ++a) A.out.x[(size_t)a * Np + s] = xn[a];
+#pragma unroll
+    for (int r = 0; r < D; ++r)
+#pragma unroll
+      for (int c = 0; c < D; ++c) {
+        const R b = apic ? Bp[r][c] : R(0.0);
+        A.out.B[(size_t)(r * D + c) * Np + s] = b;
+        S.B[r * D + c] = MTR_SCATTER_PRESCALE ? apicD * b : b;
+      }
+    A.out.id[s] = pid;
+    if (P.store_pic_flip) {
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        A.pic[(size_t)a * Np + s] = (R)pic[a];
+        A.flip[(size_t)a * Np + s] = (fr >= -1) ? flp[a] : R(0.0);
+      }
+    }
+    // re-scatter stencil, base clamped at zero like P2G (musl.cpp:35-40)
+    int lbs[3];
+    if (ok && local_base<D>(H, xp, ioh, n0, true, lbs)) {
+#pragma unroll
+      for (int a = 0; a < D; ++a)
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+          const double c = crd[a][lbs[a] + o];
+          S.w[a * 4 + o] = bspline_N<DEG>((R)((xp[a] - c) * ioh));
+          if constexpr (!kFP64<R>) S.pd[a * 4 + o] = (R)(c - xp[a]);
+        }
+      packed = lbs[0] | (lbs[1] << 4) | (lbs[2] << 8);
+    } else if (ok) {
+      raise_status(H, MTR_STATUS_STENCIL_OOB, pid);
+    }
+    return packed;
+  };
   // consecutive particles per lane group, as in k_p2g_w
   static_assert(LPP % MTR_MUSL_CHUNK_DIV == 0, "chunk divisor must divide the lanes per particle");
   constexpr int PPG = LPP / MTR_MUSL_CHUNK_DIV;
@@ -1742,49 +1813,7 @@ __device__ __forceinline__ void g2p_musl_w_body(const StepArgsT<R>& A, const uin
 #pragma unroll
             for (int c = 0; c < D; ++c) Bp[r][c] = R(0.0);
         }
-        double xn[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-        for (int a = 0; a < D; ++a) {
-          const double vn = blend_v(fr, vp[a], (double)flp[a], pic[a]);
-          if constexpr (kFP64<R>) S.x[a] = xp[a];
-          S.v[a] = (R)vn;
-          xn[a] = xp[a] + dt * pic[a];  // positionUpdate: x + dt pic
-          A.out.v[(size_t)a * Np + s] = (R)vn;
-        }
-        wrap_and_teleport(P, xn);
-#pragma unroll
-        for (int a = 0; a < D; ++a) A.out.x[(size_t)a * Np + s] = xn[a];
-#pragma unroll
-        for (int r = 0; r < D; ++r)
-#pragma unroll
-          for (int c = 0; c < D; ++c) {
-            const R b = apic ? Bp[r][c] : R(0.0);
-            A.out.B[(size_t)(r * D + c) * Np + s] = b;
-            S.B[r * D + c] = MTR_SCATTER_PRESCALE ? apicD * b : b;
-          }
-        A.out.id[s] = pid;
-        if (P.store_pic_flip) {
-#pragma unroll
-          for (int a = 0; a < D; ++a) {
-            A.pic[(size_t)a * Np + s] = (R)pic[a];
-            A.flip[(size_t)a * Np + s] = (fr >= -1) ? flp[a] : R(0.0);
-          }
-        }
-        // re-scatter stencil, base clamped at zero like P2G (musl.cpp:35-40)
-        int lbs[3];
-        if (ok && local_base<D>(H, xp, ioh, n0, true, lbs)) {
-#pragma unroll
-          for (int a = 0; a < D; ++a)
-#pragma unroll
-            for (int o = 0; o < 4; ++o) {
-              const double c = crd[a][lbs[a] + o];
-              S.w[a * 4 + o] = bspline_N<DEG>((R)((xp[a] - c) * ioh));
-              if constexpr (!kFP64<R>) S.pd[a * 4 + o] = (R)(c - xp[a]);
-            }
-          packed = lbs[0] | (lbs[1] << 4) | (lbs[2] << 8);
-        } else if (ok) {
-          raise_status(H, MTR_STATUS_STENCIL_OOB, pid);
-        }
+        packed = finish(S, s, pid, xp, vp, pic, flp, Bp, ok);
       }
       S.lb = packed;
     }
