@@ -171,8 +171,9 @@ class ClockSampler:
 
 # DRAM bytes (read + write) per launch of the dominant kernels, from ncu
 # captures (dram__bytes_read.sum + dram__bytes_write.sum), stored with the
-# hash of the kernel sources they were captured on; a figure whose hash does
-# not match the sources being run is reported as stale (traffic null).
+# hash of the device code they were captured on (the .cuh files of csrc,
+# which hold every step kernel); a figure whose hash does not match the code
+# being run is reported as stale (traffic null).
 TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dram_traffic.json")
 
 
@@ -181,7 +182,7 @@ def kernel_source_hash():
     h = hashlib.sha256()
     csrc = os.path.join(ROOT, "matter_tests_b200", "csrc")
     for f in sorted(os.listdir(csrc)):
-        if f.endswith((".cu", ".cuh")):
+        if f.endswith(".cuh"):
             with open(os.path.join(csrc, f), "rb") as fh:
                 h.update(f.encode() + b"\0" + fh.read())
     return h.hexdigest()[:16]
@@ -602,9 +603,11 @@ def ensemble_measure(args, local):
     default = [(gr["tile_threads"], gr["tile_lanes"]) for gr in batch.groups()]
     if not args.no_autotune:
         batch.autotune(args.tune_reps)  # setup, untimed: trial steps leave the scenes as they are
-    groups = batch.groups()
+        batch.set_retune(args.tune_reps)  # and again inside the timed steps when a group's grids double
     ms = timed(batch, K)
     launches = batch.launch_count()
+    retunes = batch.retunes()  # re-tunes inside the timed steps (a group's grids doubled)
+    groups = batch.groups()    # the shapes after the timed steps
     # tuned against default shapes on the same batch, interleaved in rounds of
     # 16 steps so that both see the same states; after each switch 8 untimed
     # steps rebuild the batch's graph outside the timed window
@@ -656,7 +659,7 @@ def ensemble_measure(args, local):
             "serial": {"value": serial, "ms_total": serial_ms,
                        "timed": "each scene alone through its own context and graphs, CUDA events"},
             "batched_over_serial": value / serial, "gpu_launches": launches, "dtype": "f32+f64",
-            "groups": groups, "shapes_ab": ab,
+            "groups": groups, "retunes": retunes, "shapes_ab": ab,
             "config": "seeded DP column collapses: Np log-uniform 5k-300k, P(3D) 0.5, aspect U(0.5,4), "
                       "friction angle U(20,40) deg, E log-uniform 1e5-1e7 Pa, APIC USL, quadratic",
             "all_scenes_advanced": bool(min(steps_done) >= W + K)}

@@ -354,6 +354,16 @@ int mtr_set_tile_lanes(mtr_ctx* ctx, const int* lanes /* [2] */);
 int mtr_get_tile_lanes(mtr_ctx* ctx, int* lanes /* [2] */);
 int mtr_batch_set_tile_lanes(mtr_batch* batch, int group, const int* lanes /* [2] */);
 int mtr_batch_autotune(mtr_batch* batch, int reps);
+/* Re-tuning as scenes spread: with reps > 0, mtr_batch_step tunes the batch
+ * again (mtr_batch_autotune with reps repetitions, inside the call) when a
+ * group's members together hold more than twice the grid nodes they held at
+ * the last tune; reps = 0 (the default) turns it off.  A membership change
+ * (mtr_batch_set_members) takes the next step's grid size as the new
+ * baseline.  A re-tune costs about as many batched steps as a tune, so a
+ * latency-bound caller (a serving loop with cached shapes) leaves it off.
+ * mtr_batch_retunes counts the re-tunes so far. */
+int mtr_batch_set_retune(mtr_batch* batch, int reps);
+int mtr_batch_retunes(mtr_batch* batch);
 /* The clocks of the members (in mtr_batch_create order) as of the end of the
  * last mtr_batch_step, without a device round trip; returns the member count. */
 int mtr_batch_clocks(mtr_batch* batch, mtr_clock* clocks, int n);

@@ -764,6 +764,7 @@ struct mtr_batch_group {
   uint32_t total[kBK_KINDS] = {};
   int tile_threads[kTileSlots] = {kChunk, kChunk, kChunk, kChunk};
   int tile_split[kScatterSlots] = {1, 1};
+  uint64_t tuned_nodes = 0;  // members' grid nodes at the last tune (0: take the next step's as the baseline)
 };
 
 struct mtr_batch {
@@ -780,6 +781,12 @@ struct mtr_batch {
   // host-side bookkeeping of mtr_batch_step (mtr_batch_stats)
   int64_t regrowths = 0, rebuilds = 0;
   int64_t updates = 0;  // rebuilds that updated the instantiated graph in place
+  // > 0 after mtr_batch_set_retune: mtr_batch_step re-tunes with this many
+  // repetitions when a group's grids have grown past twice their size at the
+  // last tune (the tuned shapes fit the state they were tuned on; spreading
+  // scenes move the optimum)
+  int retune_reps = 0;
+  int64_t retunes = 0;
   double regrow_ms = 0.0, rebuild_ms = 0.0;
 };
 
@@ -1958,7 +1965,10 @@ void assign_members(mtr_batch* b, mtr_ctx* const* ctxs, int n) {
   if (!b->members.empty() && ctxs[0]->device != b->device)
     throw MtrError{MTR_ERR_INVALID, "members must share the batch's device"};
   b->members.clear();
-  for (auto& g : b->groups) g.members.clear();
+  for (auto& g : b->groups) {
+    g.members.clear();
+    g.tuned_nodes = 0;  // a new membership: its grid size is the next baseline
+  }
   for (int i = 0; i < n; ++i) {
     mtr_ctx* c = ctxs[i];
     CK(cudaStreamSynchronize(c->stream));  // nothing of the member may still run on its own stream
@@ -2087,6 +2097,24 @@ int mtr_batch_step(mtr_batch* b, int nsteps) {
       } else if (steps_after == steps_before) {
         break;  // no member can advance (ended, or held by a frame stop)
       }
+      // Re-tuning (mtr_batch_set_retune) is checked after regrowths too: a
+      // spreading scene regrows at most checks, and its grid doubles at one.
+      if (b->retune_reps > 0) {
+        bool retune = false;
+        for (auto& g : b->groups) {
+          uint64_t nodes = 0;
+          for (mtr_ctx* c : g.members) nodes += c->hH->G;
+          if (g.tuned_nodes == 0)
+            g.tuned_nodes = nodes;
+          else if (nodes > 2 * g.tuned_nodes)
+            retune = true;
+        }
+        if (retune) {
+          const int rc = mtr_batch_autotune(b, b->retune_reps);
+          if (rc != MTR_OK) throw MtrError{rc, std::string("re-tuning the batch: ") + mtr_last_error()};
+          b->retunes += 1;
+        }
+      }
     }
     for (mtr_ctx* c : b->members) {
       c->hH->stop_step = c->step_limit;
@@ -2192,6 +2220,12 @@ int mtr_batch_autotune(mtr_batch* b, int reps) {
         }
       }
       if (!ready) throw MtrError{MTR_ERR_STATE, "grid kept growing during tuning"};
+      // the grid sizes the shapes are tuned on (the trial step computed them)
+      for (auto& g : b->groups) {
+        uint64_t nodes = 0;
+        for (mtr_ctx* c : g.members) nodes += c->hH->G;
+        g.tuned_nodes = nodes;
+      }
       std::vector<TuneTimes> tt(b->groups.size());
       std::vector<std::vector<int>> chosen, chosen_split;
       for (auto& g : b->groups) {
@@ -2223,6 +2257,14 @@ int mtr_batch_autotune(mtr_batch* b, int reps) {
     return MTR_OK;
   });
 }
+
+int mtr_batch_set_retune(mtr_batch* b, int reps) {
+  if (!b || reps < 0) return MTR_ERR_INVALID;
+  b->retune_reps = reps;
+  return MTR_OK;
+}
+
+int mtr_batch_retunes(mtr_batch* b) { return b ? (int)std::min<int64_t>(b->retunes, 0x7fffffff) : MTR_ERR_INVALID; }
 
 int64_t mtr_batch_launch_count(mtr_batch* b) { return b ? b->launches_last : 0; }
 

@@ -29,7 +29,7 @@ EXPORTS = (
     "mtr_batch_get_group", "mtr_batch_set_tile_threads", "mtr_frame_columns", "mtr_frame_begin",
     "mtr_frame_wait", "mtr_get_grid_friction", "mtr_set_levelset", "mtr_set_tile_lanes", "mtr_get_tile_lanes",
     "mtr_batch_set_tile_lanes", "mtr_batch_clocks", "mtr_batch_stats", "mtr_batch_set_members",
-    "mtr_batch_graph_updates",
+    "mtr_batch_graph_updates", "mtr_batch_set_retune", "mtr_batch_retunes",
 )
 
 _lib = None
@@ -77,6 +77,8 @@ def load_library(path=LIB_PATH):
     lib.mtr_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]
     lib.mtr_batch_set_members.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_int]
     lib.mtr_batch_graph_updates.argtypes = [C.c_void_p]
+    lib.mtr_batch_set_retune.argtypes = [C.c_void_p, C.c_int]
+    lib.mtr_batch_retunes.argtypes = [C.c_void_p]
     lib.mtr_batch_step.argtypes = [C.c_void_p, C.c_int]
     lib.mtr_batch_launch_count.argtypes = [C.c_void_p]
     lib.mtr_batch_launch_count.restype = C.c_int64
@@ -396,6 +398,15 @@ class GpuBatch:
     def graph_updates(self):
         """Rebuilds that updated the instantiated step graph in place."""
         return self.lib.mtr_batch_graph_updates(self.h)
+
+    def set_retune(self, reps):
+        """With reps > 0, step() tunes the batch again (reps repetitions) when a
+        group's grids have doubled since its last tune; 0 turns it off."""
+        _check(self.lib, "mtr_batch_set_retune", self.lib.mtr_batch_set_retune(self.h, int(reps)))
+
+    def retunes(self):
+        """Re-tunes step() ran because a group's grid had doubled since its last tune."""
+        return self.lib.mtr_batch_retunes(self.h)
 
     @property
     def stream(self):

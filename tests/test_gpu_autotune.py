@@ -191,3 +191,43 @@ def test_tuned_shapes_are_not_slower_than_the_defaults(prec):
     med = {k: float(np.median(v)) for k, v in times.items()}
     print(prec, default, tuned, med)
     assert med["tuned"] <= 1.03 * med["default"], (tuned, med)
+
+
+def test_batch_retunes_when_its_grids_double():
+    """With re-tuning on (mtr_batch_set_retune), a batch whose scenes fly
+    apart (their grids grow past twice their size at the tune) is tuned again
+    inside mtr_batch_step; the re-tunes, like the first tune, leave every
+    scene as it is when stepped alone.  Without it the same batch is tuned
+    only once."""
+    import cases
+    from matter_tests_b200.gpu import GpuBatch
+    scs = []
+    for seed in (3, 5):
+        # a soft block bursting outwards: its grid grows from ~2.5k nodes to
+        # ~50k over 48 steps (the oracle's remesh), four doublings
+        sc = cases.apply(cases.block(3, 2, n=4, seed=seed, E=1e3), plastic_model=cases.PM.NoPlasticity)
+        d = sc.x - sc.x.mean(0)
+        sc.v = 4.0 * d / np.linalg.norm(d, axis=1, keepdims=True)
+        scs.append(sc)
+    off = [make_sim(sc) for sc in scs]
+    b = GpuBatch(off)
+    b.autotune(1)
+    b.step(48)
+    assert b.retunes() == 0
+    b.close()
+    for g in off:
+        g.close()
+    sims = [make_sim(sc) for sc in scs]
+    b = GpuBatch(sims)
+    b.autotune(1)
+    b.set_retune(1)
+    b.step(48)
+    n = b.retunes()
+    b.close()
+    assert n >= 1, n
+    for sc, g in zip(scs, sims):
+        alone = make_sim(sc)
+        alone.step(48)
+        assert_same(state(g), state(alone), sc.params.precision)
+        alone.close()
+        g.close()
