@@ -669,7 +669,9 @@ def serve_measure(args, local):
     """The serving loop: args.serve_requests seeded requests (2D/3D, collapse
     or incline, 10k-2M particles, DP / Cam-Clay / mu(I), 200 steps each)
     arriving as a Poisson process at 20 per second, admitted within a 150 GB
-    device-memory budget, mixed precision, stepped together in ticks of 8.
+    device-memory budget, mixed precision, stepped together in ticks of up to
+    8 steps sized to a 16 ms frame interval; and the same requests again in
+    ticks of 8 steps each (`fixed_ticks`).
     Against it: the same requests one after another through the plain FP64
     single-scene path and the mixed single-scene path (device-timed steps)."""
     import copy
@@ -682,18 +684,26 @@ def serve_measure(args, local):
     # start-up, untimed: one 200k-particle request of every kind (dimension x
     # collapse or incline x material) through a warm-up server loads the
     # batched kernels of every group the measured run will meet and tunes
-    # their shapes; the measured server starts from those shapes
+    # their shapes (the measured server starts from those shapes); two 2M
+    # requests besides them take the device allocations up to the largest
+    # request's size once
     rng = np.random.default_rng(1)
-    warm = [Request(rid=i, scene=scenes.granular_scene(rng, dim, kind, 200_000, mat, 1e6, 30.0, 2.0), steps=16,
+    kinds = [(d, k, m, 200_000) for d in (2, 3) for k in ("collapse", "incline") for m in ("dp", "mcc", "mui")]
+    kinds += [(3, "collapse", "dp", 2_000_000)] * 2
+    warm = [Request(rid=i, scene=scenes.granular_scene(rng, dim, kind, n, mat, 1e6, 30.0, 2.0), steps=16,
                     arrival=0.0)
-            for i, (dim, kind, mat) in enumerate((d, k, m) for d in (2, 3) for k in ("collapse", "incline")
-                                                 for m in ("dp", "mcc", "mui"))]
+            for i, (dim, kind, mat, n) in enumerate(kinds)]
     warm_srv = Server(budget_bytes=150e9, device=local, tick_steps=8, precision=PREC_MIXED)
     warm_srv.run(warm, realtime=False)
     reqs = poisson_requests(args.serve_requests, rate=20.0, seed=4242, steps=200)
-    srv = Server(budget_bytes=150e9, device=local, tick_steps=8, precision=PREC_MIXED, shapes=warm_srv.shapes)
+    # the measured run: ticks sized to a 16 ms frame interval (1-8 steps)
+    srv = Server(budget_bytes=150e9, device=local, tick_steps=8, precision=PREC_MIXED, shapes=warm_srv.shapes,
+                 frame_ms=16.0)
     done = srv.run(reqs)
     rep = srv.report(done)
+    # beside it, the same requests with every tick 8 steps (no frame interval)
+    fixed_srv = Server(budget_bytes=150e9, device=local, tick_steps=8, precision=PREC_MIXED, shapes=warm_srv.shapes)
+    fixed = fixed_srv.report(fixed_srv.run(poisson_requests(args.serve_requests, rate=20.0, seed=4242, steps=200)))
     serial = {}
     for prec, name in ((PREC_FP64, "fp64"), (PREC_MIXED, "mixed")):
         ms, ps = 0.0, 0
@@ -718,8 +728,12 @@ def serve_measure(args, local):
                 "single_scene_fp64": serial["fp64"], "single_scene_mixed": serial["mixed"],
                 "served_over_single_scene_fp64": rep["throughput"] / serial["fp64"],
                 "served_over_single_scene_mixed": rep["throughput"] / serial["mixed"],
+                "fixed_ticks": {"throughput": fixed["throughput"],
+                                "served_over_single_scene_mixed": fixed["throughput"] / serial["mixed"],
+                                "frame_latency_ms": fixed["frame_latency_ms"], "ticks": fixed["ticks"]},
                 "config": "Poisson arrivals 20/s (seed 4242), Np log-uniform 10k-2M, 2D/3D collapse or incline, "
-                          "DP/MCC/mu(I), 200 steps, 150 GB budget, ticks of 8 steps",
+                          "DP/MCC/mu(I), 200 steps, 150 GB budget, ticks of up to 8 steps sized to a 16 ms "
+                          "frame interval (fixed_ticks: every tick 8 steps)",
                 "timed": "throughput = particle-steps of the served requests / (last completion - first "
                          "arrival), wall clock; single-scene figures are device time of the steps alone"})
     return rep

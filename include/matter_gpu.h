@@ -157,8 +157,13 @@ int mtr_ctx_create(const mtr_params* params, int device, mtr_ctx** out);
 
 /* Copies the particle state in (replaces the host-side Particles arrays the
  * reference mutates in place, data_structures.hpp:8-47).  Any of v, F, B,
- * scalars may be NULL (zero velocity, identity F, zero B, zero scalars).  With
- * use_mibf the muI slot is initialised as simulate() does (simulation.cpp:138-145). */
+ * scalars may be NULL (zero velocity, identity F, zero B, zero scalars; filled
+ * on the device, nothing is copied for them).  With use_mibf the muI slot is
+ * initialised as simulate() does (simulation.cpp:138-145).  Pinned host arrays
+ * are copied directly; pageable ones through two pinned 8 MB staging chunks
+ * per device, so that a long copy leaves the driver and the copy engine free
+ * between chunks for other threads' work (a batch stepping beside it).
+ * mtr_download copies back the same way. */
 int mtr_upload(mtr_ctx* ctx, const double* x, const double* v, const double* F, const double* B,
                const double* scalars, uint32_t Np);
 

@@ -240,6 +240,94 @@ cudaMemPool_t grid_pool(int device) {
   return g_grid_pool[device];
 }
 
+// Host copies of particle arrays.  A copy to or from pageable host memory
+// (a numpy array, a std::vector) goes through two pinned chunks per device,
+// alternately: the host copies one chunk while the DMA of the other runs.  A
+// plain pageable cudaMemcpy of a few hundred MB, issued by a serving loop's
+// worker thread, held up the batch's own launches and header copies on the
+// main thread for its whole duration (ticks of 1 step took as long as the
+// upload beside them); in chunks, the driver and the copy engine are free
+// between chunks.  Pinned host memory (cudaMallocHost, registered) is copied
+// directly.
+constexpr size_t kStageChunk = 8u << 20;
+struct HostStage {
+  std::mutex m;
+  char* buf[2] = {nullptr, nullptr};
+  cudaEvent_t done[2] = {nullptr, nullptr};
+};
+HostStage g_stage[64];
+
+bool is_pinned(const void* p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
+
+HostStage& host_stage(int device) {
+  if (device < 0 || device >= 64) throw MtrError{MTR_ERR_INVALID, "device index out of range"};
+  HostStage& S = g_stage[device];
+  if (!S.buf[0]) {  // called with S.m held
+    for (int i = 0; i < 2; ++i) {
+      if (cudaMallocHost((void**)&S.buf[i], kStageChunk) != cudaSuccess) {
+        (void)cudaGetLastError();
+        throw MtrError{MTR_ERR_OOM, "cudaMallocHost (copy staging)"};
+      }
+      CK(cudaEventCreateWithFlags(&S.done[i], cudaEventDisableTiming));
+    }
+  }
+  return S;
+}
+
+// bytes host -> device on the context's stream; returns when the copy is done
+void copy_to_device(mtr_ctx* c, void* dst, const void* host, size_t bytes) {
+  if (is_pinned(host)) {
+    CK(cudaMemcpyAsync(dst, host, bytes, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return;
+  }
+  HostStage& S = g_stage[c->device < 64 && c->device >= 0 ? c->device : 0];
+  std::lock_guard<std::mutex> lock(S.m);
+  host_stage(c->device);
+  int k = 0;
+  for (size_t off = 0; off < bytes; off += kStageChunk, k ^= 1) {
+    const size_t n = std::min(kStageChunk, bytes - off);
+    CK(cudaEventSynchronize(S.done[k]));  // the chunk's previous DMA has finished
+    std::memcpy(S.buf[k], (const char*)host + off, n);
+    CK(cudaMemcpyAsync((char*)dst + off, S.buf[k], n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaEventRecord(S.done[k], c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+}
+
+// bytes device -> host on the context's stream (work already queued on it
+// comes first); returns when the data is in host memory
+void copy_to_host(mtr_ctx* c, void* host, const void* src, size_t bytes) {
+  if (is_pinned(host)) {
+    CK(cudaMemcpyAsync(host, src, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return;
+  }
+  HostStage& S = g_stage[c->device < 64 && c->device >= 0 ? c->device : 0];
+  std::lock_guard<std::mutex> lock(S.m);
+  host_stage(c->device);
+  const size_t nchunks = (bytes + kStageChunk - 1) / kStageChunk;
+  auto issue = [&](size_t j) {
+    const size_t off = j * kStageChunk, n = std::min(kStageChunk, bytes - off);
+    CK(cudaMemcpyAsync(S.buf[j & 1], (const char*)src + off, n, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaEventRecord(S.done[j & 1], c->stream));
+  };
+  if (nchunks > 0) issue(0);
+  for (size_t j = 0; j < nchunks; ++j) {
+    if (j + 1 < nchunks) issue(j + 1);  // the next chunk's DMA runs while this one is copied out
+    CK(cudaEventSynchronize(S.done[j & 1]));
+    const size_t off = j * kStageChunk, n = std::min(kStageChunk, bytes - off);
+    std::memcpy((char*)host + off, S.buf[j & 1], n);
+  }
+}
+
 // n elements of T from the grid pool, ordered on the context's stream
 template <typename T>
 T* galloc(mtr_ctx* c, size_t n) {
@@ -435,7 +523,6 @@ int enqueue_step_t(mtr_ctx* c, int parity) {
   cudaStream_t st = c->stream;
   StepArgsT<R> A = make_args<R>(c, parity);
   int n = 0;
-  const uint32_t pblocks = (c->Np + 127) / 128;
   mark(c, "start");
   k_bbox<D, R><<<c->npartials, 256, 0, st>>>(A);
   ++n;
@@ -731,8 +818,7 @@ void get_soa(mtr_ctx* c, double* host, const void* src, const uint32_t* id, int 
       k_soa_to_aos<2, float><<<blocks, 256, 0, c->stream>>>(Np, (const float*)src, id, c->staging, kind);
   }
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(host, c->staging, sizeof(double) * Np * width, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  copy_to_host(c, host, c->staging, sizeof(double) * Np * width);
 }
 
 // n node values of the context's storage type -> FP64 host array
@@ -1190,42 +1276,36 @@ int mtr_upload(mtr_ctx* c, const double* x, const double* v, const double* F, co
     c->uploads_reused += reuse ? 1 : 0;
     // state -> buffer 0 (AoS host layout -> SoA)
     const uint32_t blocks = (Np + 255) / 256;
-    auto put = [&](const double* host, void* dst, int width, int kind, const double* fill) {
+    // an absent array is filled on the device (zeros, or identity with eye)
+    auto put = [&](const double* host, void* dst, int width, int kind, bool eye) {
+      const double* src = nullptr;
       if (host) {
-        CK(cudaMemcpyAsync(c->staging, host, sizeof(double) * Np * width, cudaMemcpyHostToDevice, c->stream));
-      } else {
-        std::vector<double> tmp((size_t)Np * width, 0.0);
-        if (fill)
-          for (uint32_t p = 0; p < Np; ++p)
-            for (int i = 0; i < width; ++i) tmp[(size_t)p * width + i] = fill[i];
-        CK(cudaMemcpyAsync(c->staging, tmp.data(), sizeof(double) * tmp.size(), cudaMemcpyHostToDevice, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
+        copy_to_device(c, c->staging, host, sizeof(double) * Np * width);
+        src = c->staging;
       }
       if (kind == 0 && dst == c->buf[0].x) {  // positions stay FP64
         if (d == 3)
-          k_aos_to_soa<3, double><<<blocks, 256, 0, c->stream>>>(Np, c->staging, (double*)dst, kind);
+          k_aos_to_soa<3, double><<<blocks, 256, 0, c->stream>>>(Np, src, (double*)dst, kind, eye);
         else
-          k_aos_to_soa<2, double><<<blocks, 256, 0, c->stream>>>(Np, c->staging, (double*)dst, kind);
+          k_aos_to_soa<2, double><<<blocks, 256, 0, c->stream>>>(Np, src, (double*)dst, kind, eye);
       } else if (c->fp32) {
         if (d == 3)
-          k_aos_to_soa<3, float><<<blocks, 256, 0, c->stream>>>(Np, c->staging, (float*)dst, kind);
+          k_aos_to_soa<3, float><<<blocks, 256, 0, c->stream>>>(Np, src, (float*)dst, kind, eye);
         else
-          k_aos_to_soa<2, float><<<blocks, 256, 0, c->stream>>>(Np, c->staging, (float*)dst, kind);
+          k_aos_to_soa<2, float><<<blocks, 256, 0, c->stream>>>(Np, src, (float*)dst, kind, eye);
       } else {
         if (d == 3)
-          k_aos_to_soa<3, double><<<blocks, 256, 0, c->stream>>>(Np, c->staging, (double*)dst, kind);
+          k_aos_to_soa<3, double><<<blocks, 256, 0, c->stream>>>(Np, src, (double*)dst, kind, eye);
         else
-          k_aos_to_soa<2, double><<<blocks, 256, 0, c->stream>>>(Np, c->staging, (double*)dst, kind);
+          k_aos_to_soa<2, double><<<blocks, 256, 0, c->stream>>>(Np, src, (double*)dst, kind, eye);
       }
       CK(cudaGetLastError());
       CK(cudaStreamSynchronize(c->stream));
     };
-    double eye[9] = {0};
-    for (int i = 0; i < d; ++i) eye[i * d + i] = 1.0;
-    put(x, c->buf[0].x, d, 0, nullptr);
-    put(v, c->buf[0].v, d, 0, nullptr);
-    put(F, c->buf[0].F, dd, c->fp32 ? 3 : 1, eye);  // FP32 keeps F - I
-    put(B, c->buf[0].B, dd, 1, nullptr);
+    put(x, c->buf[0].x, d, 0, false);
+    put(v, c->buf[0].v, d, 0, false);
+    put(F, c->buf[0].F, dd, c->fp32 ? 3 : 1, true);  // FP32 keeps F - I
+    put(B, c->buf[0].B, dd, 1, false);
     std::vector<double> sc;
     const double* scp = scalars;
     if (c->prm.use_mibf) {  // simulation.cpp:138-145
@@ -1236,7 +1316,7 @@ int mtr_upload(mtr_ctx* c, const double* x, const double* v, const double* F, co
       for (uint32_t p = 0; p < Np; ++p) sc[(size_t)p * MTR_NUM_SCALARS + MTR_SCALAR_MUI] = m0;
       scp = sc.data();
     }
-    put(scp, c->buf[0].sc, MTR_NUM_SCALARS, 2, nullptr);
+    put(scp, c->buf[0].sc, MTR_NUM_SCALARS, 2, false);
     // initial grid: kept when the new scene's extent fits the grid there is
     uint32_t want[3];
     initial_grid_extent(c, x, want);

@@ -854,7 +854,7 @@ __device__ __forceinline__ void p2g_w_body(const StepArgsT<R>& A, const uint32_t
   const double ioh = P.one_over_dx;
   const R iohR = (R)ioh, apicD = (R)P.apicDinverse;
   const bool apic = P.flip_ratio < 0;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
   // XS lanes share a stencil column, each owning HN = 4 / XS of its x nodes
   constexpr int COLS = D == 3 ? 16 : 4, LPP = COLS * XS, HN = 4 / XS;
   const int q = lane % LPP;
@@ -1718,7 +1718,7 @@ __device__ __forceinline__ void g2p_musl_w_body(const StepArgsT<R>& A, const uin
   const double dt = H->dt, fr = P.flip_ratio, ioh = P.one_over_dx;
   const R apicD = (R)P.apicDinverse;
   const bool apic = fr < 0;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
   constexpr int COLS = D == 3 ? 16 : 4, LPP = COLS * XS, HN = 4 / XS;  // as in k_p2g_w
   const int q = lane % LPP;
   const int iy = D == 3 ? ((q % COLS) >> 2) : q % COLS;
@@ -2208,24 +2208,27 @@ __global__ void k_init_state(StepCommon A, PBufT<R> b) {  // tau of the uploaded
 // AoS (host layout, column-major matrices) <-> SoA, in original particle order.
 // kind 0: vector (D), 1: matrix (D*D, column-major AoS <-> (r*D+c) SoA),
 // 2: scalars (6), 3: matrix stored as M - I (the FP32 deformation gradient).
+// A null src stands for every particle's value being zero, or with eye set
+// (matrices) the identity: absent inputs are filled here, not copied.
 template <int D, typename R>
-__global__ void k_aos_to_soa(uint32_t Np, const double* __restrict__ src, R* dst, int kind) {
+__global__ void k_aos_to_soa(uint32_t Np, const double* __restrict__ src, R* dst, int kind, bool eye = false) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= Np) return;
   if (kind == 0) {
 #pragma unroll
-    for (int a = 0; a < D; ++a) dst[(size_t)a * Np + i] = (R)src[(size_t)i * D + a];
+    for (int a = 0; a < D; ++a) dst[(size_t)a * Np + i] = src ? (R)src[(size_t)i * D + a] : (R)0;
   } else if (kind == 1 || kind == 3) {
 #pragma unroll
     for (int r = 0; r < D; ++r)
 #pragma unroll
       for (int c = 0; c < D; ++c) {
-        const double m = src[(size_t)i * D * D + c * D + r];
+        const double m = src ? src[(size_t)i * D * D + c * D + r] : (eye && r == c ? 1.0 : 0.0);
         dst[(size_t)(r * D + c) * Np + i] = (R)(kind == 3 ? m - (r == c ? 1.0 : 0.0) : m);
       }
   } else {
 #pragma unroll
-    for (int q = 0; q < MTR_NUM_SCALARS; ++q) dst[(size_t)q * Np + i] = (R)src[(size_t)i * MTR_NUM_SCALARS + q];
+    for (int q = 0; q < MTR_NUM_SCALARS; ++q)
+      dst[(size_t)q * Np + i] = src ? (R)src[(size_t)i * MTR_NUM_SCALARS + q] : (R)0;
   }
 }
 

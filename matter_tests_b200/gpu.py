@@ -273,23 +273,23 @@ class GpuSim:
         return {"grid_mass": gm.value, "grid_momentum": gp, "particle_mass": pm.value, "particle_momentum": pp}
 
     # -- read-back ------------------------------------------------------
-    def particles(self, pic_flip=False):
+    def particles(self, pic_flip=False, fields=("x", "v", "F", "B", "scalars")):
+        """The particle state in the caller's order; `fields` names the arrays
+        to read back (the others are not copied and are absent)."""
         d, n = self.dim, self.Np
-        out = {"x": np.zeros(n * d), "v": np.zeros(n * d), "F": np.zeros(n * d * d), "B": np.zeros(n * d * d),
-               "scalars": np.zeros(n * 6)}
+        size = {"x": n * d, "v": n * d, "F": n * d * d, "B": n * d * d, "scalars": n * 6}
+        out = {k: np.zeros(size[k]) for k in fields}
         _check(self.lib, "mtr_download", self.lib.mtr_download(
-            self.h, *(_ptr(out[k]) for k in ("x", "v", "F", "B", "scalars"))))
+            self.h, *(_ptr(out.get(k)) for k in ("x", "v", "F", "B", "scalars"))))
         if pic_flip:
             out["pic"], out["flip"] = np.zeros(n * d), np.zeros(n * d)
             _check(self.lib, "mtr_download_pic_flip",
                    self.lib.mtr_download_pic_flip(self.h, _ptr(out["pic"]), _ptr(out["flip"])))
             out["pic"] = out["pic"].reshape(n, d)
             out["flip"] = out["flip"].reshape(n, d)
-        out["x"] = out["x"].reshape(n, d)
-        out["v"] = out["v"].reshape(n, d)
-        out["F"] = out["F"].reshape(n, d, d)
-        out["B"] = out["B"].reshape(n, d, d)
-        out["scalars"] = out["scalars"].reshape(n, 6)
+        shape = {"x": (n, d), "v": (n, d), "F": (n, d, d), "B": (n, d, d), "scalars": (n, 6)}
+        for k in fields:
+            out[k] = out[k].reshape(shape[k])
         return out
 
     def grid(self):

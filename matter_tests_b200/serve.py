@@ -13,6 +13,13 @@ and its step graph, updated in place rather than instantiated again.  A tick
 advances every member by `tick_steps` steps; each member has a step limit,
 so it stops exactly after the steps it asked for.
 
+Frame interval: with `frame_ms` set, a tick takes as many steps (1 to
+`tick_steps`) as a step-time model predicts will fit into `frame_ms` for the
+particles admitted at the time, so that ticks keep their cadence when a burst
+of arrivals makes the batch large.  The model is a least-squares line, ms per
+step against particles stepped, over the recent ticks that neither followed a
+membership change nor regrew a grid; until it has four, ticks take one step.
+
 Finished contexts are released lazily: a request's result is read back when
 it completes, but its device memory is freed only when the budget needs the
 room for a waiting request (or at the end of the run), because freeing device
@@ -57,7 +64,9 @@ class Server:
     (None keeps it)."""
 
     def __init__(self, budget_bytes, device=0, tick_steps=8, precision=PREC_MIXED, keep_result=("x", "v"),
-                 autotune=True, tune_reps=3, workers=1, shapes=None):
+                 autotune=True, tune_reps=3, workers=1, shapes=None, frame_ms=None):
+        self.frame_ms = frame_ms  # target wall time of a tick (None: every tick takes tick_steps steps)
+        self._fit = collections.deque(maxlen=64)  # (particles, ms per step) of clean ticks
         self.workers = int(workers)  # threads that prepare, read back and release requests
         self.autotune = autotune
         self.tune_reps = int(tune_reps)
@@ -73,11 +82,15 @@ class Server:
         self.tick_members = []   # scenes stepped in each tick
         self.tick_particles = []  # particles stepped in each tick
         self.tick_rebuilt = []   # the tick's batch was (re)built just before it
+        self.tick_regrown = []   # a member's grid outgrew its capacity inside the tick
+        self.tick_worker = []    # a request was being prepared or read back during the tick
+        self.tick_nsteps = []    # steps the tick took
         self.peak_members = 0
         self.peak_bytes = 0
         # wall time outside the ticks, by cause (seconds)
         self.host_s = {"idle": 0.0, "batch_build": 0.0, "release": 0.0}
         self.graph_updates = 0   # batch rebuilds that updated the step graph in place
+        self.wall_s = 0.0        # wall time of the last run()
 
     # -- worker-thread jobs -------------------------------------------------
     def _prepare(self, req):
@@ -92,7 +105,7 @@ class Server:
         return g
 
     def _finish(self, req):
-        st = req.sim.particles()
+        st = req.sim.particles(fields=self.keep)  # only what the result keeps is read back
         req.result = {k: st[k] for k in self.keep}
         req.result["clock"] = req.sim.clock()
         req.result["status"] = req.sim.status()
@@ -175,11 +188,22 @@ class Server:
                 for r in active:
                     if r.started is None:
                         r.started = ts
-                batch.step(self.tick_steps)
-                self.tick_ms.append((now() - ts) * 1e3)
+                worker = bool(preparing) or any(not f.done() for f in finishing)
+                regrowths = batch.stats()["regrowths"]
+                particles = sum(r.scene.Np for r in active)
+                nsteps = self._tick_steps(particles)
+                batch.step(nsteps)
+                tick_ms = (now() - ts) * 1e3
+                regrown = batch.stats()["regrowths"] > regrowths
+                self.tick_ms.append(tick_ms)
+                self.tick_nsteps.append(nsteps)
                 self.tick_members.append(len(active))
-                self.tick_particles.append(sum(r.scene.Np for r in active))
+                self.tick_particles.append(particles)
                 self.tick_rebuilt.append(rebuilt)
+                self.tick_regrown.append(regrown)
+                self.tick_worker.append(worker or any(not f.done() for f in preparing))
+                if not rebuilt and not regrown:
+                    self._fit.append((particles, tick_ms / nsteps))
                 self.peak_members = max(self.peak_members, len(active))
                 still = []
                 for r, ck in zip(active, batch.clocks()):
@@ -212,6 +236,21 @@ class Server:
                 pool.submit(self._release, r).result()
         return done
 
+    def _tick_steps(self, particles):
+        """Steps of the next tick: tick_steps, or with frame_ms set, the steps
+        the step-time model fits into frame_ms (at least 1)."""
+        if self.frame_ms is None:
+            return self.tick_steps
+        if len(self._fit) < 4:  # no model yet: one step, the shortest tick there is
+            return 1
+        P = np.array([p for p, _ in self._fit], dtype=np.float64)
+        T = np.array([t for _, t in self._fit], dtype=np.float64)
+        a, b = np.linalg.lstsq(np.stack([np.ones_like(P), P], 1), T, rcond=None)[0]
+        if a < 0.0 or b <= 0.0:  # degenerate fit (too narrow a spread of batch sizes): proportional
+            a, b = 0.0, float(np.mean(T / P))
+        est = a + b * particles
+        return int(np.clip(np.floor(self.frame_ms / est), 1, self.tick_steps))
+
     @staticmethod
     def _key(gr):
         return (gr["dim"], gr["spline_deg"], gr["fp32"], gr["musl"], gr["plastic_model_kernel"])
@@ -234,9 +273,12 @@ class Server:
     # -- report ---------------------------------------------------------------
     def _split(self, frame):
         rb = np.array(self.tick_rebuilt, dtype=bool)
+        rg = np.array(self.tick_regrown, dtype=bool)
+        wk = np.array(self.tick_worker, dtype=bool)
         mp = np.array(self.tick_particles, dtype=np.float64) / 1e6
         out = {}
-        for name, m in (("after_rebuild", rb), ("steady", ~rb)):
+        for name, m in (("after_rebuild", rb), ("steady", ~rb), ("with_regrowth", rg),
+                        ("worker_busy", wk & ~rg), ("neither", ~rg & ~wk)):
             if m.any():
                 out[name] = {"ticks": int(m.sum()), "p50": float(np.percentile(frame[m], 50)),
                              "p99": float(np.percentile(frame[m], 99)),
@@ -248,7 +290,7 @@ class Server:
         lat = np.array([r.done - r.arrival for r in done])
         wait = np.array([r.admitted - r.arrival for r in done])
         psteps = sum(r.scene.Np * r.steps for r in done)
-        per_step = np.array(self.tick_ms) / self.tick_steps
+        per_step = np.array(self.tick_ms) / np.array(self.tick_nsteps, dtype=np.float64)
         frame = np.array(self.tick_ms)
         span = max(r.done for r in done) - min(r.arrival for r in done)
         return {
@@ -259,13 +301,22 @@ class Server:
             "request_latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "queue_wait_s": {"p50": float(np.percentile(wait, 50)), "p99": float(np.percentile(wait, 99))},
             "step_latency_ms": {"p50": float(np.percentile(per_step, 50)), "p99": float(np.percentile(per_step, 99))},
-            # a frame of the serving loop = one tick: tick_steps steps of every admitted scene
+            # a frame of the serving loop = one tick: tick_steps steps of every admitted
+            # scene, or with frame_ms set, the steps that fit into it
             "frame_latency_ms": {"p50": float(np.percentile(frame, 50)), "p99": float(np.percentile(frame, 99))},
             # the same, split into ticks right after a membership change (their batch
-            # was rebuilt: new tables and a new step graph) and the other ticks; and
-            # per million particles stepped, which takes out the batch's size
+            # was rebuilt: new tables and a new step graph) and the other ticks; into
+            # ticks in which a member's grid regrew, ticks that ran while the worker
+            # prepared or read back a request, and the rest; and per million
+            # particles stepped, which takes out the batch's size
             "frame_latency_split_ms": self._split(frame),
+            "ticks_s": float(frame.sum() / 1e3),
+            "wall_s": float(self.wall_s),
             "tick_steps": self.tick_steps,
+            "frame_ms": self.frame_ms,
+            "steps_per_tick": {"p1": float(np.percentile(self.tick_nsteps, 1)),
+                               "p50": float(np.percentile(self.tick_nsteps, 50)),
+                               "mean": float(np.mean(self.tick_nsteps))},
             "ticks": len(self.tick_ms),
             "peak_members": self.peak_members,
             "mean_members": float(np.mean(self.tick_members)) if self.tick_members else 0.0,

@@ -215,3 +215,43 @@ def test_reupload_into_a_used_context():
             scale = max(np.abs(ref["p"][k]).max(), 1e-300)
             assert np.abs(got[k] - ref["p"][k]).max() <= 1e-10 * scale, (sc.name, k)
     g.close()
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_upload_download_round_trip_through_the_copy_staging(pinned):
+    """mtr_upload then mtr_download, no step: every field comes back bit for
+    bit in FP64.  700,001 particles make every array several staging chunks
+    (8 MB) long with a partial last chunk; pageable numpy arrays go through the
+    pinned staging, pinned ones are copied directly.  Absent F, B and scalars
+    are filled on the device (identity, zeros, zeros), and a download of some
+    fields leaves the others out."""
+    import torch
+    from matter_tests_b200.abi import PREC_FP64, default_params
+    from matter_tests_b200.gpu import GpuSim
+    n, d = 700_001, 3
+    rng = np.random.default_rng(21)
+
+    def arr(shape, lo=None):
+        a = rng.normal(size=shape) if lo is None else rng.uniform(lo, lo + 0.5, size=shape)
+        if not pinned:
+            return a
+        t = torch.empty(shape, dtype=torch.float64).pin_memory()
+        t.numpy()[...] = a
+        return t.numpy()
+    x = arr((n, d), lo=0.1)  # a 0.5 m cube: a 50-cell grid per axis
+    v, F, B, S = arr((n, d)), arr((n, d, d)), arr((n, d, d)), arr((n, 6))
+    p = default_params(d, 2)
+    p.dx = 0.01
+    p.precision = PREC_FP64
+    g = GpuSim(p)
+    g.upload(x, v, F, B, S)
+    got = g.particles()
+    for k, a in (("x", x), ("v", v), ("F", F), ("B", B), ("scalars", S)):
+        assert np.array_equal(got[k], a), k
+    part = g.particles(fields=("x", "v"))
+    assert set(part) == {"x", "v"} and np.array_equal(part["x"], x) and np.array_equal(part["v"], v)
+    g.upload(x, v)
+    got = g.particles()
+    assert np.array_equal(got["F"], np.broadcast_to(np.eye(d), (n, d, d)))
+    assert not got["B"].any() and not got["scalars"].any()
+    g.close()

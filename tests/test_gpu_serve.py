@@ -37,13 +37,14 @@ def alone(req):
     return out, ck
 
 
-@pytest.mark.parametrize("budget_factor", [1e3, 1.0])
-def test_requests_in_the_mix_match_alone(budget_factor):
+@pytest.mark.parametrize("budget_factor,frame_ms", [(1e3, None), (1.0, None), (1e3, 1.0)])
+def test_requests_in_the_mix_match_alone(budget_factor, frame_ms):
+    """frame_ms = 1: ticks of 1 to 8 steps, sized by the step-time model."""
     from matter_tests_b200.serve import Server, poisson_requests
     reqs = poisson_requests(6, rate=400.0, seed=11, steps=24, builder=small_request)
     from matter_tests_b200.gpu import footprint
     big = max(footprint(_mixed(r.scene.params), r.scene.x) for r in reqs)
-    srv = Server(budget_bytes=int(big * budget_factor), tick_steps=8)
+    srv = Server(budget_bytes=int(big * budget_factor), tick_steps=8, frame_ms=frame_ms)
     done = srv.run(reqs)
     assert len(done) == len(reqs)
     assert srv.peak_bytes <= srv.budget  # admission never exceeds the budget
