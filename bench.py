@@ -244,6 +244,20 @@ def kernel_bytes(name, p, Np, Ga, G, wr=8.0):
     return None
 
 
+def roofline_of(kernel_ms, p, Np, Ga, G, wr):
+    """Roofline of the dominant kernel among per-launch kernel times
+    (`kernel_ms`: name -> ms per launch): its algorithmic bytes per launch
+    (kernel_bytes) over its time, against the measured HBM peak."""
+    peak, peak_kind = hbm_peak()
+    dom = max((k for k in kernel_ms if k.startswith("k_")), key=lambda k: kernel_ms[k])
+    dom_bytes = kernel_bytes(dom, p, Np, Ga, G, wr)
+    achieved = dom_bytes / (kernel_ms[dom] / 1e3) / 1e9 if dom_bytes else None
+    return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+            "kernel_ms": kernel_ms[dom], "kernel_algorithmic_bytes": dom_bytes, "active_nodes": Ga,
+            "grid_nodes": G}
+
+
 def step_bytes(p, Np, Ga, wr=8.0):
     """Whole-step algorithmic bytes: the persistent particle state read and
     written once (x v F B + 3 plastic scalars read; the same + 3 diagnostics
@@ -514,8 +528,9 @@ def config_runs(args, local):
     """Each single-scene workload at full size over its full length, plain
     FP64 and mixed: device-timed particle-steps/s (16 untimed steps first,
     which capture the step graphs; the block shapes tuned after them), the
-    per-kernel times of 3 profiled steps after the run, and the mixed
-    state's error against the FP64 state at the last step."""
+    per-kernel times of 3 profiled steps after the run with the roofline of
+    the dominant kernel there, and the mixed state's error against the FP64
+    state at the last step."""
     import copy
     import torch
     from matter_tests_b200 import scenes
@@ -547,14 +562,17 @@ def config_runs(args, local):
             states[key] = g.particles()
             status, _ = g.status()
             slots = g.profile(3)
+            Ga, G = g.active_nodes()
             agg, cnt = {}, {}
             for kn, t in slots:
                 agg[kn] = agg.get(kn, 0.0) + t
                 cnt[kn] = cnt.get(kn, 0) + 1
             g.close()
+            kms = {k: agg[k] / cnt[k] for k in agg}
             res[key] = {"value": sc.Np * (nsteps - warm) / (ms / 1e3), "ms_per_step": ms / (nsteps - warm),
                         "steps": int(ck["step"]), "status_flags": status,
-                        "kernel_ms": {k: round(agg[k] / cnt[k], 5) for k in agg}}
+                        "kernel_ms": {k: round(v, 5) for k, v in kms.items()},
+                        "roofline": roofline_of(kms, p, sc.Np, Ga, G, 4.0 if prec == PREC_MIXED else 8.0)}
         err = mixed_error(sc, states["fp64"], states["mixed"])
         out[name] = {"Np": sc.Np, "steps": nsteps, "fp64": res["fp64"], "mixed": res["mixed"],
                      "mixed_over_fp64": res["mixed"]["value"] / res["fp64"]["value"],
