@@ -188,8 +188,9 @@ def kernel_source_hash():
     return h.hexdigest()[:16]
 
 
-def measured_traffic(workload, scale, kernel, precision):
-    """(bytes per launch, source) of the ncu capture for this kernel, or (None, why)."""
+def capture_entry(workload, scale, kernel, precision):
+    """(entry, None) of the ncu capture of this kernel taken on the current
+    kernel sources, or (None, why not)."""
     try:
         with open(TRAFFIC_FILE) as f:
             tab = json.load(f)
@@ -200,8 +201,23 @@ def measured_traffic(workload, scale, kernel, precision):
                 and e.get("precision") == precision):
             if e.get("source_hash", tab.get("source_hash")) != kernel_source_hash():
                 return None, "capture predates the current kernel sources"
-            return float(e["dram_bytes_per_launch"]), "ncu capture (profiles/dram_traffic.json): " + e.get("note", "")
+            return e, None
     return None, "no capture of this kernel"
+
+
+def measured_traffic(workload, scale, kernel, precision):
+    """(bytes per launch, source) of the ncu capture for this kernel, or (None, why)."""
+    e, why = capture_entry(workload, scale, kernel, precision)
+    if e is None:
+        return None, why
+    return float(e["dram_bytes_per_launch"]), "ncu capture (profiles/dram_traffic.json): " + e.get("note", "")
+
+
+def measured_pipes(workload, scale, kernel, precision):
+    """Pipe utilisation and top stalls of the same capture (what bounds a
+    kernel that is far from the HBM roofline), or None."""
+    e, _ = capture_entry(workload, scale, kernel, precision)
+    return None if e is None else e.get("pipes")
 
 
 def hbm_peak():
@@ -481,6 +497,8 @@ def measure(args, world, rank, local, sc, precision, sampler=None):
            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                         "traffic": traffic, "traffic_source": traffic_src,
+                        "pipes": measured_pipes(args.workload, args.scale, dom,
+                                                "mixed" if precision == PREC_MIXED else "fp64"),
                         "peak_source": peak_kind,
                         "kernel_ms": dom_ms, "kernel_algorithmic_bytes": dom_bytes,
                         "step_algorithmic_GBps": whole, "step_frac": whole / peak,

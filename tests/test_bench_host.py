@@ -22,3 +22,19 @@ def test_mixed_kernels_count_four_bytes_per_value_except_positions():
     b8 = bench.kernel_bytes("k_p2g", p, 1000, 0, 0, 8.0)
     b4 = bench.kernel_bytes("k_p2g", p, 1000, 0, 0, 4.0)
     assert b8 > b4 > b8 / 2  # positions stay FP64 on the mixed path
+
+
+def test_capture_figures_are_used_only_on_the_kernel_sources_they_were_taken_on(monkeypatch):
+    """profiles/dram_traffic.json: DRAM bytes and pipe utilisation of the C2
+    tile kernels, reported while the kernel headers hash as at capture."""
+    for prec in ("fp64", "mixed"):
+        for k in ("k_p2g", "k_g2p_musl", "k_defgrad"):
+            b, src = bench.measured_traffic("collapse3d_mui", 1.0, k, prec)
+            assert b and b > 0 and src.startswith("ncu capture"), (k, prec, src)
+            pipes = bench.measured_pipes("collapse3d_mui", 1.0, k, prec)
+            assert 0 < pipes["issue_active_pct"] <= 100 and pipes["top_stalls"]
+    assert bench.measured_pipes("incline3d_mcc", 1.0, "k_g2p", "fp64") is None
+    monkeypatch.setattr(bench, "kernel_source_hash", lambda: "0" * 16)
+    b, why = bench.measured_traffic("collapse3d_mui", 1.0, "k_p2g", "fp64")
+    assert b is None and "predates" in why
+    assert bench.measured_pipes("collapse3d_mui", 1.0, "k_p2g", "fp64") is None
